@@ -1,0 +1,325 @@
+"""Benchmark of the FR residual + SSP-RK3 hot path: DOF-RHS evaluations/s.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Workload: the 256x256 jittered (seed 1, +-0.15h) Q1 Taylor-Green mesh on
+[0,pi]^2 with slip walls, P3 (65 536 elements, 1 048 576 DOF per variable),
+TGV initial state at M=0.3.  One bench step = one SSP-RK3 time step = three
+residual evaluations over the whole mesh; DOF-RHS/s = E * n_sp * 3 * K / t.
+
+ours:      the CUDA path, timed with CUDA events on the solver's stream, max
+           over ranks; N > 1 runs one independent replica per GPU (the path
+           has no exchange on one GPU; weak scaling).
+reference: the oracle (the CPU restatement of the reference's residual, the
+           reference having no CPU path) with every host thread, rank 0 only.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "DOF-RHS evals/s, FP32-split vs FP64 GPU at stated L2 err; adjoint/fwd ratio"
+UNIT = "DOF-RHS/s"
+GAMMA, MACH = 1.4, 0.3
+NX = 256
+P = 3
+DT = 2.0e-4
+
+
+def workload_name():
+    return f"TGV {NX}x{NX} jittered Q1 quads on [0,pi]^2, slip walls, P{P}, SSP-RK3"
+
+
+def load_peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def algorithmic_bytes_per_element(p, w_s=8, w_g=8, w_t=8, viscous=False):
+    """Bytes one element moves per residual evaluation with the fused RK stage:
+    w_s*12*n_sp (stage state, base state, output) + w_g*5*n_sp (J and four
+    metric terms) + w_t*32*n_f (own trace write + neighbour trace read)
+    [+ w_t*64*n_f for the gradient traces of Navier-Stokes]."""
+    nsp, nf = (p + 1) ** 2, p + 1
+    b = w_s * 12 * nsp + w_g * 5 * nsp + w_t * 32 * nf
+    if viscous:
+        b += w_t * 64 * nf
+    return b
+
+
+def traffic_from_profile(kernel_key):
+    """Per-launch DRAM bytes of the dominant kernel from the committed ncu
+    summary (profiles/traffic.json), or None."""
+    try:
+        with open(os.path.join(ROOT, "profiles", "traffic.json")) as f:
+            return json.load(f).get(kernel_key)
+    except Exception:
+        return None
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.Q}",
+                 "--format=csv,noheader,nounits", "-lms", "100"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        self.t.join(timeout=2)
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax = float(f[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def build_case():
+    from zhijian_b200 import meshgen as M
+    mesh = M.tgv_mesh(NX, seed=1)
+    return mesh
+
+
+def make_solver(mesh):
+    from zhijian_b200.solver import FRSolver, make_params
+    prm = make_params(poly_order=P, gamma=GAMMA, rho_inf=1.0, p_inf=1.0 / (GAMMA * MACH * MACH),
+                      Mach=MACH, flux_type="HU", riemann="Rusanov", viscous=False,
+                      bcs=[(1, "slipwall")])
+    return FRSolver(mesh, prm)
+
+
+def cpu_baseline(mesh, seconds=10.0):
+    """The oracle (compat FP64) on the host cores over a bounded sample: SSP-RK3
+    steps on a 64x64-element block of the same mesh density."""
+    from oracle import oracle as O
+    from zhijian_b200 import meshgen as M
+    threads = os.cpu_count() or 1
+    sub = M.structured_quads(64, 64, 0.0, math.pi / 4, 0.0, math.pi / 4, 0.15, 1, (1, 1, 1, 1),
+                             {1: "slipwall"})
+    orc = O.Oracle(sub, P, GAMMA, 1.0, 1.0 / (GAMMA * MACH * MACH), MACH, 0.0, threads=threads)
+    U = M.taylor_green(orc.sp_coords())
+    orc.step(U, DT, 1)  # warm-up
+    n, t0 = 0, time.perf_counter()
+    while True:
+        U, _ = orc.step(U, DT, 1)
+        n += 1
+        el = time.perf_counter() - t0
+        if el >= seconds or n >= 1000:
+            break
+    dof = sub.n_elem * (P + 1) ** 2
+    return {"value": dof * 3 * n / el, "unit": UNIT, "cores": threads, "kind": "port",
+            "sample": f"{n} SSP-RK3 steps of a 64x64 jittered P{P} TGV block "
+                      f"({sub.n_elem} elements), {el:.1f} s"}
+
+
+def run_reference(args):
+    """--impl reference: the oracle port with all host threads, rank 0 only."""
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return None
+    from oracle import oracle as O
+    from zhijian_b200 import meshgen as M
+    threads = os.cpu_count() or 1
+    sub = M.structured_quads(64, 64, 0.0, math.pi / 4, 0.0, math.pi / 4, 0.15, 1, (1, 1, 1, 1),
+                             {1: "slipwall"})
+    orc = O.Oracle(sub, P, GAMMA, 1.0, 1.0 / (GAMMA * MACH * MACH), MACH, 0.0, threads=threads)
+    U = M.taylor_green(orc.sp_coords())
+    for _ in range(args.warmup):
+        U, _ = orc.step(U, DT, 1)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        U, _ = orc.step(U, DT, 1)
+    el = time.perf_counter() - t0
+    dof = sub.n_elem * (P + 1) ** 2
+    v = dof * 3 * args.steps / el
+    return {"metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": 1e3 * el / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "impl": "reference",
+            "config": {"workload": workload_name() + " (CPU sample: 64x64 block per step)",
+                       "mode": "compat", "precision": "fp64"},
+            "cpu_baseline": {"value": v, "unit": UNIT, "cores": threads, "kind": "port",
+                             "sample": f"each step: one SSP-RK3 step of a 64x64 jittered block "
+                                       f"({sub.n_elem} elements, P{P})"},
+            "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+
+
+def run_ours(args):
+    import torch
+    import torch.distributed as dist
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+
+    def barrier_sync():
+        torch.cuda.synchronize()
+        if world > 1:
+            dist.barrier(device_ids=[local])
+        torch.cuda.synchronize()
+
+    def max_over_ranks(x):
+        if world == 1:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    from zhijian_b200 import meshgen as M
+    mesh = build_case()
+    s = make_solver(mesh)
+    stream = torch.cuda.current_stream(dev)
+    s.set_stream(stream.cuda_stream)
+    U0 = M.taylor_green(s.solution_point_coords())
+    s.copyToDevice(U0)
+    dof = s.n_elem * s.n_sp
+    s.advance(DT, args.warmup)
+    barrier_sync()
+
+    sampler = ClockSampler(local)
+    sampler.start()
+    time.sleep(0.3)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    barrier_sync()
+    e0.record(stream)
+    s.advance(DT, args.steps, sync=False)
+    e1.record(stream)
+    barrier_sync()
+    ms = e0.elapsed_time(e1)
+    clocks = sampler.stop()
+    s.check_state()
+    ms = max_over_ranks(ms)
+    value = world * dof * 3 * args.steps / (ms * 1e-3)
+    launches = 3 * args.steps
+
+    # roofline of the dominant kernel (the fused stage kernel: every launch)
+    per_launch_s = ms * 1e-3 / launches
+    bytes_launch = algorithmic_bytes_per_element(P) * s.n_elem
+    peak, peak_kind = load_peaks()
+    achieved = bytes_launch / per_launch_s / 1e9
+    traffic = traffic_from_profile(f"k_compat_stage<3>|tgv{NX}")
+    roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                "frac": achieved / peak, "traffic": traffic, "peak_kind": peak_kind,
+                "kernel": "k_compat_stage<3>",
+                "algorithmic_bytes_per_launch": bytes_launch}
+
+    # end to end through the C-ABI with host buffers: per step the state goes
+    # H2D from pinned memory, one SSP-RK3 step, the new state comes back D2H
+    n_e2e = max(3, min(args.steps, 50))
+    host = torch.from_numpy(U0.copy()).pin_memory()
+    hnp = host.numpy()
+    s.copyToDevice(hnp)
+    s.advance(DT, 1)
+    barrier_sync()
+    f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    f0.record(stream)
+    for _ in range(n_e2e):
+        s.copyToDevice(hnp)
+        s.advance(DT, 1, sync=False)
+        s.copyToHost(out=hnp)
+    f1.record(stream)
+    barrier_sync()
+    ems = max_over_ranks(f0.elapsed_time(f1))
+    e2e = {"value": world * dof * 3 * n_e2e / (ems * 1e-3), "unit": UNIT,
+           "h2d_bytes_per_step": int(U0.nbytes), "d2h_bytes_per_step": int(U0.nbytes),
+           "steps": n_e2e}
+
+    out = None
+    if rank == 0:
+        out = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+               "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
+               "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+               "dtype": "f64", "data": "synthetic",
+               "config": {"workload": workload_name(), "elements": s.n_elem,
+                          "dof_per_var": dof, "rhs_per_step": 3, "mode": "compat",
+                          "precision": "fp64", "dt": DT,
+                          "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
+                          "l2": "no flush: each stage streams ~200 MB > 126 MB L2"},
+               "roofline": roofline, "e2e": e2e, "gpu_launches": launches, "clocks": clocks}
+        if world == 1 and not args.no_cpu_baseline:
+            out["cpu_baseline"] = cpu_baseline(mesh, args.cpu_seconds)
+    s.close()
+    if world > 1:
+        dist.destroy_process_group()
+    return out
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=300)
+    ap.add_argument("--warmup", type=int, default=10)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-seconds", type=float, default=10.0)
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        out = run_reference(args)
+    else:
+        from zhijian_b200 import build
+        build.build()
+        out = run_ours(args)
+    if out is not None:
+        print(json.dumps(out), flush=True)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,187 @@
+/*
+ * zj_fr.h -- C-ABI of the B200-native Flux-Reconstruction hot path.
+ *
+ * One handle (zj_solver) replaces one reference zhijian::FRSolver
+ * (include/solver/fr_solver.hpp:77-180 in the Zhijian project).  Plain
+ * pointers and sizes only; no C++ or torch types cross this boundary.
+ * Every call returns a zj_status and never exits the process; the text of the
+ * last error is available from zj_last_error().
+ *
+ * State layout on both sides of the boundary is the reference's AoS layout
+ * [element][solution point][variable], variables (rho, rho*u, rho*v, rho*E),
+ * solution point sp = j*(P+1) + i with i the xi index and j the eta index
+ * (src/basis/basis.cpp:479-487).
+ */
+#ifndef ZJ_FR_H
+#define ZJ_FR_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define ZJ_ABI_VERSION 1
+
+/* Error codes.  The reference aborts through CUDA_CHECK -> std::exit
+ * (include/common/cuda_utils.hpp:13-21); here every failure is returned. */
+typedef enum zj_status {
+    ZJ_OK = 0,
+    ZJ_ERR_ARG = 1,          /* bad argument, size or mesh */
+    ZJ_ERR_CUDA = 2,         /* CUDA runtime error */
+    ZJ_ERR_NAN = 3,          /* non-finite value detected in the state */
+    ZJ_ERR_TIMEOUT = 4,      /* a bounded device wait gave up */
+    ZJ_ERR_UNSUPPORTED = 5,  /* valid request this build does not implement */
+    ZJ_ERR_IO = 6            /* file could not be read or parsed */
+} zj_status;
+
+/* Boundary types, numbered as the reference BCType (include/common/types.hpp:47-56). */
+typedef enum zj_bc_type {
+    ZJ_BC_INTERIOR = 0, ZJ_BC_WALL = 1, ZJ_BC_SLIPWALL = 2, ZJ_BC_SYMMETRY = 3,
+    ZJ_BC_FARFIELD = 4, ZJ_BC_INFLOW = 5, ZJ_BC_OUTFLOW = 6, ZJ_BC_PERIODIC = 7
+} zj_bc_type;
+
+/* FR correction family (types.hpp:59-64) and Riemann solver (types.hpp:67-71). */
+typedef enum zj_flux_type { ZJ_FLUX_DG = 0, ZJ_FLUX_SD = 1, ZJ_FLUX_HU = 2, ZJ_FLUX_GA = 3 } zj_flux_type;
+typedef enum zj_riemann { ZJ_RIEMANN_RUSANOV = 0, ZJ_RIEMANN_ROE = 1, ZJ_RIEMANN_HLLC = 2 } zj_riemann;
+
+/* Arithmetic of the residual.  ZJ_FP64: FP64 end to end.  ZJ_MIXED: FP32
+ * volume and face work, FP64 stage accumulation, reductions and metrics. */
+typedef enum zj_precision { ZJ_FP64 = 0, ZJ_MIXED = 1 } zj_precision;
+
+/* Element kinds of the mesh descriptor (types.hpp:41-44). */
+typedef enum zj_elem_type { ZJ_ELEM_TRI = 0, ZJ_ELEM_QUAD = 1 } zj_elem_type;
+
+#define ZJ_MAX_BC 32
+
+/* One "bc <tag> <type> [key value ...]" config line (src/main.cpp:132-166). */
+typedef struct zj_bc_spec {
+    int tag;
+    int type;          /* zj_bc_type */
+    double p_static;   /* outflow; 0 = p_inf */
+    double p_total;    /* inflow; 0 = 1.2 p_inf */
+    double T_total;    /* inflow; 0 = T_inf */
+    double T_wall;     /* isothermal wall; 0 = adiabatic */
+    double dir_x, dir_y;
+} zj_bc_spec;
+
+/* Solver parameters: the fields of the reference SimParams
+ * (include/common/types.hpp:130-172) plus the two selectors of this build.
+ * zj_params_default() gives the reference defaults. */
+typedef struct zj_params {
+    double gamma, Pr, Re, Mach, T_inf, p_inf, rho_inf, AoA;
+    int poly_order;
+    int flux_type;     /* zj_flux_type */
+    int riemann;       /* zj_riemann */
+    double CFL, dt, t_final;
+    int max_iter;
+    int viscous;
+    int output_freq, restart_freq;
+    char case_name[64];
+    /* compat = 1: reproduce the reference residual exactly, quirks included
+     * (hard-coded Rusanov, inviscid, Radau correction, no metric scaling of
+     * the correction, dimensional clamps).  compat = 0: the conservative FR
+     * scheme the parameters ask for (physics mode). */
+    int compat;
+    int precision;     /* zj_precision */
+    int n_bc;
+    zj_bc_spec bc[ZJ_MAX_BC];
+} zj_params;
+
+/* Mesh descriptor: borrowed for the duration of zj_solver_create only.
+ * Element e has nodes conn[conn_offsets[e] .. conn_offsets[e+1]), vertices
+ * first and counter-clockwise (Q1: 4 nodes, Q2: 9, Q4: 25; gmsh ordering as
+ * src/basis/basis.cpp:706-770).  bnd_edges[3*k .. 3*k+2] = (v0, v1, tag);
+ * the bc table of zj_params maps tags to boundary types.  Untagged boundary
+ * edges are far-field (src/mesh/mesh.cpp:48-57). */
+typedef struct zj_mesh_desc {
+    int64_t n_nodes;
+    const double* xy;            /* [n_nodes][2] */
+    int64_t n_elem;
+    const int32_t* elem_type;    /* [n_elem] zj_elem_type */
+    const int32_t* elem_order;   /* [n_elem] 1, 2 or 4 */
+    const int64_t* conn_offsets; /* [n_elem + 1] */
+    const int64_t* conn;
+    int64_t n_bnd_edges;
+    const int64_t* bnd_edges;    /* [n_bnd_edges][3] */
+} zj_mesh_desc;
+
+typedef struct zj_solver zj_solver;
+
+/* ---- parameters and configuration (src/main.cpp:78-170) ----------------- */
+void zj_params_default(zj_params* p);
+/* Parse a config file with the reference grammar: "key value" lines, '#'
+ * comments, unknown keys ignored; adds keys "compat on|off" and
+ * "precision fp64|mixed". */
+zj_status zj_params_parse_file(const char* path, zj_params* p);
+zj_status zj_params_parse_string(const char* text, zj_params* p);
+
+/* ---- lifetime (FRSolver::initialize, fr_solver.cpp:30-73) -------------- */
+/* Builds faces, normals, metrics and operators on the host, allocates every
+ * device buffer once and uploads; later calls allocate nothing. */
+zj_status zj_solver_create(const zj_mesh_desc* mesh, const zj_params* params,
+                           zj_solver** out);
+void zj_solver_destroy(zj_solver* s);
+/* Last error text of this handle, or of the last failed create when s is NULL. */
+const char* zj_last_error(const zj_solver* s);
+int zj_abi_version(void);
+
+/* ---- sizes ---------------------------------------------------------------- */
+int64_t zj_num_elements(const zj_solver* s);
+int zj_num_solution_points(const zj_solver* s);      /* per element */
+int64_t zj_num_faces(const zj_solver* s);
+int64_t zj_state_size(const zj_solver* s);            /* E * n_sp * 4 */
+
+/* ---- initial condition (FRSolver::setInitialCondition, fr_solver.cpp:268-299)
+ * A C ABI cannot carry std::function: fetch the physical coordinates of the
+ * solution points, evaluate the initial state on the host, then set it. */
+zj_status zj_solution_point_coords(const zj_solver* s, double* xy /* [E][n_sp][2] */);
+/* copyToDevice / copyToHost (fr_solver.cpp:835-871), host buffers.  Setting
+ * the state resets time and iteration like setInitialCondition. */
+zj_status zj_set_state(zj_solver* s, const double* U_host);
+zj_status zj_get_state(zj_solver* s, double* U_host);
+/* Same with device buffers (no host copy). */
+zj_status zj_set_state_device(zj_solver* s, const double* U_dev);
+zj_status zj_get_state_device(zj_solver* s, double* U_dev);
+
+/* ---- the hot path ---------------------------------------------------------- */
+/* nsteps SSP-RK3 steps of size dt (FRSolver::advance, fr_solver.cpp:305-333),
+ * queued on the handle's stream; returns once the steps are enqueued and
+ * checked for launch errors.  zj_synchronize waits for them. */
+zj_status zj_step(zj_solver* s, double dt, int nsteps);
+zj_status zj_synchronize(zj_solver* s);
+/* One residual R = dU/dt on device buffers of E*n_sp*4 doubles, on the
+ * handle's stream (computeResidual_GPU, fr_solver.cpp:335-608).  Borrowed. */
+zj_status zj_rhs(zj_solver* s, const double* U_dev, double* R_dev);
+/* Same through host buffers: H2D, residual, D2H, synchronised. */
+zj_status zj_rhs_host(zj_solver* s, const double* U_host, double* R_host);
+/* L2 norm of the residual of the last stage of the last step
+ * (FRSolver::computeResidual, fr_solver.cpp:818-833), reduced on the device. */
+zj_status zj_residual_norm(zj_solver* s, double* out);
+/* CFL time step over the current device state (FRSolver::computeTimeStep,
+ * fr_solver.cpp:784-816; the reference evaluates it on a stale host copy). */
+zj_status zj_compute_dt(zj_solver* s, double* dt_out);
+/* Non-finite check of the current state: ZJ_ERR_NAN if any value is NaN/Inf
+ * (replaces the reference's host-side checkNaN, fr_solver.cpp:11-22). */
+zj_status zj_check_state(zj_solver* s);
+double zj_time(const zj_solver* s);
+int zj_iteration(const zj_solver* s);
+
+/* Stream: the handle owns a stream; a caller stream may be set instead
+ * (NULL restores the owned one).  cudaStream_t passed as void*. */
+zj_status zj_set_stream(zj_solver* s, void* stream);
+void* zj_get_stream(const zj_solver* s);
+
+/* ---- config-file convenience: parse + mesh from a Gmsh file ---------------- */
+/* Read an ASCII Gmsh MSH v2.2 / v4.1 quad mesh (src/mesh/gmsh_reader.cpp:161)
+ * and create a solver.  Physical names map to boundary types as
+ * GmshReader::inferBCType (gmsh_reader.cpp:117-155) unless the params' bc
+ * table names the tag. */
+zj_status zj_solver_create_from_gmsh(const char* msh_path, const zj_params* params,
+                                     zj_solver** out);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* ZJ_FR_H */

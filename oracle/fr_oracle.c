@@ -1,0 +1,771 @@
+/*
+ * fr_oracle.c -- TEST INFRASTRUCTURE, NOT PRODUCT CODE (see fr_oracle.h).
+ *
+ * Plain-C restatement of the reference FR hot path in its own loop and
+ * summation order.  Compile with -ffp-contract=off: every product and sum is
+ * rounded as written, like the reference host code and unlike an FMA-fused
+ * GPU build (which differs from it by a few ulp per operation).
+ *
+ * Reference map (paths inside the Zhijian project):
+ *   Gauss-Legendre points      src/basis/basis.cpp:12-104
+ *   Lagrange eval / deriv      src/basis/basis.cpp:169-224
+ *   correction derivatives     src/basis/basis.cpp:314-379
+ *   FROperators::initQuad      src/basis/basis.cpp:464-613
+ *   shape functions, Jacobian  src/basis/basis.cpp:717-893
+ *   Mesh::buildFaces           src/mesh/mesh.cpp:18-83
+ *   areas, normals, centroids  src/mesh/mesh.cpp:109-194
+ *   initGeometry               src/solver/fr_solver.cpp:85-129
+ *   BC packing                 src/solver/fr_solver.cpp:432-494
+ *   advance                    src/solver/fr_solver.cpp:305-333
+ *   computeTimeStep            src/solver/fr_solver.cpp:784-816
+ *   IdealGas                   include/physics/euler.hpp:16-129
+ *   kernels K1,K4,K8,K9,K10,K13,K15,K17,K18  src/gpu/kernels.cu (see each fn)
+ */
+#include "fr_oracle.h"
+
+#include <math.h>
+#include <stdlib.h>
+#include <string.h>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+enum { BC_INTERIOR = 0, BC_WALL = 1, BC_SLIPWALL = 2, BC_SYMMETRY = 3,
+       BC_FARFIELD = 4, BC_INFLOW = 5, BC_OUTFLOW = 6, BC_PERIODIC = 7 };
+
+struct orc_ctx {
+    int P, n1, nsp, nfp, nn, eorder;
+    int64_t n_elem, n_nodes, n_faces;
+    double gamma, rho_inf, u_inf, v_inf, p_inf;
+    double* xy;       /* [n_nodes][2] */
+    int64_t* conn;    /* [E][nn] */
+    /* geometry */
+    double *J, *Jinv, *area;
+    /* faces */
+    int *fle, *fll, *fre, *frl, *fbct, *ftag, *fbcmap;
+    double *fn, *bc_data;
+    /* operators */
+    double *pts, *D1, *dxi, *deta, *interp, *corr;
+    /* work */
+    double *Fx, *Fy, *Ufp, *Fcom, *Fdiff, *U0, *U1;
+    int nthreads;
+};
+
+/* ---------------------------------------------------------------- basis -- */
+
+/* basis.cpp:12-104 */
+static void gl_points(int n, double* x, double* w) {
+    switch (n) {
+    case 1: x[0] = 0.0; w[0] = 2.0; break;
+    case 2: x[0] = -1.0 / sqrt(3.0); x[1] = 1.0 / sqrt(3.0); w[0] = w[1] = 1.0; break;
+    case 3:
+        x[0] = -sqrt(3.0 / 5.0); x[1] = 0.0; x[2] = sqrt(3.0 / 5.0);
+        w[0] = w[2] = 5.0 / 9.0; w[1] = 8.0 / 9.0; break;
+    case 4:
+        x[0] = -sqrt(3.0 / 7.0 + 2.0 / 7.0 * sqrt(6.0 / 5.0));
+        x[1] = -sqrt(3.0 / 7.0 - 2.0 / 7.0 * sqrt(6.0 / 5.0));
+        x[2] = sqrt(3.0 / 7.0 - 2.0 / 7.0 * sqrt(6.0 / 5.0));
+        x[3] = sqrt(3.0 / 7.0 + 2.0 / 7.0 * sqrt(6.0 / 5.0));
+        w[0] = w[3] = (18.0 - sqrt(30.0)) / 36.0;
+        w[1] = w[2] = (18.0 + sqrt(30.0)) / 36.0; break;
+    case 5:
+        x[0] = -sqrt(5.0 + 2.0 * sqrt(10.0 / 7.0)) / 3.0;
+        x[1] = -sqrt(5.0 - 2.0 * sqrt(10.0 / 7.0)) / 3.0;
+        x[2] = 0.0;
+        x[3] = sqrt(5.0 - 2.0 * sqrt(10.0 / 7.0)) / 3.0;
+        x[4] = sqrt(5.0 + 2.0 * sqrt(10.0 / 7.0)) / 3.0;
+        w[0] = w[4] = (322.0 - 13.0 * sqrt(70.0)) / 900.0;
+        w[1] = w[3] = (322.0 + 13.0 * sqrt(70.0)) / 900.0;
+        w[2] = 128.0 / 225.0; break;
+    case 6: /* the reference's 15-digit table */
+        x[0] = -0.932469514203152; x[1] = -0.661209386466265; x[2] = -0.238619186083197;
+        x[3] = 0.238619186083197;  x[4] = 0.661209386466265;  x[5] = 0.932469514203152;
+        w[0] = w[5] = 0.171324492379170; w[1] = w[4] = 0.360761573048139;
+        w[2] = w[3] = 0.467913934572691; break;
+    default:
+        for (int i = 0; i < n; ++i) {
+            double xx = cos(M_PI * (i + 0.75) / (n + 0.5));
+            for (int it = 0; it < 20; ++it) {
+                double P0 = 1.0, P1 = xx;
+                for (int j = 2; j <= n; ++j) {
+                    double Pn = ((2 * j - 1) * xx * P1 - (j - 1) * P0) / j;
+                    P0 = P1; P1 = Pn;
+                }
+                double dP = n * (xx * P1 - P0) / (xx * xx - 1.0);
+                double dx = P1 / dP;
+                xx -= dx;
+                if (fabs(dx) < 1e-15) break;
+            }
+            x[i] = xx;
+            double P0 = 1.0, P1 = xx;
+            for (int j = 2; j <= n; ++j) {
+                double Pn = ((2 * j - 1) * xx * P1 - (j - 1) * P0) / j;
+                P0 = P1; P1 = Pn;
+            }
+            double dP = n * (xx * P1 - P0) / (xx * xx - 1.0);
+            w[i] = 2.0 / ((1.0 - xx * xx) * dP * dP);
+        }
+    }
+}
+
+/* basis.cpp:169-178 */
+static double lag_eval(const double* nodes, int n, int j, double x) {
+    double r = 1.0;
+    for (int i = 0; i < n; ++i)
+        if (i != j) r *= (x - nodes[i]) / (nodes[j] - nodes[i]);
+    return r;
+}
+
+/* basis.cpp:180-196 */
+static double lag_deriv(const double* nodes, int n, int j, double x) {
+    double r = 0.0;
+    for (int k = 0; k < n; ++k) {
+        if (k == j) continue;
+        double term = 1.0 / (nodes[j] - nodes[k]);
+        for (int i = 0; i < n; ++i)
+            if (i != j && i != k) term *= (x - nodes[i]) / (nodes[j] - nodes[i]);
+        r += term;
+    }
+    return r;
+}
+
+static double legendre(int n, double x) {
+    if (n == 0) return 1.0;
+    if (n == 1) return x;
+    double P0 = 1.0, P1 = x;
+    for (int i = 2; i <= n; ++i) {
+        double Pn = ((2 * i - 1) * x * P1 - (i - 1) * P0) / i;
+        P0 = P1; P1 = Pn;
+    }
+    return P1;
+}
+
+static double legendre_deriv(int n, double x) {
+    if (n == 0) return 0.0;
+    double Pn = legendre(n, x), Pn1 = legendre(n - 1, x);
+    if (fabs(x * x - 1.0) < 1e-14)
+        return n * (n + 1) / 2.0 * ((x > 0) ? 1.0 : ((n % 2 == 0) ? 1.0 : -1.0));
+    return n / (x * x - 1.0) * (x * Pn - Pn1);
+}
+
+/* basis.cpp:314-348 (Radau left; the reference ignores flux_type) */
+static double gL_deriv(int p, double x) {
+    double dPp = legendre_deriv(p, x), dPp1 = legendre_deriv(p + 1, x);
+    double sign = (p % 2 == 0) ? 1.0 : -1.0;
+    return sign * 0.5 * (dPp - dPp1);
+}
+
+/* basis.cpp:350-379 */
+static double gR_deriv(int p, double x) {
+    double dPp = legendre_deriv(p, x), dPp1 = legendre_deriv(p + 1, x);
+    return 0.5 * (dPp + dPp1);
+}
+
+/* basis.cpp:464-613 */
+static void build_operators(orc_ctx* c) {
+    int p = c->P, n1 = c->n1, nsp = c->nsp;
+    double w[16];
+    gl_points(n1, c->pts, w);
+    const double* pts = c->pts;
+    for (int i = 0; i < n1; ++i)
+        for (int j = 0; j < n1; ++j) c->D1[i * n1 + j] = lag_deriv(pts, n1, j, pts[i]);
+    memset(c->dxi, 0, sizeof(double) * nsp * nsp);
+    memset(c->deta, 0, sizeof(double) * nsp * nsp);
+    for (int j = 0; j <= p; ++j)
+        for (int i = 0; i <= p; ++i) {
+            int row = j * n1 + i;
+            for (int k = 0; k <= p; ++k) {
+                c->dxi[row * nsp + j * n1 + k] = c->D1[i * n1 + k];
+                c->deta[row * nsp + k * n1 + i] = c->D1[j * n1 + k];
+            }
+        }
+    for (int e = 0; e < 4; ++e)
+        for (int fp = 0; fp < n1; ++fp) {
+            double s = pts[fp], xf, ef;
+            if (e == 0) { xf = s; ef = -1.0; }
+            else if (e == 1) { xf = 1.0; ef = s; }
+            else if (e == 2) { xf = -s; ef = 1.0; }
+            else { xf = -1.0; ef = -s; }
+            double Lx[16], Le[16];
+            for (int j = 0; j < n1; ++j) { Lx[j] = lag_eval(pts, n1, j, xf); Le[j] = lag_eval(pts, n1, j, ef); }
+            for (int j = 0; j <= p; ++j)
+                for (int i = 0; i <= p; ++i)
+                    c->interp[(e * n1 + fp) * nsp + j * n1 + i] = Lx[i] * Le[j];
+        }
+    for (int e = 0; e < 4; ++e)
+        for (int j = 0; j <= p; ++j)
+            for (int i = 0; i <= p; ++i) {
+                int sp = j * n1 + i;
+                double xi = pts[i], eta = pts[j], v;
+                if (e == 0) v = gL_deriv(p, eta) * lag_eval(pts, n1, i, xi);
+                else if (e == 2) v = gR_deriv(p, eta) * lag_eval(pts, n1, i, xi);
+                else if (e == 3) v = gL_deriv(p, xi) * lag_eval(pts, n1, j, eta);
+                else v = gR_deriv(p, xi) * lag_eval(pts, n1, j, eta);
+                c->corr[e * nsp + sp] = v;
+            }
+}
+
+/* ------------------------------------------------------------- geometry -- */
+
+static const int Q4_XI[25] = {0,4,4,0, 1,2,3, 4,4,4, 3,2,1, 0,0,0, 1,2,3,1,2,3,1,2,3};
+static const int Q4_ETA[25] = {0,0,4,4, 0,0,0, 1,2,3, 4,4,4, 3,2,1, 1,1,1,2,2,2,3,3,3};
+
+static void q4_lag(double t, double* L, double* dL) {
+    static const double nd[5] = {-1.0, -0.5, 0.0, 0.5, 1.0};
+    for (int i = 0; i < 5; ++i) {
+        L[i] = 1.0;
+        for (int j = 0; j < 5; ++j) if (j != i) L[i] *= (t - nd[j]) / (nd[i] - nd[j]);
+        dL[i] = 0.0;
+        for (int k = 0; k < 5; ++k) {
+            if (k == i) continue;
+            double pr = 1.0 / (nd[i] - nd[k]);
+            for (int j = 0; j < 5; ++j) if (j != i && j != k) pr *= (t - nd[j]) / (nd[i] - nd[j]);
+            dL[i] += pr;
+        }
+    }
+}
+
+/* basis.cpp:717-847: shape functions and derivatives of quads. */
+static int shape_quad(int order, double xi, double eta, double* N, double* dNx, double* dNe) {
+    if (order == 1) {
+        N[0] = 0.25 * (1 - xi) * (1 - eta); N[1] = 0.25 * (1 + xi) * (1 - eta);
+        N[2] = 0.25 * (1 + xi) * (1 + eta); N[3] = 0.25 * (1 - xi) * (1 + eta);
+        dNx[0] = -0.25 * (1 - eta); dNe[0] = -0.25 * (1 - xi);
+        dNx[1] = 0.25 * (1 - eta);  dNe[1] = -0.25 * (1 + xi);
+        dNx[2] = 0.25 * (1 + eta);  dNe[2] = 0.25 * (1 + xi);
+        dNx[3] = -0.25 * (1 + eta); dNe[3] = 0.25 * (1 - xi);
+        return 4;
+    }
+    if (order == 2) {
+        N[0] = 0.25 * xi * (xi - 1) * eta * (eta - 1);
+        N[1] = 0.25 * xi * (xi + 1) * eta * (eta - 1);
+        N[2] = 0.25 * xi * (xi + 1) * eta * (eta + 1);
+        N[3] = 0.25 * xi * (xi - 1) * eta * (eta + 1);
+        N[4] = 0.5 * (1 - xi * xi) * eta * (eta - 1);
+        N[5] = 0.5 * xi * (xi + 1) * (1 - eta * eta);
+        N[6] = 0.5 * (1 - xi * xi) * eta * (eta + 1);
+        N[7] = 0.5 * xi * (xi - 1) * (1 - eta * eta);
+        N[8] = (1 - xi * xi) * (1 - eta * eta);
+        dNx[0] = 0.25 * (2 * xi - 1) * eta * (eta - 1); dNe[0] = 0.25 * xi * (xi - 1) * (2 * eta - 1);
+        dNx[1] = 0.25 * (2 * xi + 1) * eta * (eta - 1); dNe[1] = 0.25 * xi * (xi + 1) * (2 * eta - 1);
+        dNx[2] = 0.25 * (2 * xi + 1) * eta * (eta + 1); dNe[2] = 0.25 * xi * (xi + 1) * (2 * eta + 1);
+        dNx[3] = 0.25 * (2 * xi - 1) * eta * (eta + 1); dNe[3] = 0.25 * xi * (xi - 1) * (2 * eta + 1);
+        dNx[4] = -xi * eta * (eta - 1);               dNe[4] = 0.5 * (1 - xi * xi) * (2 * eta - 1);
+        dNx[5] = 0.5 * (2 * xi + 1) * (1 - eta * eta); dNe[5] = -xi * (xi + 1) * eta;
+        dNx[6] = -xi * eta * (eta + 1);               dNe[6] = 0.5 * (1 - xi * xi) * (2 * eta + 1);
+        dNx[7] = 0.5 * (2 * xi - 1) * (1 - eta * eta); dNe[7] = -xi * (xi - 1) * eta;
+        dNx[8] = -2 * xi * (1 - eta * eta);            dNe[8] = -2 * eta * (1 - xi * xi);
+        return 9;
+    }
+    if (order == 4) {
+        double Lx[5], Le[5], dLx[5], dLe[5];
+        q4_lag(xi, Lx, dLx);
+        q4_lag(eta, Le, dLe);
+        for (int k = 0; k < 25; ++k) {
+            N[k] = Lx[Q4_XI[k]] * Le[Q4_ETA[k]];
+            dNx[k] = dLx[Q4_XI[k]] * Le[Q4_ETA[k]];
+            dNe[k] = Lx[Q4_XI[k]] * dLe[Q4_ETA[k]];
+        }
+        return 25;
+    }
+    return 0;
+}
+
+/* fr_solver.cpp:85-129 with basis.cpp:849-863 */
+static void build_geometry(orc_ctx* c) {
+    int nsp = c->nsp, n1 = c->n1;
+    for (int64_t e = 0; e < c->n_elem; ++e) {
+        const int64_t* nd = c->conn + e * c->nn;
+        for (int sp = 0; sp < nsp; ++sp) {
+            double xi = c->pts[sp % n1], eta = c->pts[sp / n1];
+            double N[25], dNx[25], dNe[25];
+            int n = shape_quad(c->eorder, xi, eta, N, dNx, dNe);
+            double dxdxi = 0.0, dxdeta = 0.0, dydxi = 0.0, dydeta = 0.0;
+            for (int i = 0; i < n; ++i) {
+                double x = c->xy[2 * nd[i]], y = c->xy[2 * nd[i] + 1];
+                dxdxi += dNx[i] * x; dxdeta += dNe[i] * x;
+                dydxi += dNx[i] * y; dydeta += dNe[i] * y;
+            }
+            double Jd = dxdxi * dydeta - dxdeta * dydxi;
+            double invJ = 1.0 / Jd;
+            c->J[e * nsp + sp] = Jd;
+            double* Ji = c->Jinv + (e * nsp + sp) * 4;
+            Ji[0] = dydeta * invJ; Ji[1] = -dxdeta * invJ;
+            Ji[2] = -dydxi * invJ; Ji[3] = dxdxi * invJ;
+        }
+        /* mesh.cpp:122-146 (quad split into two triangles) */
+        const double *p0 = c->xy + 2 * nd[0], *p1 = c->xy + 2 * nd[1];
+        const double *p2 = c->xy + 2 * nd[2], *p3 = c->xy + 2 * nd[3];
+        double a1 = 0.5 * fabs((p1[0] - p0[0]) * (p2[1] - p0[1]) - (p2[0] - p0[0]) * (p1[1] - p0[1]));
+        double a2 = 0.5 * fabs((p2[0] - p0[0]) * (p3[1] - p0[1]) - (p3[0] - p0[0]) * (p2[1] - p0[1]));
+        c->area[e] = a1 + a2;
+    }
+}
+
+/* ---------------------------------------------------------------- faces -- */
+
+typedef struct { int64_t a, b, seq; int e, l; } edge_ent;
+
+static int cmp_edge(const void* x, const void* y) {
+    const edge_ent *p = (const edge_ent*)x, *q = (const edge_ent*)y;
+    if (p->a != q->a) return p->a < q->a ? -1 : 1;
+    if (p->b != q->b) return p->b < q->b ? -1 : 1;
+    if (p->seq != q->seq) return p->seq < q->seq ? -1 : 1;
+    return 0;
+}
+
+/* mesh.cpp:159-183 */
+static void face_normal(const orc_ctx* c, int e, int lf, double* n) {
+    const int64_t* nd = c->conn + (int64_t)e * c->nn;
+    const double* v0 = c->xy + 2 * nd[lf];
+    const double* v1 = c->xy + 2 * nd[(lf + 1) % 4];
+    double tx = v1[0] - v0[0], ty = v1[1] - v0[1];
+    double len = sqrt(tx * tx + ty * ty);
+    double nx = ty / len, ny = -tx / len;
+    double cx = 0.0, cy = 0.0;
+    for (int i = 0; i < 4; ++i) { cx = cx + c->xy[2 * nd[i]]; cy = cy + c->xy[2 * nd[i] + 1]; }
+    cx = cx / 4.0; cy = cy / 4.0;
+    double fx = (v0[0] + v1[0]) * 0.5, fy = (v0[1] + v1[1]) * 0.5;
+    double dx = fx - cx, dy = fy - cy;
+    if (nx * dx + ny * dy < 0) { nx = nx * (-1.0); ny = ny * (-1.0); }
+    n[0] = nx; n[1] = ny;
+}
+
+static int build_faces(orc_ctx* c, int64_t n_bnd, const int64_t* bnd,
+                       int n_tags, const int* tag_ids, const int* tag_types,
+                       const double* tag_ps) {
+    int64_t ne = c->n_elem;
+    edge_ent* ent = (edge_ent*)malloc(sizeof(edge_ent) * (size_t)(ne * 4 + 1));
+    if (!ent) return -1;
+    for (int64_t e = 0; e < ne; ++e)
+        for (int l = 0; l < 4; ++l) {
+            int64_t v0 = c->conn[e * c->nn + l], v1 = c->conn[e * c->nn + (l + 1) % 4];
+            edge_ent* q = ent + e * 4 + l;
+            q->a = v0 < v1 ? v0 : v1; q->b = v0 < v1 ? v1 : v0;
+            q->seq = e * 4 + l; q->e = (int)e; q->l = l;
+        }
+    qsort(ent, (size_t)(ne * 4), sizeof(edge_ent), cmp_edge);
+    /* boundary-edge tag lookup: last definition of a vertex pair wins */
+    edge_ent* be = (edge_ent*)malloc(sizeof(edge_ent) * (size_t)(n_bnd + 1));
+    int64_t nbe = 0;
+    for (int64_t i = 0; i < n_bnd; ++i) {
+        int64_t v0 = bnd[3 * i], v1 = bnd[3 * i + 1];
+        int tag = (int)bnd[3 * i + 2];
+        if (tag <= 0) continue;
+        be[nbe].a = v0 < v1 ? v0 : v1; be[nbe].b = v0 < v1 ? v1 : v0;
+        be[nbe].seq = i; be[nbe].e = tag; be[nbe].l = 0; ++nbe;
+    }
+    qsort(be, (size_t)nbe, sizeof(edge_ent), cmp_edge);
+
+    int64_t cap = ne * 4, nf = 0, nbc = 0;
+    c->fle = (int*)malloc(sizeof(int) * cap); c->fll = (int*)malloc(sizeof(int) * cap);
+    c->fre = (int*)malloc(sizeof(int) * cap); c->frl = (int*)malloc(sizeof(int) * cap);
+    c->fbct = (int*)malloc(sizeof(int) * cap); c->ftag = (int*)malloc(sizeof(int) * cap);
+    c->fbcmap = (int*)malloc(sizeof(int) * cap);
+    c->fn = (double*)malloc(sizeof(double) * 2 * cap);
+    c->bc_data = (double*)calloc((size_t)(cap * 8 + 8), sizeof(double));
+    double c_inf = sqrt(c->gamma * c->p_inf / c->rho_inf);
+    (void)c_inf;
+    int64_t i = 0, jb = 0;
+    while (i < ne * 4) {
+        int64_t j = i;
+        while (j < ne * 4 && ent[j].a == ent[i].a && ent[j].b == ent[i].b) ++j;
+        int64_t cnt = j - i;
+        if (cnt == 1 || cnt == 2) {
+            int f = (int)nf++;
+            c->fle[f] = ent[i].e; c->fll[f] = ent[i].l;
+            if (cnt == 1) {
+                c->fre[f] = -1; c->frl[f] = -1;
+                c->fbct[f] = BC_FARFIELD; c->ftag[f] = 0;
+                /* mesh.cpp:48-57 default, then gmsh_reader.cpp:736-758 tagging */
+                while (jb < nbe && (be[jb].a < ent[i].a || (be[jb].a == ent[i].a && be[jb].b < ent[i].b))) ++jb;
+                int64_t k = jb, last = -1;
+                while (k < nbe && be[k].a == ent[i].a && be[k].b == ent[i].b) last = k++;
+                if (last >= 0) {
+                    int tag = be[last].e;
+                    c->ftag[f] = tag;
+                    for (int t = 0; t < n_tags; ++t)
+                        if (tag_ids[t] == tag) c->fbct[f] = tag_types[t];
+                }
+            } else {
+                c->fre[f] = ent[i + 1].e; c->frl[f] = ent[i + 1].l;
+                c->fbct[f] = BC_INTERIOR; c->ftag[f] = -1;
+            }
+            face_normal(c, c->fle[f], c->fll[f], c->fn + 2 * f);
+            /* fr_solver.cpp:432-482 BC packing, 8 values per boundary face */
+            if (cnt == 1) {
+                c->fbcmap[f] = (int)nbc;
+                double* d = c->bc_data + 8 * nbc;
+                if (c->fbct[f] == BC_FARFIELD) {
+                    d[0] = c->rho_inf; d[1] = c->u_inf; d[2] = c->v_inf; d[3] = c->p_inf;
+                } else if (c->fbct[f] == BC_OUTFLOW) {
+                    double ps = c->p_inf;
+                    for (int t = 0; t < n_tags; ++t)
+                        if (c->ftag[f] > 0 && tag_ids[t] == c->ftag[f] && tag_ps[t] > 0) ps = tag_ps[t];
+                    d[0] = ps;
+                }
+                ++nbc;
+            } else {
+                c->fbcmap[f] = -1;
+            }
+        }
+        i = j;
+    }
+    c->n_faces = nf;
+    free(ent);
+    free(be);
+    return 0;
+}
+
+/* ---------------------------------------------------------------- create -- */
+
+orc_ctx* orc_create(int P, double gamma, double rho_inf, double p_inf,
+                    double Mach, double AoA_deg,
+                    int64_t n_nodes, const double* xy,
+                    int64_t n_elem, int nn, int elem_order, const int64_t* conn,
+                    int64_t n_bnd, const int64_t* bnd,
+                    int n_tags, const int* tag_ids, const int* tag_types,
+                    const double* tag_pstatic) {
+    if (P < 0 || P > 8 || n_elem <= 0 || n_nodes <= 0) return NULL;
+    if (!((elem_order == 1 && nn == 4) || (elem_order == 2 && nn == 9) || (elem_order == 4 && nn == 25)))
+        return NULL;
+    orc_ctx* c = (orc_ctx*)calloc(1, sizeof(orc_ctx));
+    c->P = P; c->n1 = P + 1; c->nsp = (P + 1) * (P + 1); c->nfp = P + 1;
+    c->nn = nn; c->eorder = elem_order;
+    c->n_elem = n_elem; c->n_nodes = n_nodes;
+    c->gamma = gamma; c->rho_inf = rho_inf; c->p_inf = p_inf;
+    /* fr_solver.cpp:439-443 */
+    double c_inf = sqrt(gamma * p_inf / rho_inf);
+    double vel_inf = Mach * c_inf;
+    c->u_inf = vel_inf * cos(AoA_deg * M_PI / 180.0);
+    c->v_inf = vel_inf * sin(AoA_deg * M_PI / 180.0);
+    c->xy = (double*)malloc(sizeof(double) * 2 * n_nodes);
+    memcpy(c->xy, xy, sizeof(double) * 2 * n_nodes);
+    c->conn = (int64_t*)malloc(sizeof(int64_t) * n_elem * nn);
+    memcpy(c->conn, conn, sizeof(int64_t) * n_elem * nn);
+    for (int64_t k = 0; k < n_elem * nn; ++k)
+        if (conn[k] < 0 || conn[k] >= n_nodes) { orc_destroy(c); return NULL; }
+    int nsp = c->nsp, n1 = c->n1;
+    c->pts = (double*)malloc(sizeof(double) * n1);
+    c->D1 = (double*)malloc(sizeof(double) * n1 * n1);
+    c->dxi = (double*)malloc(sizeof(double) * nsp * nsp);
+    c->deta = (double*)malloc(sizeof(double) * nsp * nsp);
+    c->interp = (double*)malloc(sizeof(double) * 4 * n1 * nsp);
+    c->corr = (double*)malloc(sizeof(double) * 4 * nsp);
+    build_operators(c);
+    c->J = (double*)malloc(sizeof(double) * n_elem * nsp);
+    c->Jinv = (double*)malloc(sizeof(double) * n_elem * nsp * 4);
+    c->area = (double*)malloc(sizeof(double) * n_elem);
+    build_geometry(c);
+    if (build_faces(c, n_bnd, bnd, n_tags, tag_ids, tag_types, tag_pstatic) != 0) {
+        orc_destroy(c); return NULL;
+    }
+    size_t sol = (size_t)n_elem * nsp * 4, fpn = (size_t)n_elem * 4 * n1 * 4;
+    c->Fx = (double*)malloc(sizeof(double) * sol);
+    c->Fy = (double*)malloc(sizeof(double) * sol);
+    c->U0 = (double*)malloc(sizeof(double) * sol);
+    c->U1 = (double*)malloc(sizeof(double) * sol);
+    c->Ufp = (double*)malloc(sizeof(double) * fpn);
+    c->Fdiff = (double*)malloc(sizeof(double) * fpn);
+    c->Fcom = (double*)malloc(sizeof(double) * (size_t)(c->n_faces > 0 ? c->n_faces : 1) * n1 * 4);
+    c->nthreads = 1;
+    return c;
+}
+
+void orc_destroy(orc_ctx* c) {
+    if (!c) return;
+    void* ps[] = {c->xy, c->conn, c->J, c->Jinv, c->area, c->fle, c->fll, c->fre, c->frl,
+                  c->fbct, c->ftag, c->fbcmap, c->fn, c->bc_data, c->pts, c->D1, c->dxi,
+                  c->deta, c->interp, c->corr, c->Fx, c->Fy, c->Ufp, c->Fcom, c->Fdiff,
+                  c->U0, c->U1};
+    for (size_t i = 0; i < sizeof(ps) / sizeof(ps[0]); ++i) free(ps[i]);
+    free(c);
+}
+
+void orc_set_threads(orc_ctx* c, int n) { c->nthreads = n > 0 ? n : 1; }
+int64_t orc_num_faces(const orc_ctx* c) { return c->n_faces; }
+int orc_num_sp(const orc_ctx* c) { return c->nsp; }
+
+void orc_faces(const orc_ctx* c, int* le, int* ll, int* re, int* rl, int* bct, int* tag, double* n) {
+    size_t nf = (size_t)c->n_faces;
+    memcpy(le, c->fle, nf * sizeof(int)); memcpy(ll, c->fll, nf * sizeof(int));
+    memcpy(re, c->fre, nf * sizeof(int)); memcpy(rl, c->frl, nf * sizeof(int));
+    memcpy(bct, c->fbct, nf * sizeof(int)); memcpy(tag, c->ftag, nf * sizeof(int));
+    memcpy(n, c->fn, nf * 2 * sizeof(double));
+}
+
+void orc_geometry(const orc_ctx* c, double* J, double* Jinv) {
+    memcpy(J, c->J, sizeof(double) * c->n_elem * c->nsp);
+    memcpy(Jinv, c->Jinv, sizeof(double) * c->n_elem * c->nsp * 4);
+}
+
+void orc_operators(const orc_ctx* c, double* pts, double* D1, double* dxi, double* deta,
+                   double* interp, double* corr) {
+    int n1 = c->n1, nsp = c->nsp;
+    memcpy(pts, c->pts, sizeof(double) * n1);
+    memcpy(D1, c->D1, sizeof(double) * n1 * n1);
+    memcpy(dxi, c->dxi, sizeof(double) * nsp * nsp);
+    memcpy(deta, c->deta, sizeof(double) * nsp * nsp);
+    memcpy(interp, c->interp, sizeof(double) * 4 * n1 * nsp);
+    memcpy(corr, c->corr, sizeof(double) * 4 * nsp);
+}
+
+/* fr_solver.cpp:268-299 with basis.cpp:882-893 */
+void orc_sp_coords(const orc_ctx* c, double* out) {
+    int nsp = c->nsp, n1 = c->n1;
+    for (int64_t e = 0; e < c->n_elem; ++e) {
+        const int64_t* nd = c->conn + e * c->nn;
+        for (int sp = 0; sp < nsp; ++sp) {
+            double N[25], dNx[25], dNe[25];
+            int n = shape_quad(c->eorder, c->pts[sp % n1], c->pts[sp / n1], N, dNx, dNe);
+            double x = 0.0, y = 0.0;
+            for (int i = 0; i < n; ++i) { x += N[i] * c->xy[2 * nd[i]]; y += N[i] * c->xy[2 * nd[i] + 1]; }
+            out[(e * nsp + sp) * 2] = x;
+            out[(e * nsp + sp) * 2 + 1] = y;
+        }
+    }
+}
+
+/* --------------------------------------------------------------- physics -- */
+
+/* euler.hpp:16-23 */
+static double pressure(const double* U, double g) {
+    double rho = U[0], u = U[1] / rho, v = U[2] / rho, E = U[3] / rho;
+    double ke = 0.5 * (u * u + v * v);
+    return (g - 1.0) * rho * (E - ke);
+}
+
+/* euler.hpp:101-129 */
+static void flux_xy(const double* U, double g, double* F, double* G) {
+    double rho = U[0], u = U[1] / rho, v = U[2] / rho, p = pressure(U, g);
+    F[0] = U[1]; F[1] = U[1] * u + p; F[2] = U[1] * v; F[3] = (U[3] + p) * u;
+    G[0] = U[2]; G[1] = U[2] * u; G[2] = U[2] * v + p; G[3] = (U[3] + p) * v;
+}
+
+/* euler.hpp:81-88 */
+static void prim2cons(double rho, double u, double v, double p, double g, double* U) {
+    U[0] = rho; U[1] = rho * u; U[2] = rho * v;
+    U[3] = p / (g - 1.0) + 0.5 * rho * (u * u + v * v);
+}
+
+/* kernels.cu:453-525 */
+static void ghost_state(const double* Ui, double nx, double ny, int bct,
+                        const double* bcd, int bci, double g, double* Ug) {
+    switch (bct) {
+    case BC_WALL: case BC_SLIPWALL: case BC_SYMMETRY: {
+        double rho = Ui[0], u = Ui[1] / rho, v = Ui[2] / rho;
+        double p = pressure(Ui, g);
+        double vn = u * nx + v * ny;
+        prim2cons(rho, u - 2.0 * vn * nx, v - 2.0 * vn * ny, p, g, Ug);
+        break;
+    }
+    case BC_FARFIELD: {
+        const double* d = bcd + bci * 8;
+        double rho_inf = d[0], u_inf = d[1], v_inf = d[2], p_inf = d[3];
+        double rho_i = fmax(Ui[0], 1e-10);
+        double u_i = Ui[1] / rho_i, v_i = Ui[2] / rho_i;
+        double p_i = fmax((g - 1.0) * (Ui[3] - 0.5 * rho_i * (u_i * u_i + v_i * v_i)), 1e-10);
+        double vn_inf = u_inf * nx + v_inf * ny;
+        double rb, ub, vb, pb;
+        if (vn_inf > 0) { rb = rho_inf; ub = u_inf; vb = v_inf; pb = 0.5 * (p_inf + p_i); }
+        else { rb = rho_i; ub = u_i; vb = v_i; pb = 0.5 * (p_inf + p_i); }
+        rb = fmax(fmin(rb, 100.0), 0.01);
+        ub = fmax(fmin(ub, 1000.0), -1000.0);
+        vb = fmax(fmin(vb, 1000.0), -1000.0);
+        pb = fmax(fmin(pb, 1e7), 1e3);
+        prim2cons(rb, ub, vb, pb, g, Ug);
+        break;
+    }
+    case BC_OUTFLOW: {
+        double rho = Ui[0], u = Ui[1] / rho, v = Ui[2] / rho;
+        prim2cons(rho, u, v, bcd[bci * 8], g, Ug);
+        break;
+    }
+    default:
+        Ug[0] = Ui[0]; Ug[1] = Ui[1]; Ug[2] = Ui[2]; Ug[3] = Ui[3];
+    }
+}
+
+/* kernels.cu:597-669 (hard-coded Rusanov with floors; NaN/Inf -> 0) */
+static void rusanov_compat(const double* UL, const double* UR, double nx, double ny,
+                           double g, double* F) {
+    double rhoL = fmax(UL[0], 1e-10), rhoR = fmax(UR[0], 1e-10);
+    double uL = UL[1] / rhoL, vL = UL[2] / rhoL, uR = UR[1] / rhoR, vR = UR[2] / rhoR;
+    double EL = UL[3] / rhoL, ER = UR[3] / rhoR;
+    double pL = fmax((g - 1.0) * rhoL * (EL - 0.5 * (uL * uL + vL * vL)), 1e-10);
+    double pR = fmax((g - 1.0) * rhoR * (ER - 0.5 * (uR * uR + vR * vR)), 1e-10);
+    double cL = sqrt(fmax(g * pL / rhoL, 1e-10)), cR = sqrt(fmax(g * pR / rhoR, 1e-10));
+    double vnL = uL * nx + vL * ny, vnR = uR * nx + vR * ny;
+    double velL = sqrt(uL * uL + vL * vL), velR = sqrt(uR * uR + vR * vR);
+    double smax = fmax(velL + cL, velR + cR);
+    double HL = EL + pL / rhoL, HR = ER + pR / rhoR;
+    double FL[4] = {rhoL * vnL, rhoL * uL * vnL + pL * nx, rhoL * vL * vnL + pL * ny, rhoL * HL * vnL};
+    double FR[4] = {rhoR * vnR, rhoR * uR * vnR + pR * nx, rhoR * vR * vnR + pR * ny, rhoR * HR * vnR};
+    for (int v = 0; v < 4; ++v) {
+        F[v] = 0.5 * (FL[v] + FR[v]) - 0.5 * smax * (UR[v] - UL[v]);
+        if (isnan(F[v]) || isinf(F[v])) F[v] = 0.0;
+    }
+}
+
+/* ------------------------------------------------------------------- RHS -- */
+
+void orc_rhs(orc_ctx* c, const double* U, double* R) {
+    const int nsp = c->nsp, n1 = c->n1, nfp = c->nfp;
+    const int64_t ne = c->n_elem, nf = c->n_faces;
+    const double g = c->gamma;
+    int nt = c->nthreads;
+    (void)nt;
+    /* K4 kernels.cu:157-194 */
+#pragma omp parallel for num_threads(nt) schedule(static)
+    for (int64_t idx = 0; idx < ne * nsp; ++idx)
+        flux_xy(U + idx * 4, g, c->Fx + idx * 4, c->Fy + idx * 4);
+    /* K1 kernels.cu:30-67 */
+#pragma omp parallel for num_threads(nt) schedule(static)
+    for (int64_t e = 0; e < ne; ++e)
+        for (int t = 0; t < 4 * nfp; ++t) {
+            int edge = t / nfp, fp = t % nfp;
+            for (int v = 0; v < 4; ++v) {
+                double val = 0.0;
+                for (int sp = 0; sp < nsp; ++sp)
+                    val += c->interp[edge * nfp * nsp + fp * nsp + sp] * U[e * nsp * 4 + sp * 4 + v];
+                c->Ufp[(e * 4 + edge) * nfp * 4 + fp * 4 + v] = val;
+            }
+        }
+    memset(c->Fdiff, 0, sizeof(double) * (size_t)ne * 4 * nfp * 4);
+    /* K10 kernels.cu:528-701 then K8 kernels.cu:346-450 */
+#pragma omp parallel for num_threads(nt) schedule(static)
+    for (int64_t f = 0; f < nf; ++f) {
+        int le = c->fle[f], ll = c->fll[f], re = c->fre[f], rl = c->frl[f];
+        double nx = c->fn[2 * f], ny = c->fn[2 * f + 1];
+        for (int fp = 0; fp < nfp; ++fp) {
+            const double* UL = c->Ufp + ((int64_t)le * 4 + ll) * nfp * 4 + fp * 4;
+            double UR[4];
+            if (re >= 0) {
+                const double* q = c->Ufp + ((int64_t)re * 4 + rl) * nfp * 4 + (nfp - 1 - fp) * 4;
+                UR[0] = q[0]; UR[1] = q[1]; UR[2] = q[2]; UR[3] = q[3];
+            } else {
+                int bct = c->fbct[f], bci = c->fbcmap[f];
+                if (bci < 0) { bct = BC_SLIPWALL; bci = 0; }
+                ghost_state(UL, nx, ny, bct, c->bc_data, bci, g, UR);
+            }
+            rusanov_compat(UL, UR, nx, ny, g, c->Fcom + (f * nfp + fp) * 4);
+        }
+    }
+#pragma omp parallel for num_threads(nt) schedule(static)
+    for (int64_t f = 0; f < nf; ++f) {
+        int le = c->fle[f], ll = c->fll[f], re = c->fre[f], rl = c->frl[f];
+        double nx = c->fn[2 * f], ny = c->fn[2 * f + 1];
+        for (int fp = 0; fp < nfp; ++fp) {
+            const double* Fc = c->Fcom + (f * nfp + fp) * 4;
+            int64_t lo = ((int64_t)le * 4 + ll) * nfp * 4 + fp * 4;
+            double Fx[4], Fy[4];
+            flux_xy(c->Ufp + lo, g, Fx, Fy);
+            for (int v = 0; v < 4; ++v) c->Fdiff[lo + v] = Fc[v] - (Fx[v] * nx + Fy[v] * ny);
+            if (re >= 0) {
+                int64_t ro = ((int64_t)re * 4 + rl) * nfp * 4 + fp * 4;
+                flux_xy(c->Ufp + ro, g, Fx, Fy);
+                for (int v = 0; v < 4; ++v) c->Fdiff[ro + v] = -Fc[v] + (Fx[v] * nx + Fy[v] * ny);
+            }
+        }
+    }
+    /* K13 kernels.cu:813-872 then K15 kernels.cu:948-1034 */
+#pragma omp parallel for num_threads(nt) schedule(static)
+    for (int64_t e = 0; e < ne; ++e)
+        for (int sp = 0; sp < nsp; ++sp) {
+            const double* Ji = c->Jinv + (e * nsp + sp) * 4;
+            int si = sp / n1, sj = sp % n1;
+            for (int v = 0; v < 4; ++v) {
+                double a = 0.0, b = 0.0, cc = 0.0, d = 0.0;
+                for (int k = 0; k < nsp; ++k) {
+                    double fx = c->Fx[e * nsp * 4 + k * 4 + v], fy = c->Fy[e * nsp * 4 + k * 4 + v];
+                    a += c->dxi[sp * nsp + k] * fx;
+                    b += c->deta[sp * nsp + k] * fx;
+                    cc += c->dxi[sp * nsp + k] * fy;
+                    d += c->deta[sp * nsp + k] * fy;
+                }
+                double div = (a * Ji[0] + b * Ji[2]) + (cc * Ji[1] + d * Ji[3]);
+                double r = -div;
+                const double* Fd = c->Fdiff + e * 4 * nfp * 4;
+                double corr = 0.0;
+                corr += Fd[(0 * nfp + sj) * 4 + v] * c->corr[0 * nsp + sp];
+                corr += Fd[(1 * nfp + si) * 4 + v] * c->corr[1 * nsp + sp];
+                corr += Fd[(2 * nfp + sj) * 4 + v] * c->corr[2 * nsp + sp];
+                corr += Fd[(3 * nfp + si) * 4 + v] * c->corr[3 * nsp + sp];
+                r -= corr;
+                R[e * nsp * 4 + sp * 4 + v] = r;
+            }
+        }
+}
+
+/* ------------------------------------------------------------ RK + clamp -- */
+
+/* kernels.cu:1236-1288 */
+static void positivity(double* U) {
+    const double RHO_MIN = 0.01, RHO_MAX = 100.0, P_MIN = 100.0, P_MAX = 1e8;
+    const double VEL_MAX = 2000.0, GPP = 1.4;
+    double rho = U[0], rhou = U[1], rhov = U[2], rhoE = U[3];
+    double rn = fmax(RHO_MIN, fmin(RHO_MAX, rho));
+    double u = rhou / fmax(rn, 1e-10), v = rhov / fmax(rn, 1e-10);
+    double vm = sqrt(u * u + v * v);
+    if (vm > VEL_MAX) { double s = VEL_MAX / vm; u *= s; v *= s; }
+    double ke = 0.5 * rn * (u * u + v * v);
+    double p = (GPP - 1.0) * (rhoE - ke);
+    p = fmax(P_MIN, fmin(P_MAX, p));
+    double E = p / (GPP - 1.0) + ke;
+    U[0] = rn; U[1] = rn * u; U[2] = rn * v; U[3] = E;
+}
+
+/* fr_solver.cpp:305-333 with kernels.cu:1297-1349 */
+void orc_step(orc_ctx* c, double* U, double dt, int nsteps, double* R_last) {
+    int64_t n = c->n_elem * c->nsp * 4, ns = c->n_elem * c->nsp;
+    double* R = (double*)malloc(sizeof(double) * (size_t)n);
+    int nt = c->nthreads;
+    (void)nt;
+    for (int s = 0; s < nsteps; ++s) {
+        memcpy(c->U0, U, sizeof(double) * (size_t)n);
+        orc_rhs(c, U, R);
+#pragma omp parallel for num_threads(nt) schedule(static)
+        for (int64_t i = 0; i < n; ++i) U[i] = c->U0[i] + dt * R[i];
+#pragma omp parallel for num_threads(nt) schedule(static)
+        for (int64_t i = 0; i < ns; ++i) positivity(U + 4 * i);
+        memcpy(c->U1, U, sizeof(double) * (size_t)n);
+        orc_rhs(c, U, R);
+#pragma omp parallel for num_threads(nt) schedule(static)
+        for (int64_t i = 0; i < n; ++i) U[i] = 0.75 * c->U0[i] + 0.25 * c->U1[i] + 0.25 * dt * R[i];
+#pragma omp parallel for num_threads(nt) schedule(static)
+        for (int64_t i = 0; i < ns; ++i) positivity(U + 4 * i);
+        orc_rhs(c, U, R);
+#pragma omp parallel for num_threads(nt) schedule(static)
+        for (int64_t i = 0; i < n; ++i)
+            U[i] = (1.0 / 3.0) * c->U0[i] + (2.0 / 3.0) * U[i] + (2.0 / 3.0) * dt * R[i];
+#pragma omp parallel for num_threads(nt) schedule(static)
+        for (int64_t i = 0; i < ns; ++i) positivity(U + 4 * i);
+    }
+    if (R_last) memcpy(R_last, R, sizeof(double) * (size_t)n);
+    free(R);
+}
+
+/* fr_solver.cpp:784-816 with euler.hpp:34-41,166-171 */
+double orc_compute_dt(const orc_ctx* c, const double* U, double CFL) {
+    double dt_min = 1e20;
+    double cfl_factor = 2.0 * c->P + 1.0;
+    for (int64_t e = 0; e < c->n_elem; ++e) {
+        double h = sqrt(c->area[e]);
+        for (int sp = 0; sp < c->nsp; ++sp) {
+            const double* s = U + (e * c->nsp + sp) * 4;
+            double u = s[1] / s[0], v = s[2] / s[0];
+            double vel = sqrt(u * u + v * v);
+            double p = fmax(pressure(s, c->gamma), 1e-10), rho = fmax(s[0], 1e-10);
+            double ws = vel + sqrt(c->gamma * p / rho);
+            double dl = CFL * h / (ws * cfl_factor);
+            if (dl < dt_min) dt_min = dl;
+        }
+    }
+    return dt_min;
+}
+
+double orc_l2(const double* R, int64_t n) {
+    double s = 0.0;
+    for (int64_t i = 0; i < n; ++i) s += R[i] * R[i];
+    return sqrt(s);
+}

@@ -1,0 +1,274 @@
+// ref_harness.cpp -- TEST INFRASTRUCTURE: drives the reference's own code.
+//
+// Built by oracle/ref/Makefile from the reference sources where they lie
+// (nothing is copied); output binaries go to oracle/_ref/.  Two builds:
+//   ref_cpu : basis.cpp + mesh.cpp + gmsh_reader.cpp, runs on any host.
+//             "ops P out"            -> FROperators (basis.cpp:464-613)
+//             "mesh mesh.bin P out"  -> faces, normals (mesh.cpp:18-194) and
+//                                       J/Jinv exactly as fr_solver.cpp:85-129
+//             "gmsh file.msh out"    -> GmshReader::read (gmsh_reader.cpp:161)
+//   ref_gpu : + kernels.cu + fr_solver.cpp, needs a GPU.
+//             "rhs mesh.bin params state out"           -> computeResidual_GPU
+//             "step mesh.bin params state dt n out"     -> n x advance(dt)
+// Files are raw little-endian arrays; layouts are written by
+// oracle/oracle.py (write_mesh_bin) and read back by it.
+#include <cstdint>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <fstream>
+#include <functional>
+#include <iostream>
+#include <map>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "common/types.hpp"
+#include "mesh/mesh.hpp"
+#include "basis/basis.hpp"
+
+#ifdef ZJ_REF_GPU
+#include <cuda_runtime.h>
+#define private public
+#define protected public
+#include "solver/fr_solver.hpp"
+#undef private
+#undef protected
+#endif
+
+using namespace zhijian;
+
+namespace {
+
+struct Reader {
+    std::ifstream f;
+    explicit Reader(const char* p) : f(p, std::ios::binary) {
+        if (!f) { std::fprintf(stderr, "cannot open %s\n", p); std::exit(2); }
+    }
+    template <class T> T get() { T v; f.read(reinterpret_cast<char*>(&v), sizeof(T)); return v; }
+    template <class T> void arr(std::vector<T>& v, size_t n) {
+        v.resize(n);
+        f.read(reinterpret_cast<char*>(v.data()), n * sizeof(T));
+    }
+};
+
+struct Writer {
+    std::ofstream f;
+    explicit Writer(const char* p) : f(p, std::ios::binary) {}
+    template <class T> void put(T v) { f.write(reinterpret_cast<const char*>(&v), sizeof(T)); }
+    template <class T> void arr(const std::vector<T>& v) {
+        f.write(reinterpret_cast<const char*>(v.data()), v.size() * sizeof(T));
+    }
+};
+
+// Mesh file: int64 n_nodes, f64 xy[n][2], int64 n_elem, int32 nn, int32 order,
+// int64 conn[E][nn], int64 n_bnd, int64 bnd[n][3], int32 n_tags,
+// n_tags x (int32 id, int32 type, f64 p_static)
+void load_mesh(const char* path, Mesh& mesh) {
+    Reader r(path);
+    int64_t nn_nodes = r.get<int64_t>();
+    std::vector<double> xy; r.arr(xy, 2 * nn_nodes);
+    for (int64_t i = 0; i < nn_nodes; ++i) mesh.nodes().push_back(Vec2(xy[2 * i], xy[2 * i + 1]));
+    int64_t ne = r.get<int64_t>();
+    int32_t nn = r.get<int32_t>(), order = r.get<int32_t>();
+    std::vector<int64_t> conn; r.arr(conn, ne * nn);
+    for (int64_t e = 0; e < ne; ++e) {
+        Element el;
+        el.type = ElementType::Quadrilateral;
+        el.order = order;
+        el.partition = 0;
+        for (int k = 0; k < nn; ++k) el.node_ids.push_back(conn[e * nn + k]);
+        mesh.elements().push_back(el);
+    }
+    int64_t nb = r.get<int64_t>();
+    std::vector<int64_t> bnd; r.arr(bnd, 3 * nb);
+    int32_t nt = r.get<int32_t>();
+    for (int t = 0; t < nt; ++t) {
+        int32_t id = r.get<int32_t>(), ty = r.get<int32_t>();
+        double ps = r.get<double>();
+        BCInfo info;
+        info.tag = id; info.type = static_cast<BCType>(ty); info.name = "tag";
+        info.p_total = 0; info.T_total = 0; info.flow_direction = Vec2(1, 0);
+        info.p_static = ps; info.T_wall = 0;
+        mesh.addBCInfo(id, info);
+    }
+    mesh.buildFaces();
+    // gmsh_reader.cpp:720-758: vertex pair -> tag (last wins), then stamp.
+    std::map<std::pair<Index, Index>, int> tags;
+    for (int64_t i = 0; i < nb; ++i) {
+        Index a = bnd[3 * i], b = bnd[3 * i + 1];
+        int tag = static_cast<int>(bnd[3 * i + 2]);
+        if (tag <= 0) continue;
+        if (a > b) std::swap(a, b);
+        tags[{a, b}] = tag;
+    }
+    for (Index f = 0; f < mesh.numFaces(); ++f) {
+        Face& face = mesh.face(f);
+        if (!face.is_boundary) continue;
+        const Element& el = mesh.element(face.left_elem);
+        Index a = el.node_ids[face.left_face % 4], b = el.node_ids[(face.left_face + 1) % 4];
+        if (a > b) std::swap(a, b);
+        auto it = tags.find({a, b});
+        if (it != tags.end()) {
+            face.bc_tag = it->second;
+            if (mesh.hasBCInfo(it->second)) face.bc_type = mesh.getBCInfo(it->second).type;
+        }
+    }
+    mesh.computeGeometry();
+}
+
+int cmd_ops(int P, const char* out) {
+    FROperators ops;
+    ops.init(ElementType::Quadrilateral, P, FluxType::HU);
+    int nsp = ops.numSolutionPoints(), n1 = P + 1;
+    std::vector<double> pts, w;
+    GaussLegendre::getQuadrature(n1, pts, w);
+    std::vector<std::vector<double>> D;
+    Lagrange1D::buildDiffMatrix(pts, D);
+    Writer wr(out);
+    wr.arr(pts);
+    for (auto& row : D) wr.arr(row);
+    for (int i = 0; i < nsp; ++i) wr.arr(ops.diffXi()[i]);
+    for (int i = 0; i < nsp; ++i) wr.arr(ops.diffEta()[i]);
+    for (int e = 0; e < 4; ++e)
+        for (int fp = 0; fp < n1; ++fp) wr.arr(ops.interpToFlux(e)[fp]);
+    for (int e = 0; e < 4; ++e) wr.arr(ops.correctionDeriv()[e]);
+    return 0;
+}
+
+int cmd_mesh(const char* mpath, int P, const char* out) {
+    Mesh mesh;
+    load_mesh(mpath, mesh);
+    FROperators ops;
+    ops.init(ElementType::Quadrilateral, P, FluxType::HU);
+    Writer wr(out);
+    int64_t nf = mesh.numFaces();
+    wr.put(nf);
+    for (int64_t f = 0; f < nf; ++f) {
+        const Face& fc = mesh.face(f);
+        Vec2 n = mesh.faceNormal(f);
+        wr.put<int32_t>(fc.left_elem); wr.put<int32_t>(fc.left_face);
+        wr.put<int32_t>(fc.right_elem); wr.put<int32_t>(fc.right_face);
+        wr.put<int32_t>(static_cast<int32_t>(fc.bc_type)); wr.put<int32_t>(fc.bc_tag);
+        wr.put(n.x); wr.put(n.y);
+    }
+    // fr_solver.cpp:85-129, restated around ElementGeometry::jacobian
+    std::vector<double> J, Jinv, sxy;
+    for (Index i = 0; i < mesh.numElements(); ++i) {
+        const Element& el = mesh.element(i);
+        std::vector<Vec2> nodes;
+        for (Index id : el.node_ids) nodes.push_back(mesh.node(id));
+        for (int sp = 0; sp < ops.numSolutionPoints(); ++sp) {
+            Real xi = ops.solutionXi()[sp], eta = ops.solutionEta()[sp];
+            Real a, b, c, d;
+            ElementGeometry::jacobian(nodes, el.type, el.order, xi, eta, a, b, c, d);
+            Real Jd = a * d - b * c;
+            J.push_back(Jd);
+            Real invJ = 1.0 / Jd;
+            Jinv.push_back(d * invJ); Jinv.push_back(-b * invJ);
+            Jinv.push_back(-c * invJ); Jinv.push_back(a * invJ);
+            Vec2 p = ElementGeometry::refToPhys(nodes, el.type, el.order, xi, eta);
+            sxy.push_back(p.x); sxy.push_back(p.y);
+        }
+    }
+    wr.arr(J); wr.arr(Jinv); wr.arr(sxy);
+    std::vector<double> area;
+    for (Index i = 0; i < mesh.numElements(); ++i) area.push_back(mesh.elementArea(i));
+    wr.arr(area);
+    return 0;
+}
+
+int cmd_gmsh(const char* path, const char* out) {
+    Mesh mesh;
+    GmshReader rd;
+    if (!rd.read(path, mesh)) { std::fprintf(stderr, "%s\n", rd.errorMessage().c_str()); return 3; }
+    Writer wr(out);
+    wr.put<int64_t>(mesh.numNodes());
+    for (auto& n : mesh.nodes()) { wr.put(n.x); wr.put(n.y); }
+    wr.put<int64_t>(mesh.numElements());
+    for (auto& e : mesh.elements()) {
+        wr.put<int32_t>(static_cast<int32_t>(e.type)); wr.put<int32_t>(e.order);
+        wr.put<int32_t>(static_cast<int32_t>(e.node_ids.size()));
+        for (Index id : e.node_ids) wr.put<int64_t>(id);
+    }
+    wr.put<int64_t>(mesh.numFaces());
+    for (Index f = 0; f < mesh.numFaces(); ++f) {
+        const Face& fc = mesh.face(f);
+        wr.put<int32_t>(fc.left_elem); wr.put<int32_t>(fc.left_face);
+        wr.put<int32_t>(fc.right_elem); wr.put<int32_t>(fc.right_face);
+        wr.put<int32_t>(static_cast<int32_t>(fc.bc_type)); wr.put<int32_t>(fc.bc_tag);
+    }
+    wr.put<int32_t>(static_cast<int32_t>(mesh.allBCInfo().size()));
+    for (auto& kv : mesh.allBCInfo()) {
+        wr.put<int32_t>(kv.first); wr.put<int32_t>(static_cast<int32_t>(kv.second.type));
+    }
+    return 0;
+}
+
+#ifdef ZJ_REF_GPU
+// params: "P gamma rho_inf p_inf Mach AoA"
+SimParams make_params(char** a) {
+    SimParams p;
+    p.poly_order = std::atoi(a[0]);
+    p.gamma = std::atof(a[1]); p.rho_inf = std::atof(a[2]); p.p_inf = std::atof(a[3]);
+    p.Mach_inf = std::atof(a[4]); p.AoA = std::atof(a[5]);
+    p.riemann = RiemannSolver::Rusanov; p.flux_type = FluxType::HU; p.viscous = false;
+    return p;
+}
+
+void put_state(FRSolver& s, const std::vector<double>& U) {
+    size_t idx = 0;
+    for (auto& es : s.solution_)
+        for (auto& st : es.sol_pts)
+            for (int v = 0; v < 4; ++v) st[v] = U[idx++];
+    s.copyToDevice();
+}
+
+int cmd_gpu(int argc, char** argv) {
+    std::string cmd = argv[1];
+    Mesh mesh;
+    load_mesh(argv[2], mesh);
+    SimParams p = make_params(argv + 3);
+    FRSolver s;
+    s.initialize(mesh, p);
+    size_t n = static_cast<size_t>(mesh.numElements()) * (p.poly_order + 1) * (p.poly_order + 1) * 4;
+    Reader r(argv[9]);
+    std::vector<double> U; r.arr(U, n);
+    put_state(s, U);
+    std::vector<double> out(n);
+    if (cmd == "rhs") {
+        s.computeResidual_GPU();
+        cudaDeviceSynchronize();
+        s.gpu_data_->dUdt.copyToHost(out.data(), n);
+        Writer(argv[10]).arr(out);
+    } else {
+        double dt = std::atof(argv[10]);
+        int ns = std::atoi(argv[11]);
+        for (int k = 0; k < ns; ++k) s.advance(dt);
+        s.gpu_data_->U.copyToHost(out.data(), n);
+        Writer w(argv[12]);
+        w.arr(out);
+        s.gpu_data_->dUdt.copyToHost(out.data(), n);
+        w.arr(out);
+        double res = s.computeResidual();
+        w.put(res);
+    }
+    return 0;
+}
+#endif
+
+}  // namespace
+
+int main(int argc, char** argv) {
+    if (argc < 2) { std::fprintf(stderr, "usage: see header\n"); return 1; }
+    std::string cmd = argv[1];
+    if (cmd == "ops" && argc == 4) return cmd_ops(std::atoi(argv[2]), argv[3]);
+    if (cmd == "mesh" && argc == 5) return cmd_mesh(argv[2], std::atoi(argv[3]), argv[4]);
+    if (cmd == "gmsh" && argc == 4) return cmd_gmsh(argv[2], argv[3]);
+#ifdef ZJ_REF_GPU
+    if ((cmd == "rhs" && argc == 11) || (cmd == "step" && argc == 13)) return cmd_gpu(argc, argv);
+#endif
+    std::fprintf(stderr, "bad command\n");
+    return 1;
+}

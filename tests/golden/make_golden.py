@@ -1,0 +1,150 @@
+"""Generates the golden fixtures of tests/golden/ from the reference's own code.
+
+    python tests/golden/make_golden.py cpu  [--out DIR]   # any host
+    python tests/golden/make_golden.py gpu  [--out DIR]   # on a GPU host
+
+"cpu" runs oracle/_ref/ref_cpu (the reference's basis.cpp, mesh.cpp and
+gmsh_reader.cpp compiled from the reference sources by oracle/ref/Makefile) and
+stores its operators, faces, normals and metric terms.  "gpu" runs
+oracle/_ref/ref_gpu (the reference's kernels.cu and fr_solver.cpp) on the cases
+of GPU_CASES and stores the reference's own residuals and stepped states.
+Inputs are seeded (SplitMix64), so every case is regenerated from its recipe.
+"""
+from __future__ import annotations
+
+import argparse
+import math
+import os
+import subprocess
+import sys
+import tempfile
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+sys.path.insert(0, ROOT)
+
+from oracle import oracle as O  # noqa: E402
+from zhijian_b200 import meshgen as M  # noqa: E402
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+GAMMA = 1.4
+# the dimensional twin of the vortex: every reference clamp stays inactive
+RHO_S, P_S = 1.225, 101325.0 * 1.4
+
+
+def mixed_mesh(n=6, seed=7):
+    """Jittered n x n quads, one boundary type per side."""
+    return M.structured_quads(n, n, 0.0, 1.0, 0.0, 1.0, 0.15, seed, (1, 2, 3, 4),
+                              {1: "slipwall", 2: "outflow", 3: "farfield", 4: "wall"})
+
+
+def mixed_tags(p_out):
+    return [(1, O.BC_TYPES["slipwall"], 0.0), (2, O.BC_TYPES["outflow"], p_out),
+            (3, O.BC_TYPES["farfield"], 0.0), (4, O.BC_TYPES["wall"], 0.0)]
+
+
+def case_defs():
+    """name -> dict(mesh, tags, P, params(rho,p,Mach,AoA), state, [dt, nsteps])."""
+    cases = {}
+    vm = M.vortex_mesh(20)
+    # raw non-dimensional vortex (the reference clamps fire)
+    cases["vortex_raw_p3"] = dict(mesh=vm, tags=None, P=3, prm=(1.0, 1.0 / GAMMA, 0.5, 0.0),
+                                  state=("vortex", 1.0, 1.0), dt=0.01, nsteps=3)
+    cases["vortex_dim_p3"] = dict(mesh=vm, tags=None, P=3,
+                                  prm=(RHO_S, P_S / GAMMA, 0.5, 0.0),
+                                  state=("vortex", RHO_S, P_S), dt=1e-4, nsteps=5)
+    for P in range(1, 6):
+        cases[f"mixed_p{P}"] = dict(mesh=mixed_mesh(), tags=mixed_tags(0.9e5), P=P,
+                                    prm=(1.2, 1.0e5, 0.4, 10.0),
+                                    state=("random", 1.2, 1.0e5, 11 + P), dt=2e-5, nsteps=2)
+    cases["tgv16_p3"] = dict(mesh=M.tgv_mesh(16, seed=1), tags=None, P=3,
+                             prm=(1.0, 1.0 / (GAMMA * 0.09), 0.3, 0.0), state=("tgv",),
+                             dt=1e-3, nsteps=2)
+    return cases
+
+
+def make_state(c, coords):
+    kind = c["state"][0]
+    if kind == "vortex":
+        return M.isentropic_vortex(coords, GAMMA, rho_scale=c["state"][1], p_scale=c["state"][2])
+    if kind == "tgv":
+        return M.taylor_green(coords, GAMMA, 0.3)
+    _, rho0, p0, seed = c["state"]
+    n_elem, nsp = coords.shape[0], coords.shape[1]
+    return M.random_state(n_elem, nsp, seed, GAMMA, rho0, p0, 0.1)
+
+
+def run(cmd):
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError(" ".join(cmd) + "\n" + r.stdout[-2000:] + r.stderr[-2000:])
+    return r
+
+
+def gen_cpu(out):
+    tmp = tempfile.mkdtemp()
+    ops = {}
+    for P in range(1, 6):
+        f = os.path.join(tmp, f"ops{P}.bin")
+        run([O.REF_CPU, "ops", str(P), f])
+        for k, v in O.read_ops_bin(f, P).items():
+            ops[f"P{P}_{k}"] = v
+    np.savez_compressed(os.path.join(out, "ref_operators.npz"), **ops)
+    geo = {}
+    for name, mesh, tags, P in (("mixed", mixed_mesh(), mixed_tags(0.9e5), 3),
+                                ("mixed", mixed_mesh(), mixed_tags(0.9e5), 5),
+                                ("tgv12", M.tgv_mesh(12, seed=1), None, 3)):
+        mb = os.path.join(tmp, "m.bin")
+        O.write_mesh_bin(mb, mesh, tags)
+        mo = os.path.join(tmp, "mo.bin")
+        run([O.REF_CPU, "mesh", mb, str(P), mo])
+        faces, J, Ji, sxy, area = O.read_mesh_out(mo, mesh.n_elem, (P + 1) ** 2)
+        key = f"{name}_P{P}"
+        for fld in faces.dtype.names:
+            geo[f"{key}_face_{fld}"] = np.asarray(faces[fld])
+        geo[f"{key}_J"], geo[f"{key}_Jinv"], geo[f"{key}_spxy"], geo[f"{key}_area"] = J, Ji, sxy, area
+    np.savez_compressed(os.path.join(out, "ref_geometry.npz"), **geo)
+    print("cpu goldens written to", out)
+
+
+def gen_gpu(out):
+    tmp = tempfile.mkdtemp()
+    res = {}
+    for name, c in case_defs().items():
+        mesh, P = c["mesh"], c["P"]
+        rho, p, mach, aoa = c["prm"]
+        orc = O.Oracle(mesh, P, GAMMA, rho, p, mach, aoa, tags=c["tags"])
+        U = make_state(c, orc.sp_coords())
+        mb, ub, rb = (os.path.join(tmp, x) for x in ("m.bin", "u.bin", "r.bin"))
+        O.write_mesh_bin(mb, mesh, c["tags"])
+        U.tofile(ub)
+        prm = [str(P), repr(GAMMA), repr(rho), repr(p), repr(mach), repr(aoa)]
+        run([O.REF_GPU, "rhs", mb, *prm, ub, rb])
+        R = np.fromfile(rb, dtype=np.float64).reshape(U.shape)
+        res[f"{name}_U"] = U
+        res[f"{name}_R"] = R
+        if c.get("nsteps"):
+            sb = os.path.join(tmp, "s.bin")
+            run([O.REF_GPU, "step", mb, *prm, ub, repr(c["dt"]), str(c["nsteps"]), sb])
+            a = np.fromfile(sb, dtype=np.float64)
+            n = U.size
+            res[f"{name}_Ustep"] = a[:n].reshape(U.shape)
+            res[f"{name}_Rstep"] = a[n:2 * n].reshape(U.shape)
+            res[f"{name}_norm"] = a[2 * n:2 * n + 1]
+        print(name, "max|R|", float(np.abs(R).max()), flush=True)
+    np.savez_compressed(os.path.join(out, "ref_gpu_residuals.npz"), **res)
+    print("gpu goldens written to", out)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("what", choices=["cpu", "gpu"])
+    ap.add_argument("--out", default=HERE)
+    a = ap.parse_args()
+    os.makedirs(a.out, exist_ok=True)
+    (gen_cpu if a.what == "cpu" else gen_gpu)(a.out)
+
+
+if __name__ == "__main__":
+    main()

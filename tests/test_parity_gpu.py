@@ -1,0 +1,169 @@
+"""Parity of the CUDA path (through the C-ABI) with the oracle and with the
+reference's own CUDA build, FP64 compat mode.
+
+Bar (north star): max |R - R_ref| / max(max|R_ref|, s_F) <= 1e-12 per
+variable per residual evaluation, s_F = max|F| * max|metric|.
+"""
+import os
+
+import numpy as np
+import pytest
+
+from tests import _util as T
+from tests.golden import make_golden as G
+from zhijian_b200 import _lib as L
+from zhijian_b200 import meshgen as M
+from zhijian_b200.solver import FRSolver, make_params
+
+pytestmark = pytest.mark.gpu
+TOL = 1e-12
+GOLD = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "ref_gpu_residuals.npz")
+
+
+def solver_for(case, zjlib):
+    rho, p, mach, aoa = case["prm"]
+    tags = case["tags"] or [(t, L.BC_TYPES[n], 0.0) for t, n in sorted(case["mesh"].tag_names.items())]
+    prm = make_params(poly_order=case["P"], gamma=G.GAMMA, rho_inf=rho, p_inf=p, Mach=mach, AoA=aoa,
+                      bcs=tags)
+    return FRSolver(case["mesh"], prm)
+
+
+def oracle_for(case, oracle_mod, threads=1):
+    rho, p, mach, aoa = case["prm"]
+    return oracle_mod.Oracle(case["mesh"], case["P"], G.GAMMA, rho, p, mach, aoa, tags=case["tags"],
+                             threads=threads)
+
+
+@pytest.mark.parametrize("name", sorted(G.case_defs()))
+def test_rhs_matches_oracle(zjlib, oracle_mod, name):
+    c = G.case_defs()[name]
+    s = solver_for(c, zjlib)
+    orc = oracle_for(c, oracle_mod)
+    xy = s.solution_point_coords()
+    assert np.array_equal(xy, orc.sp_coords())
+    U = G.make_state(c, xy)
+    R = s.rhs(U)
+    Ro = orc.rhs(U)
+    scale = T.euler_flux_scale(U, orc.geometry()[1])
+    assert T.rel_err(R, Ro, scale) <= TOL
+
+
+@pytest.mark.parametrize("name", sorted(G.case_defs()))
+def test_rhs_matches_reference_gpu_build(zjlib, name):
+    assert os.path.exists(GOLD), "reference GPU goldens missing"
+    gold = np.load(GOLD)
+    c = G.case_defs()[name]
+    s = solver_for(c, zjlib)
+    U = gold[f"{name}_U"]
+    R = s.rhs(U)
+    scale = T.euler_flux_scale(U, None) * T.metric_scale(c["mesh"], c["P"])
+    assert T.rel_err(R, gold[f"{name}_R"], scale) <= TOL
+
+
+@pytest.mark.parametrize("name", sorted(G.case_defs()))
+def test_steps_match_reference_gpu_build(zjlib, name):
+    gold = np.load(GOLD)
+    c = G.case_defs()[name]
+    if f"{name}_Ustep" not in gold:
+        pytest.skip("no stepped golden for this case")
+    s = solver_for(c, zjlib)
+    s.copyToDevice(gold[f"{name}_U"])
+    s.advance(c["dt"], c["nsteps"])
+    Us = s.copyToHost()
+    ref = gold[f"{name}_Ustep"]
+    assert T.rel_err(Us, ref, T.euler_flux_scale(ref)) <= TOL
+    norm = s.computeResidual()
+    g = float(gold[f"{name}_norm"][0])
+    assert abs(norm - g) <= 1e-11 * max(g, 1e-300)
+
+
+@pytest.mark.parametrize("P", [1, 2, 3, 4, 5])
+def test_steps_match_oracle(zjlib, oracle_mod, P):
+    c = G.case_defs()[f"mixed_p{P}"]
+    s = solver_for(c, zjlib)
+    orc = oracle_for(c, oracle_mod)
+    U = G.make_state(c, s.solution_point_coords())
+    s.copyToDevice(U)
+    s.advance(c["dt"], 4)
+    Uo, Ro = orc.step(U, c["dt"], 4)
+    assert T.rel_err(s.copyToHost(), Uo, T.euler_flux_scale(Uo)) <= TOL
+    n = s.computeResidual()
+    no = float(np.sqrt(np.sum(Ro * Ro)))
+    assert abs(n - no) <= 1e-11 * no
+    assert s.iteration == 4 and abs(s.time - 4 * c["dt"]) < 1e-18
+
+
+def test_compute_dt_matches_oracle(zjlib, oracle_mod):
+    c = G.case_defs()["vortex_dim_p3"]
+    s = solver_for(c, zjlib)
+    orc = oracle_for(c, oracle_mod)
+    U = G.make_state(c, s.solution_point_coords())
+    s.copyToDevice(U)
+    assert s.computeTimeStep() == pytest.approx(orc.compute_dt(U, 0.5), rel=1e-14)
+
+
+def test_full_size_tgv_rhs_and_step(zjlib, oracle_mod):
+    """The 256x256 jittered TGV mesh at P3 (65 536 elements): residual and
+    one step against the oracle at full size."""
+    mesh = M.tgv_mesh(256, seed=1)
+    c = dict(mesh=mesh, tags=None, P=3, prm=(1.0, 1.0 / (1.4 * 0.09), 0.3, 0.0))
+    s = solver_for(c, zjlib)
+    orc = oracle_for(c, oracle_mod, threads=os.cpu_count() or 1)
+    U = M.taylor_green(s.solution_point_coords())
+    R = s.rhs(U)
+    Ro = orc.rhs(U)
+    assert T.rel_err(R, Ro, T.euler_flux_scale(U, orc.geometry()[1])) <= TOL
+    s.copyToDevice(U)
+    s.advance(1e-3, 1)
+    Uo, _ = orc.step(U, 1e-3, 1)
+    assert T.rel_err(s.copyToHost(), Uo, T.euler_flux_scale(Uo)) <= TOL
+
+
+def test_device_pointer_rhs_equals_host_rhs(zjlib):
+    import torch
+    c = G.case_defs()["mixed_p3"]
+    s = solver_for(c, zjlib)
+    U = G.make_state(c, s.solution_point_coords())
+    Rh = s.rhs(U)
+    Ud = torch.from_numpy(U).cuda()
+    Rd = torch.empty_like(Ud)
+    s.set_stream(torch.cuda.current_stream().cuda_stream)
+    s.rhs_device(Ud.data_ptr(), Rd.data_ptr())
+    torch.cuda.synchronize()
+    assert np.array_equal(Rd.cpu().numpy(), Rh)
+
+
+def test_state_roundtrip_and_nan_detection(zjlib):
+    c = G.case_defs()["mixed_p2"]
+    s = solver_for(c, zjlib)
+    U = G.make_state(c, s.solution_point_coords())
+    s.copyToDevice(U)
+    assert np.array_equal(s.copyToHost(), U)
+    s.check_state()
+    U2 = U.copy()
+    U2[3, 2, 1] = np.nan
+    s.copyToDevice(U2)
+    with pytest.raises(L.ZJError) as e:
+        s.check_state()
+    assert e.value.code == L.ERR_NAN
+
+
+@pytest.mark.parametrize("nx,ny", [(1, 1), (1, 5), (3, 1)])
+def test_tiny_and_ragged_meshes(zjlib, oracle_mod, nx, ny):
+    """One element (four boundary edges), strips, every boundary type."""
+    mesh = M.structured_quads(nx, ny, 0.0, 1.0, 0.0, 2.0, 0.0, 0, (1, 2, 3, 4),
+                              {1: "symmetry", 2: "outflow", 3: "farfield", 4: "inflow"})
+    tags = [(1, 3, 0.0), (2, 6, 0.8e5), (3, 4, 0.0), (4, 5, 0.0)]
+    for P in (1, 3, 5):
+        c = dict(mesh=mesh, tags=tags, P=P, prm=(1.2, 1.0e5, 0.6, 30.0))
+        s = solver_for(c, zjlib)
+        orc = oracle_for(c, oracle_mod)
+        U = M.random_state(mesh.n_elem, (P + 1) ** 2, 5 + P, 1.4, 1.2, 1.0e5, 0.1)
+        assert T.rel_err(s.rhs(U), orc.rhs(U), T.euler_flux_scale(U, orc.geometry()[1])) <= TOL
+
+
+def test_step_errors(zjlib):
+    s = solver_for(G.case_defs()["mixed_p1"], zjlib)
+    assert zjlib.zj_step(s.h, 1e-3, -1) == L.ERR_ARG
+    assert zjlib.zj_step(s.h, float("nan"), 1) == L.ERR_ARG
+    assert zjlib.zj_step(s.h, 1e-3, 0) == L.OK

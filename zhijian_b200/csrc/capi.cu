@@ -1,0 +1,380 @@
+// capi.cu -- the extern "C" boundary declared in include/zj_fr.h.
+//
+// A zj_solver owns every device buffer, allocated once in zj_solver_create:
+//   state   3 x [E][n_sp][4] f64   rotating stage buffers (no stage writes a
+//                                  buffer it reads, so no aliasing)
+//   traces  3 x [E][4][n1][4] f64  ping-pong pair for the stepper + one for
+//                                  zj_rhs
+//   metrics [E][n_sp][4] Jinv, [E][n_sp] J, per-element edge records, bc
+//   scratch state + residual for the host-buffer entry points, reductions
+// An SSP-RK3 step is three fused stage launches; the first step after a state
+// upload is preceded by one trace launch.
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "zj_internal.h"
+#include "zj_kernels.h"
+
+using namespace zj;
+
+struct zj_solver {
+    zj_params prm{};
+    HostMesh mesh;
+    Operators1D ops;
+    int P = 0, n1 = 0, nsp = 0;
+    long long E = 0;
+    size_t state_n = 0, trace_n = 0;
+    double* dU[3] = {nullptr, nullptr, nullptr};
+    double* dT[3] = {nullptr, nullptr, nullptr};
+    double* dUs = nullptr;      // scratch state (host-buffer residual)
+    double* dRs = nullptr;      // scratch residual
+    double* dJinv = nullptr;
+    double* dJ = nullptr;
+    double* dOps = nullptr;
+    double* dBC = nullptr;
+    double* dH = nullptr;       // sqrt(element area) for the CFL step
+    double* dScal = nullptr;    // [0] dt, [1] step norm^2, [2] dt out, [3] rhs norm^2
+    double* dPart = nullptr;    // per-CTA partial sums, stepper
+    double* dPartR = nullptr;   // per-CTA partial sums, zj_rhs
+    double* dScratch = nullptr; // CFL reduction scratch
+    int scratch_n = 0;
+    int* dFlag = nullptr;
+    EdgeRec* dEdges = nullptr;
+    double4* dNrm = nullptr;
+    int grid = 0;
+    int cur = 0, tpar = 0;
+    bool traces_valid = false;
+    bool has_norm = false;
+    cudaStream_t own = nullptr, stream = nullptr;
+    double time = 0.0;
+    int iter = 0;
+    double last_dt = -1.0;
+    std::string err;
+};
+
+namespace {
+
+thread_local std::string g_create_err;
+
+zj_status fail(zj_solver* s, zj_status code, const std::string& msg) {
+    if (s) s->err = msg; else g_create_err = msg;
+    return code;
+}
+
+zj_status cuda_fail(zj_solver* s, cudaError_t e, const char* what) {
+    std::string m = std::string(what) + ": " + cudaGetErrorName(e) + " (" + cudaGetErrorString(e) + ")";
+    return fail(s, ZJ_ERR_CUDA, m);
+}
+
+#define ZJ_CK(s, call, what)                                   \
+    do {                                                       \
+        cudaError_t e_ = (call);                               \
+        if (e_ != cudaSuccess) return cuda_fail((s), e_, what); \
+    } while (0)
+
+template <class T>
+cudaError_t dalloc(T** p, size_t n) {
+    return cudaMalloc(reinterpret_cast<void**>(p), (n ? n : 1) * sizeof(T));
+}
+
+void free_all(zj_solver* s) {
+    for (auto& p : s->dU) { if (p) cudaFree(p); p = nullptr; }
+    for (auto& p : s->dT) { if (p) cudaFree(p); p = nullptr; }
+    double** ds[] = {&s->dUs, &s->dRs, &s->dJinv, &s->dJ, &s->dOps, &s->dBC, &s->dH,
+                     &s->dScal, &s->dPart, &s->dPartR, &s->dScratch};
+    for (auto pp : ds) { if (*pp) cudaFree(*pp); *pp = nullptr; }
+    if (s->dFlag) cudaFree(s->dFlag);
+    if (s->dEdges) cudaFree(s->dEdges);
+    if (s->dNrm) cudaFree(s->dNrm);
+    s->dFlag = nullptr; s->dEdges = nullptr; s->dNrm = nullptr;
+    if (s->own) cudaStreamDestroy(s->own);
+    s->own = nullptr;
+}
+
+zj_status validate_params(const zj_params* p, std::string& msg) {
+    if (p->poly_order < 1 || p->poly_order > kMaxP) { msg = "poly_order must be 1..5"; return ZJ_ERR_ARG; }
+    if (!(p->gamma > 1.0)) { msg = "gamma must be > 1"; return ZJ_ERR_ARG; }
+    if (!(p->rho_inf > 0.0) || !(p->p_inf > 0.0)) { msg = "rho_inf and p_inf must be > 0"; return ZJ_ERR_ARG; }
+    if (p->flux_type < 0 || p->flux_type > 3) { msg = "flux_type must be DG, SD, HU or GA"; return ZJ_ERR_ARG; }
+    if (p->riemann < 0 || p->riemann > 2) { msg = "riemann must be Rusanov, Roe or HLLC"; return ZJ_ERR_ARG; }
+    if (p->n_bc < 0 || p->n_bc > ZJ_MAX_BC) { msg = "n_bc out of range"; return ZJ_ERR_ARG; }
+    if (!p->compat) { msg = "physics mode (compat off) is not built yet"; return ZJ_ERR_UNSUPPORTED; }
+    if (p->precision != ZJ_FP64) { msg = "the mixed-precision form is not built yet"; return ZJ_ERR_UNSUPPORTED; }
+    return ZJ_OK;
+}
+
+StageArgs base_args(const zj_solver* s) {
+    StageArgs a{};
+    a.Jinv = s->dJinv;
+    a.J = s->dJ;
+    a.edges = s->dEdges;
+    a.enrm = s->dNrm;
+    a.bc = s->dBC;
+    a.ops = s->dOps;
+    a.dt = s->dScal;
+    a.n_elem = s->E;
+    a.gamma = s->prm.gamma;
+    return a;
+}
+
+zj_status enqueue_step(zj_solver* s) {
+    const int c = s->cur, a1 = (c + 1) % 3, b1 = (c + 2) % 3, p = s->tpar;
+    StageArgs a = base_args(s);
+    a.partials = s->dPart;
+    // stage 1: U(1) = U0 + dt R(U0)
+    a.U = s->dU[c]; a.U0 = s->dU[c]; a.Uout = s->dU[a1]; a.Tin = s->dT[p]; a.Tout = s->dT[1 - p];
+    a.stage = 1;
+    ZJ_CK(s, launch_compat_stage(s->P, a, s->stream, nullptr), "stage 1 launch");
+    // stage 2: U(2) = 3/4 U0 + 1/4 U(1) + 1/4 dt R(U(1))
+    a.U = s->dU[a1]; a.Uout = s->dU[b1]; a.Tin = s->dT[1 - p]; a.Tout = s->dT[p];
+    a.stage = 2;
+    ZJ_CK(s, launch_compat_stage(s->P, a, s->stream, nullptr), "stage 2 launch");
+    // stage 3: U = 1/3 U0 + 2/3 U(2) + 2/3 dt R(U(2))
+    a.U = s->dU[b1]; a.Uout = s->dU[a1]; a.Tin = s->dT[p]; a.Tout = s->dT[1 - p];
+    a.stage = 3;
+    ZJ_CK(s, launch_compat_stage(s->P, a, s->stream, nullptr), "stage 3 launch");
+    s->cur = a1;
+    s->tpar = 1 - p;
+    return ZJ_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int zj_abi_version(void) { return ZJ_ABI_VERSION; }
+
+const char* zj_last_error(const zj_solver* s) {
+    return s ? s->err.c_str() : g_create_err.c_str();
+}
+
+zj_status zj_solver_create(const zj_mesh_desc* mesh, const zj_params* params, zj_solver** out) {
+    if (!out) return fail(nullptr, ZJ_ERR_ARG, "out is NULL");
+    *out = nullptr;
+    if (!mesh || !params) return fail(nullptr, ZJ_ERR_ARG, "mesh or params is NULL");
+    std::string msg;
+    zj_status st = validate_params(params, msg);
+    if (st != ZJ_OK) return fail(nullptr, st, msg);
+
+    zj_solver* s = new zj_solver();
+    s->prm = *params;
+    s->P = params->poly_order;
+    s->n1 = s->P + 1;
+    s->nsp = s->n1 * s->n1;
+    if (!build_mesh(mesh, params, s->mesh, msg)) { delete s; return fail(nullptr, ZJ_ERR_ARG, msg); }
+    s->E = s->mesh.n_elem;
+    if (s->E > (1LL << 31) / (4LL * s->nsp)) { delete s; return fail(nullptr, ZJ_ERR_ARG, "mesh too large"); }
+    build_operators_compat(s->P, s->ops);
+    std::vector<double> J, Jinv, bc, nrm, area, packed;
+    std::vector<EdgeRec> rec;
+    if (!build_metrics(s->mesh, s->ops, J, Jinv, msg)) { delete s; return fail(nullptr, ZJ_ERR_ARG, msg); }
+    build_bc_data(s->mesh, params, bc);
+    build_edge_records(s->mesh, rec, nrm);
+    element_areas(s->mesh, area);
+    for (auto& a : area) a = std::sqrt(a);
+    pack_ops(s->ops, packed);
+
+    s->state_n = (size_t)s->E * s->nsp * 4;
+    s->trace_n = (size_t)s->E * 4 * s->n1 * 4;
+    s->grid = stage_grid(s->P, s->E);
+    s->scratch_n = 148 * 8;
+    cudaError_t e = cudaSuccess;
+#define ZJ_ALLOC(ptr, n)                                                     \
+    if (e == cudaSuccess) e = dalloc(&(ptr), (n));
+    for (int i = 0; i < 3; ++i) { ZJ_ALLOC(s->dU[i], s->state_n); }
+    for (int i = 0; i < 3; ++i) { ZJ_ALLOC(s->dT[i], s->trace_n); }
+    ZJ_ALLOC(s->dUs, s->state_n);
+    ZJ_ALLOC(s->dRs, s->state_n);
+    ZJ_ALLOC(s->dJinv, Jinv.size());
+    ZJ_ALLOC(s->dJ, J.size());
+    ZJ_ALLOC(s->dOps, packed.size());
+    ZJ_ALLOC(s->dBC, bc.size());
+    ZJ_ALLOC(s->dH, area.size());
+    ZJ_ALLOC(s->dScal, 8);
+    ZJ_ALLOC(s->dPart, (size_t)s->grid);
+    ZJ_ALLOC(s->dPartR, (size_t)s->grid);
+    ZJ_ALLOC(s->dScratch, (size_t)s->scratch_n);
+    ZJ_ALLOC(s->dFlag, 1);
+    ZJ_ALLOC(s->dEdges, rec.size());
+    ZJ_ALLOC(s->dNrm, rec.size());
+#undef ZJ_ALLOC
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&s->own, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaMemcpy(s->dJinv, Jinv.data(), Jinv.size() * 8, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemcpy(s->dJ, J.data(), J.size() * 8, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemcpy(s->dOps, packed.data(), packed.size() * 8, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemcpy(s->dBC, bc.data(), bc.size() * 8, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemcpy(s->dH, area.data(), area.size() * 8, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemcpy(s->dEdges, rec.data(), rec.size() * sizeof(EdgeRec), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemcpy(s->dNrm, nrm.data(), nrm.size() * 8, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemset(s->dU[0], 0, s->state_n * 8);
+    if (e == cudaSuccess) e = cudaMemset(s->dScal, 0, 8 * 8);
+    if (e == cudaSuccess) e = cudaDeviceSynchronize();
+    if (e != cudaSuccess) {
+        std::string m = std::string("device setup: ") + cudaGetErrorName(e) + " (" + cudaGetErrorString(e) + ")";
+        free_all(s);
+        delete s;
+        return fail(nullptr, ZJ_ERR_CUDA, m);
+    }
+    s->stream = s->own;
+    *out = s;
+    return ZJ_OK;
+}
+
+void zj_solver_destroy(zj_solver* s) {
+    if (!s) return;
+    if (s->stream) cudaStreamSynchronize(s->stream);
+    free_all(s);
+    delete s;
+}
+
+int64_t zj_num_elements(const zj_solver* s) { return s ? s->E : 0; }
+int zj_num_solution_points(const zj_solver* s) { return s ? s->nsp : 0; }
+int64_t zj_num_faces(const zj_solver* s) { return s ? s->mesh.n_faces : 0; }
+int64_t zj_state_size(const zj_solver* s) { return s ? (int64_t)s->state_n : 0; }
+double zj_time(const zj_solver* s) { return s ? s->time : 0.0; }
+int zj_iteration(const zj_solver* s) { return s ? s->iter : 0; }
+
+zj_status zj_solution_point_coords(const zj_solver* s, double* xy) {
+    if (!s || !xy) return ZJ_ERR_ARG;
+    std::vector<double> c;
+    sp_coords(s->mesh, s->ops, c);
+    std::memcpy(xy, c.data(), c.size() * sizeof(double));
+    return ZJ_OK;
+}
+
+zj_status zj_set_stream(zj_solver* s, void* stream) {
+    if (!s) return ZJ_ERR_ARG;
+    s->stream = stream ? static_cast<cudaStream_t>(stream) : s->own;
+    return ZJ_OK;
+}
+
+void* zj_get_stream(const zj_solver* s) { return s ? static_cast<void*>(s->stream) : nullptr; }
+
+zj_status zj_set_state(zj_solver* s, const double* U) {
+    if (!s || !U) return ZJ_ERR_ARG;
+    ZJ_CK(s, cudaMemcpyAsync(s->dU[s->cur], U, s->state_n * 8, cudaMemcpyHostToDevice, s->stream), "set_state copy");
+    ZJ_CK(s, cudaStreamSynchronize(s->stream), "set_state sync");
+    s->traces_valid = false;
+    s->has_norm = false;
+    s->time = 0.0;
+    s->iter = 0;
+    return ZJ_OK;
+}
+
+zj_status zj_get_state(zj_solver* s, double* U) {
+    if (!s || !U) return ZJ_ERR_ARG;
+    ZJ_CK(s, cudaMemcpyAsync(U, s->dU[s->cur], s->state_n * 8, cudaMemcpyDeviceToHost, s->stream), "get_state copy");
+    ZJ_CK(s, cudaStreamSynchronize(s->stream), "get_state sync");
+    return ZJ_OK;
+}
+
+zj_status zj_set_state_device(zj_solver* s, const double* U) {
+    if (!s || !U) return ZJ_ERR_ARG;
+    ZJ_CK(s, cudaMemcpyAsync(s->dU[s->cur], U, s->state_n * 8, cudaMemcpyDeviceToDevice, s->stream), "set_state_device copy");
+    s->traces_valid = false;
+    s->has_norm = false;
+    s->time = 0.0;
+    s->iter = 0;
+    return ZJ_OK;
+}
+
+zj_status zj_get_state_device(zj_solver* s, double* U) {
+    if (!s || !U) return ZJ_ERR_ARG;
+    ZJ_CK(s, cudaMemcpyAsync(U, s->dU[s->cur], s->state_n * 8, cudaMemcpyDeviceToDevice, s->stream), "get_state_device copy");
+    return ZJ_OK;
+}
+
+zj_status zj_step(zj_solver* s, double dt, int nsteps) {
+    if (!s) return ZJ_ERR_ARG;
+    if (nsteps < 0 || !std::isfinite(dt)) return fail(s, ZJ_ERR_ARG, "bad dt or nsteps");
+    if (nsteps == 0) return ZJ_OK;
+    if (dt != s->last_dt) {
+        ZJ_CK(s, cudaMemcpyAsync(s->dScal, &dt, sizeof(double), cudaMemcpyHostToDevice, s->stream), "dt upload");
+        s->last_dt = dt;
+    }
+    if (!s->traces_valid) {
+        ZJ_CK(s, launch_traces(s->P, s->dU[s->cur], s->dT[s->tpar], s->dOps, s->E, s->stream), "trace launch");
+        s->traces_valid = true;
+    }
+    for (int k = 0; k < nsteps; ++k) {
+        zj_status st = enqueue_step(s);
+        if (st != ZJ_OK) return st;
+        s->time += dt;
+        s->iter += 1;
+    }
+    s->has_norm = true;
+    return ZJ_OK;
+}
+
+zj_status zj_synchronize(zj_solver* s) {
+    if (!s) return ZJ_ERR_ARG;
+    ZJ_CK(s, cudaStreamSynchronize(s->stream), "synchronize");
+    return ZJ_OK;
+}
+
+zj_status zj_rhs(zj_solver* s, const double* U_dev, double* R_dev) {
+    if (!s || !U_dev || !R_dev) return ZJ_ERR_ARG;
+    if ((reinterpret_cast<uintptr_t>(U_dev) | reinterpret_cast<uintptr_t>(R_dev)) & 15u)
+        return fail(s, ZJ_ERR_ARG, "U_dev and R_dev must be 16-byte aligned");
+    ZJ_CK(s, launch_traces(s->P, U_dev, s->dT[2], s->dOps, s->E, s->stream), "trace launch");
+    StageArgs a = base_args(s);
+    a.U = U_dev; a.U0 = U_dev; a.Uout = nullptr; a.Tin = s->dT[2]; a.Tout = nullptr;
+    a.R = R_dev; a.partials = s->dPartR; a.stage = 0;
+    ZJ_CK(s, launch_compat_stage(s->P, a, s->stream, nullptr), "residual launch");
+    return ZJ_OK;
+}
+
+zj_status zj_rhs_host(zj_solver* s, const double* U, double* R) {
+    if (!s || !U || !R) return ZJ_ERR_ARG;
+    ZJ_CK(s, cudaMemcpyAsync(s->dUs, U, s->state_n * 8, cudaMemcpyHostToDevice, s->stream), "rhs upload");
+    zj_status st = zj_rhs(s, s->dUs, s->dRs);
+    if (st != ZJ_OK) return st;
+    ZJ_CK(s, cudaMemcpyAsync(R, s->dRs, s->state_n * 8, cudaMemcpyDeviceToHost, s->stream), "rhs download");
+    ZJ_CK(s, cudaStreamSynchronize(s->stream), "rhs sync");
+    return ZJ_OK;
+}
+
+zj_status zj_residual_norm(zj_solver* s, double* out) {
+    if (!s || !out) return ZJ_ERR_ARG;
+    if (!s->has_norm) { *out = 0.0; return ZJ_OK; }
+    ZJ_CK(s, launch_reduce_sum(s->dPart, s->grid, s->dScal + 1, s->stream), "norm reduce");
+    double v = 0.0;
+    ZJ_CK(s, cudaMemcpyAsync(&v, s->dScal + 1, sizeof(double), cudaMemcpyDeviceToHost, s->stream), "norm copy");
+    ZJ_CK(s, cudaStreamSynchronize(s->stream), "norm sync");
+    *out = std::sqrt(v);
+    return ZJ_OK;
+}
+
+zj_status zj_compute_dt(zj_solver* s, double* dt_out) {
+    if (!s || !dt_out) return ZJ_ERR_ARG;
+    ZJ_CK(s, launch_compute_dt(s->dU[s->cur], s->dH, s->E, s->nsp, s->prm.gamma, s->prm.CFL, s->P,
+                               s->dScratch, s->scratch_n, s->dScal + 2, s->stream), "dt launch");
+    double v = 0.0;
+    ZJ_CK(s, cudaMemcpyAsync(&v, s->dScal + 2, sizeof(double), cudaMemcpyDeviceToHost, s->stream), "dt copy");
+    ZJ_CK(s, cudaStreamSynchronize(s->stream), "dt sync");
+    *dt_out = v;
+    return ZJ_OK;
+}
+
+zj_status zj_check_state(zj_solver* s) {
+    if (!s) return ZJ_ERR_ARG;
+    ZJ_CK(s, launch_check_finite(s->dU[s->cur], (long long)s->state_n, s->dFlag, s->stream), "check launch");
+    int flag = 0;
+    ZJ_CK(s, cudaMemcpyAsync(&flag, s->dFlag, sizeof(int), cudaMemcpyDeviceToHost, s->stream), "check copy");
+    ZJ_CK(s, cudaStreamSynchronize(s->stream), "check sync");
+    if (flag) return fail(s, ZJ_ERR_NAN, "state holds NaN or Inf");
+    return ZJ_OK;
+}
+
+zj_status zj_solver_create_from_gmsh(const char* msh_path, const zj_params* params, zj_solver** out) {
+    (void)msh_path; (void)params;
+    if (out) *out = nullptr;
+    return fail(nullptr, ZJ_ERR_UNSUPPORTED, "Gmsh reader not built yet");
+}
+
+}  // extern "C"

@@ -1,0 +1,523 @@
+// compat_fp64.cu -- FP64 residual and SSP-RK3 stage kernels with the
+// reference's residual semantics ("compat" mode).
+//
+// One fused launch per RK stage.  A CTA owns EB consecutive elements; every
+// element has TPE threads.  Per stage:
+//   A  thread per solution point: load the stage state (32 contiguous bytes
+//      per point, coalesced across the warp), Euler fluxes into shared memory.
+//   B  thread per flux point: own trace + the neighbour's trace (written by
+//      the previous stage), ghost state on boundaries, Rusanov flux and the
+//      flux difference of this element's side, into shared memory.
+//   C  thread per solution point: sum-factorised divergence, FR correction,
+//      SSP-RK3 update and positivity clamp; write the new state.
+//   D  thread per flux point: traces of the new state for the next stage.
+// The 2D reference operators are Kronecker products of 1D ones with exact
+// 0/1 factors, so the sum-factorised sums add the same nonzero terms in the
+// same order as the reference's dense loops.
+//
+// Reference: src/gpu/kernels.cu K1 :30-67, K4 :157-194, K8 :346-450,
+// K9 :453-525, K10 :528-701, K13 :813-872, K15 :948-1034, K17 :1245-1295,
+// K18 :1297-1349; include/physics/euler.hpp:16-129.
+#include <cuda_runtime.h>
+
+#include "zj_kernels.h"
+
+namespace zj {
+
+void pack_ops(const Operators1D& o, std::vector<double>& out) {
+    const int n1 = o.n1;
+    out.assign(ops_size(n1), 0.0);
+    for (int i = 0; i < n1 * n1; ++i) out[i] = o.D1[i];
+    for (int j = 0; j < n1; ++j) {
+        out[n1 * n1 + j] = o.Lm[j];
+        out[n1 * n1 + n1 + j] = o.Lp[j];
+        out[n1 * n1 + 2 * n1 + j] = o.gL[j];
+        out[n1 * n1 + 3 * n1 + j] = o.gR[j];
+    }
+}
+
+namespace {
+
+template <int P>
+struct Shape {
+    static constexpr int N1 = P + 1;
+    static constexpr int NSP = N1 * N1;
+    static constexpr int NFT = 4 * N1;                 // flux points per element
+    static constexpr int TPE = NSP > NFT ? NSP : NFT;  // threads per element
+    static constexpr int EB = (256 / TPE) > 0 ? (256 / TPE) : 1;
+    static constexpr int THREADS = EB * TPE;
+    static constexpr int NOPS = N1 * N1 + 4 * N1;
+};
+
+// ---------------------------------------------------------------- physics --
+
+// IdealGas::pressure (euler.hpp:16-23)
+__device__ __forceinline__ double pressure(const double* U, double g) {
+    const double rho = U[0], u = U[1] / rho, v = U[2] / rho, E = U[3] / rho;
+    const double ke = 0.5 * (u * u + v * v);
+    return (g - 1.0) * rho * (E - ke);
+}
+
+// IdealGas::fluxX / fluxY (euler.hpp:101-129)
+__device__ __forceinline__ void flux_xy(const double* U, double g, double* F, double* G) {
+    const double rho = U[0], u = U[1] / rho, v = U[2] / rho, p = pressure(U, g);
+    F[0] = U[1]; F[1] = U[1] * u + p; F[2] = U[1] * v; F[3] = (U[3] + p) * u;
+    G[0] = U[2]; G[1] = U[2] * u; G[2] = U[2] * v + p; G[3] = (U[3] + p) * v;
+}
+
+__device__ __forceinline__ void prim2cons(double rho, double u, double v, double p, double g,
+                                          double* U) {
+    U[0] = rho; U[1] = rho * u; U[2] = rho * v;
+    U[3] = p / (g - 1.0) + 0.5 * rho * (u * u + v * v);
+}
+
+// computeGhostState (kernels.cu:453-525)
+__device__ void ghost_compat(const double* Ui, double nx, double ny, int bct,
+                             const double* __restrict__ bcd, double g, double* Ug) {
+    switch (bct) {
+        case ZJ_BC_WALL: case ZJ_BC_SLIPWALL: case ZJ_BC_SYMMETRY: {
+            const double rho = Ui[0], u = Ui[1] / rho, v = Ui[2] / rho;
+            const double p = pressure(Ui, g);
+            const double vn = u * nx + v * ny;
+            prim2cons(rho, u - 2.0 * vn * nx, v - 2.0 * vn * ny, p, g, Ug);
+            break;
+        }
+        case ZJ_BC_FARFIELD: {
+            const double rho_inf = bcd[0], u_inf = bcd[1], v_inf = bcd[2], p_inf = bcd[3];
+            const double rho_i = fmax(Ui[0], 1e-10);
+            const double u_i = Ui[1] / rho_i, v_i = Ui[2] / rho_i;
+            const double p_i = fmax((g - 1.0) * (Ui[3] - 0.5 * rho_i * (u_i * u_i + v_i * v_i)), 1e-10);
+            const double vn_inf = u_inf * nx + v_inf * ny;
+            double rb, ub, vb;
+            if (vn_inf > 0) { rb = rho_inf; ub = u_inf; vb = v_inf; }
+            else { rb = rho_i; ub = u_i; vb = v_i; }
+            double pb = 0.5 * (p_inf + p_i);
+            rb = fmax(fmin(rb, 100.0), 0.01);
+            ub = fmax(fmin(ub, 1000.0), -1000.0);
+            vb = fmax(fmin(vb, 1000.0), -1000.0);
+            pb = fmax(fmin(pb, 1e7), 1e3);
+            prim2cons(rb, ub, vb, pb, g, Ug);
+            break;
+        }
+        case ZJ_BC_OUTFLOW: {
+            const double rho = Ui[0], u = Ui[1] / rho, v = Ui[2] / rho;
+            prim2cons(rho, u, v, bcd[0], g, Ug);
+            break;
+        }
+        default:
+            Ug[0] = Ui[0]; Ug[1] = Ui[1]; Ug[2] = Ui[2]; Ug[3] = Ui[3];
+    }
+}
+
+// The reference's hard-coded Rusanov with floors (kernels.cu:597-669).
+__device__ void rusanov_compat(const double* UL, const double* UR, double nx, double ny,
+                               double g, double* F) {
+    const double rhoL = fmax(UL[0], 1e-10), rhoR = fmax(UR[0], 1e-10);
+    const double uL = UL[1] / rhoL, vL = UL[2] / rhoL, uR = UR[1] / rhoR, vR = UR[2] / rhoR;
+    const double EL = UL[3] / rhoL, ER = UR[3] / rhoR;
+    const double pL = fmax((g - 1.0) * rhoL * (EL - 0.5 * (uL * uL + vL * vL)), 1e-10);
+    const double pR = fmax((g - 1.0) * rhoR * (ER - 0.5 * (uR * uR + vR * vR)), 1e-10);
+    const double cL = sqrt(fmax(g * pL / rhoL, 1e-10)), cR = sqrt(fmax(g * pR / rhoR, 1e-10));
+    const double vnL = uL * nx + vL * ny, vnR = uR * nx + vR * ny;
+    const double smax = fmax(sqrt(uL * uL + vL * vL) + cL, sqrt(uR * uR + vR * vR) + cR);
+    const double HL = EL + pL / rhoL, HR = ER + pR / rhoR;
+    const double FL[4] = {rhoL * vnL, rhoL * uL * vnL + pL * nx, rhoL * vL * vnL + pL * ny, rhoL * HL * vnL};
+    const double FR[4] = {rhoR * vnR, rhoR * uR * vnR + pR * nx, rhoR * vR * vnR + pR * ny, rhoR * HR * vnR};
+#pragma unroll
+    for (int v = 0; v < 4; ++v) {
+        double f = 0.5 * (FL[v] + FR[v]) - 0.5 * smax * (UR[v] - UL[v]);
+        F[v] = isfinite(f) ? f : 0.0;
+    }
+}
+
+// enforcePositivityKernel (kernels.cu:1236-1288): gamma fixed at 1.4.
+__device__ __forceinline__ void positivity(double* U) {
+    const double rn = fmax(0.01, fmin(100.0, U[0]));
+    double u = U[1] / fmax(rn, 1e-10), v = U[2] / fmax(rn, 1e-10);
+    const double vm = sqrt(u * u + v * v);
+    if (vm > 2000.0) { const double s = 2000.0 / vm; u *= s; v *= s; }
+    const double ke = 0.5 * rn * (u * u + v * v);
+    double p = (1.4 - 1.0) * (U[3] - ke);
+    p = fmax(100.0, fmin(1e8, p));
+    U[0] = rn; U[1] = rn * u; U[2] = rn * v; U[3] = p / (1.4 - 1.0) + ke;
+}
+
+__device__ __forceinline__ void load4(const double* p, double* v) {
+    const double2 a = *reinterpret_cast<const double2*>(p);
+    const double2 b = *reinterpret_cast<const double2*>(p + 2);
+    v[0] = a.x; v[1] = a.y; v[2] = b.x; v[3] = b.y;
+}
+__device__ __forceinline__ void load4_nc(const double* p, double* v) {
+    const double2 a = __ldg(reinterpret_cast<const double2*>(p));
+    const double2 b = __ldg(reinterpret_cast<const double2*>(p + 2));
+    v[0] = a.x; v[1] = a.y; v[2] = b.x; v[3] = b.y;
+}
+__device__ __forceinline__ void store4(double* p, const double* v) {
+    *reinterpret_cast<double2*>(p) = make_double2(v[0], v[1]);
+    *reinterpret_cast<double2*>(p + 2) = make_double2(v[2], v[3]);
+}
+
+// Trace of one flux point from a state held in shared memory as
+// s[var][j*N1 + i] (i: xi index, j: eta index).  Edge parametrisations follow
+// FROperators::initQuad (basis.cpp:540-552): edges 0,1 run with +s, edges 2,3
+// with -s, so fp on edges 2,3 meets xi/eta index N1-1-fp.  Sums run over the
+// index the reference's dense row has nonzero weights on, ascending.
+template <int N1>
+__device__ __forceinline__ void trace_point(const double (*s)[N1 * N1], const double* Lm,
+                                            const double* Lp, int edge, int fp, double* out) {
+#pragma unroll
+    for (int v = 0; v < 4; ++v) {
+        double t = 0.0;
+        if (edge == 0) {
+#pragma unroll
+            for (int j = 0; j < N1; ++j) t = fma(Lm[j], s[v][j * N1 + fp], t);
+        } else if (edge == 1) {
+#pragma unroll
+            for (int i = 0; i < N1; ++i) t = fma(Lp[i], s[v][fp * N1 + i], t);
+        } else if (edge == 2) {
+#pragma unroll
+            for (int j = 0; j < N1; ++j) t = fma(Lp[j], s[v][j * N1 + (N1 - 1 - fp)], t);
+        } else {
+#pragma unroll
+            for (int i = 0; i < N1; ++i) t = fma(Lm[i], s[v][(N1 - 1 - fp) * N1 + i], t);
+        }
+        out[v] = t;
+    }
+}
+
+// Block-wide deterministic sum; result valid in thread 0.
+__device__ double block_sum(double x, double* red) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) x += __shfl_down_sync(0xffffffffu, x, o);
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    if (lane == 0) red[w] = x;
+    __syncthreads();
+    double s = 0.0;
+    if (threadIdx.x == 0) {
+        const int nw = (blockDim.x + 31) >> 5;
+        for (int i = 0; i < nw; ++i) s += red[i];
+    }
+    return s;
+}
+
+// -------------------------------------------------------------- kernels --
+
+template <int P>
+__global__ void __launch_bounds__(Shape<P>::THREADS)
+k_compat_stage(const StageArgs a) {
+    using S = Shape<P>;
+    constexpr int N1 = S::N1, NSP = S::NSP, NFT = S::NFT, TPE = S::TPE, EB = S::EB;
+    __shared__ double sOps[S::NOPS];
+    __shared__ double sF[EB][4][NSP];
+    __shared__ double sG[EB][4][NSP];
+    __shared__ double sD[EB][NFT][4];
+    __shared__ double sU[EB][4][NSP];
+    __shared__ double sRed[32];
+
+    const int tid = threadIdx.x;
+    for (int i = tid; i < S::NOPS; i += blockDim.x) sOps[i] = a.ops[i];
+    const double* D1 = sOps;
+    const double* Lm = sOps + N1 * N1;
+    const double* Lp = Lm + N1;
+    const double* gL = Lp + N1;
+    const double* gR = gL + N1;
+
+    const int el = tid / TPE, k = tid - el * TPE;
+    const long long e = (long long)blockIdx.x * EB + el;
+    const bool valid = (el < EB) && (e < a.n_elem);
+    const double g = a.gamma;
+
+    // ---- A: fluxes at the solution points
+    double u[4], ji[4], u0[4];
+    if (valid && k < NSP) {
+        const long long idx = e * NSP + k;
+        load4(a.U + idx * 4, u);
+        double F[4], G[4];
+        flux_xy(u, g, F, G);
+#pragma unroll
+        for (int v = 0; v < 4; ++v) { sF[el][v][k] = F[v]; sG[el][v][k] = G[v]; }
+        load4_nc(a.Jinv + idx * 4, ji);
+        if (a.stage >= 2) load4(a.U0 + idx * 4, u0);
+        else { u0[0] = u[0]; u0[1] = u[1]; u0[2] = u[2]; u0[3] = u[3]; }
+    }
+    __syncthreads();   // sOps ready
+
+    // ---- B: interface fluxes, this element's side
+    if (valid && k < NFT) {
+        const int edge = k / N1, fp = k - edge * N1;
+        const EdgeRec r = a.edges[e * 4 + edge];
+        const double2 nr = __ldg(reinterpret_cast<const double2*>(a.enrm + e * 4 + edge));
+        const double nx = nr.x, ny = nr.y;
+        double Fd[4] = {0.0, 0.0, 0.0, 0.0};
+        if (!(r.flags & kEdgeOrphan)) {
+            const double* own = a.Tin + (e * 4 + edge) * N1 * 4;
+            double UL[4], UR[4], Fc[4], Fx[4], Fy[4], Uo[4];
+            if (!(r.flags & kEdgeRight)) {
+                load4_nc(own + fp * 4, UL);
+                if (r.nbr >= 0) {
+                    load4_nc(a.Tin + ((long long)r.nbr * 4 + r.nbr_edge) * N1 * 4 + (N1 - 1 - fp) * 4, UR);
+                } else {
+                    ghost_compat(UL, nx, ny, edge_bc_type(r.flags), a.bc + (long long)r.nbr_edge * 8, g, UR);
+                }
+                rusanov_compat(UL, UR, nx, ny, g, Fc);
+                flux_xy(UL, g, Fx, Fy);
+#pragma unroll
+                for (int v = 0; v < 4; ++v) Fd[v] = Fc[v] - (Fx[v] * nx + Fy[v] * ny);
+            } else {
+                // Right side: the common flux at fp pairs the left trace at fp
+                // with this trace at N1-1-fp (kernels.cu:577), while the
+                // interior flux uses this trace at fp (kernels.cu:402-425).
+                load4_nc(a.Tin + ((long long)r.nbr * 4 + r.nbr_edge) * N1 * 4 + fp * 4, UL);
+                load4_nc(own + (N1 - 1 - fp) * 4, UR);
+                rusanov_compat(UL, UR, nx, ny, g, Fc);
+                load4_nc(own + fp * 4, Uo);
+                flux_xy(Uo, g, Fx, Fy);
+#pragma unroll
+                for (int v = 0; v < 4; ++v) Fd[v] = -Fc[v] + (Fx[v] * nx + Fy[v] * ny);
+            }
+        }
+#pragma unroll
+        for (int v = 0; v < 4; ++v) sD[el][k][v] = Fd[v];
+    }
+    __syncthreads();
+
+    // ---- C: divergence, correction, stage update
+    double rsq = 0.0;
+    if (valid && k < NSP) {
+        const int i = k % N1, j = k / N1;   // xi index, eta index
+        const long long idx = e * NSP + k;
+        double res[4];
+#pragma unroll
+        for (int v = 0; v < 4; ++v) {
+            double dFdxi = 0.0, dFdeta = 0.0, dGdxi = 0.0, dGdeta = 0.0;
+#pragma unroll
+            for (int m = 0; m < N1; ++m) {
+                const double dxi = D1[i * N1 + m], deta = D1[j * N1 + m];
+                dFdxi = fma(dxi, sF[el][v][j * N1 + m], dFdxi);
+                dFdeta = fma(deta, sF[el][v][m * N1 + i], dFdeta);
+                dGdxi = fma(dxi, sG[el][v][j * N1 + m], dGdxi);
+                dGdeta = fma(deta, sG[el][v][m * N1 + i], dGdeta);
+            }
+            const double div = (dFdxi * ji[0] + dFdeta * ji[2]) + (dGdxi * ji[1] + dGdeta * ji[3]);
+            double rr = -div;
+            double corr = 0.0;
+            corr += sD[el][0 * N1 + i][v] * gL[j];
+            corr += sD[el][1 * N1 + j][v] * gR[i];
+            corr += sD[el][2 * N1 + i][v] * gR[j];
+            corr += sD[el][3 * N1 + j][v] * gL[i];
+            rr -= corr;
+            res[v] = rr;
+        }
+        if (a.stage == 0) {
+            store4(a.R + idx * 4, res);
+#pragma unroll
+            for (int v = 0; v < 4; ++v) rsq += res[v] * res[v];
+        } else {
+            const double dt = *a.dt;
+            double uo[4];
+#pragma unroll
+            for (int v = 0; v < 4; ++v) {
+                if (a.stage == 1) uo[v] = u0[v] + dt * res[v];
+                else if (a.stage == 2) uo[v] = 0.75 * u0[v] + 0.25 * u[v] + 0.25 * dt * res[v];
+                else uo[v] = (1.0 / 3.0) * u0[v] + (2.0 / 3.0) * u[v] + (2.0 / 3.0) * dt * res[v];
+            }
+            positivity(uo);
+            store4(a.Uout + idx * 4, uo);
+#pragma unroll
+            for (int v = 0; v < 4; ++v) sU[el][v][k] = uo[v];
+            if (a.stage == 3) {
+#pragma unroll
+                for (int v = 0; v < 4; ++v) rsq += res[v] * res[v];
+            }
+        }
+    }
+    if (a.stage == 0 || a.stage == 3) {
+        const double bs = block_sum(rsq, sRed);
+        if (tid == 0) a.partials[blockIdx.x] = bs;
+    }
+    if (a.stage == 0) return;
+    __syncthreads();
+
+    // ---- D: traces of the new state
+    if (valid && k < NFT) {
+        const int edge = k / N1, fp = k - edge * N1;
+        double t[4];
+        trace_point<N1>(sU[el], Lm, Lp, edge, fp, t);
+        store4(a.Tout + (e * NFT + k) * 4, t);
+    }
+}
+
+template <int P>
+__global__ void __launch_bounds__(Shape<P>::THREADS)
+k_traces(const double* __restrict__ U, double* __restrict__ T, const double* __restrict__ ops,
+         long long n_elem) {
+    using S = Shape<P>;
+    constexpr int N1 = S::N1, NSP = S::NSP, NFT = S::NFT, TPE = S::TPE, EB = S::EB;
+    __shared__ double sOps[S::NOPS];
+    __shared__ double sU[EB][4][NSP];
+    const int tid = threadIdx.x;
+    for (int i = tid; i < S::NOPS; i += blockDim.x) sOps[i] = ops[i];
+    const int el = tid / TPE, k = tid - el * TPE;
+    const long long e = (long long)blockIdx.x * EB + el;
+    const bool valid = (el < EB) && (e < n_elem);
+    if (valid && k < NSP) {
+        double u[4];
+        load4_nc(U + (e * NSP + k) * 4, u);
+#pragma unroll
+        for (int v = 0; v < 4; ++v) sU[el][v][k] = u[v];
+    }
+    __syncthreads();
+    if (valid && k < NFT) {
+        const int edge = k / N1, fp = k - edge * N1;
+        double t[4];
+        trace_point<N1>(sU[el], sOps + N1 * N1, sOps + N1 * N1 + N1, edge, fp, t);
+        store4(T + (e * NFT + k) * 4, t);
+    }
+}
+
+__global__ void k_reduce_sum(const double* __restrict__ x, int n, double* out) {
+    __shared__ double red[32];
+    double s = 0.0;
+    for (int i = threadIdx.x; i < n; i += blockDim.x) s += x[i];
+    const double t = block_sum(s, red);
+    if (threadIdx.x == 0) out[0] = t;
+}
+
+__global__ void k_dt_partial(const double* __restrict__ U, const double* __restrict__ h,
+                             long long n_states, int n_sp, double g, double cfl, double cf,
+                             double* partial) {
+    __shared__ double red[32];
+    double m = 1e20;
+    for (long long s = (long long)blockIdx.x * blockDim.x + threadIdx.x; s < n_states;
+         s += (long long)gridDim.x * blockDim.x) {
+        double q[4];
+        load4_nc(U + s * 4, q);
+        const double u = q[1] / q[0], v = q[2] / q[0];
+        const double vel = sqrt(u * u + v * v);
+        const double p = fmax(pressure(q, g), 1e-10), rho = fmax(q[0], 1e-10);
+        const double ws = vel + sqrt(g * p / rho);
+        const double dl = cfl * h[s / n_sp] / (ws * cf);
+        if (dl < m) m = dl;
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) m = fmin(m, __shfl_down_sync(0xffffffffu, m, o));
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = m;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double r = 1e20;
+        for (int i = 0; i < (int)((blockDim.x + 31) >> 5); ++i) r = fmin(r, red[i]);
+        partial[blockIdx.x] = r;
+    }
+}
+
+__global__ void k_min_reduce(const double* __restrict__ x, int n, double* out) {
+    __shared__ double red[32];
+    double m = 1e20;
+    for (int i = threadIdx.x; i < n; i += blockDim.x) m = fmin(m, x[i]);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) m = fmin(m, __shfl_down_sync(0xffffffffu, m, o));
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = m;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double r = 1e20;
+        for (int i = 0; i < (int)((blockDim.x + 31) >> 5); ++i) r = fmin(r, red[i]);
+        out[0] = r;
+    }
+}
+
+__global__ void k_check_finite(const double* __restrict__ x, long long n, int* flag) {
+    int bad = 0;
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+         i += (long long)gridDim.x * blockDim.x)
+        if (!isfinite(x[i])) bad = 1;
+    if (__any_sync(0xffffffffu, bad) && (threadIdx.x & 31) == 0) atomicOr(flag, 1);
+}
+
+template <int P>
+cudaError_t launch_stage_t(const StageArgs& a, cudaStream_t s, int* grid_out) {
+    using S = Shape<P>;
+    const long long grid = (a.n_elem + S::EB - 1) / S::EB;
+    if (grid_out) *grid_out = (int)grid;
+    if (grid <= 0) return cudaSuccess;
+    k_compat_stage<P><<<(unsigned)grid, S::THREADS, 0, s>>>(a);
+    return cudaGetLastError();
+}
+
+template <int P>
+cudaError_t launch_traces_t(const double* U, double* T, const double* ops, long long n, cudaStream_t s) {
+    using S = Shape<P>;
+    const long long grid = (n + S::EB - 1) / S::EB;
+    if (grid <= 0) return cudaSuccess;
+    k_traces<P><<<(unsigned)grid, S::THREADS, 0, s>>>(U, T, ops, n);
+    return cudaGetLastError();
+}
+
+template <int P>
+int grid_t(long long n) { return (int)((n + Shape<P>::EB - 1) / Shape<P>::EB); }
+
+}  // namespace
+
+int stage_grid(int P, long long n_elem) {
+    switch (P) {
+        case 1: return grid_t<1>(n_elem);
+        case 2: return grid_t<2>(n_elem);
+        case 3: return grid_t<3>(n_elem);
+        case 4: return grid_t<4>(n_elem);
+        case 5: return grid_t<5>(n_elem);
+        default: return 0;
+    }
+}
+
+cudaError_t launch_compat_stage(int P, const StageArgs& a, cudaStream_t s, int* grid_out) {
+    switch (P) {
+        case 1: return launch_stage_t<1>(a, s, grid_out);
+        case 2: return launch_stage_t<2>(a, s, grid_out);
+        case 3: return launch_stage_t<3>(a, s, grid_out);
+        case 4: return launch_stage_t<4>(a, s, grid_out);
+        case 5: return launch_stage_t<5>(a, s, grid_out);
+        default: return cudaErrorInvalidValue;
+    }
+}
+
+cudaError_t launch_traces(int P, const double* U, double* T, const double* ops, long long n,
+                          cudaStream_t s) {
+    switch (P) {
+        case 1: return launch_traces_t<1>(U, T, ops, n, s);
+        case 2: return launch_traces_t<2>(U, T, ops, n, s);
+        case 3: return launch_traces_t<3>(U, T, ops, n, s);
+        case 4: return launch_traces_t<4>(U, T, ops, n, s);
+        case 5: return launch_traces_t<5>(U, T, ops, n, s);
+        default: return cudaErrorInvalidValue;
+    }
+}
+
+cudaError_t launch_reduce_sum(const double* partials, int n, double* out, cudaStream_t s) {
+    k_reduce_sum<<<1, 1024, 0, s>>>(partials, n, out);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_compute_dt(const double* U, const double* h, long long n_elem, int n_sp,
+                              double gamma, double cfl, int P, double* scratch, int scratch_n,
+                              double* out, cudaStream_t s) {
+    const long long n_states = n_elem * n_sp;
+    int blocks = (int)((n_states + 255) / 256);
+    if (blocks > scratch_n) blocks = scratch_n;
+    if (blocks < 1) blocks = 1;
+    k_dt_partial<<<blocks, 256, 0, s>>>(U, h, n_states, n_sp, gamma, cfl, 2.0 * P + 1.0, scratch);
+    cudaError_t err = cudaGetLastError();
+    if (err != cudaSuccess) return err;
+    k_min_reduce<<<1, 1024, 0, s>>>(scratch, blocks, out);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_check_finite(const double* x, long long n, int* flag, cudaStream_t s) {
+    cudaError_t err = cudaMemsetAsync(flag, 0, sizeof(int), s);
+    if (err != cudaSuccess) return err;
+    long long blocks = (n + 255) / 256;
+    if (blocks > 148 * 16) blocks = 148 * 16;
+    if (blocks < 1) blocks = 1;
+    k_check_finite<<<(unsigned)blocks, 256, 0, s>>>(x, n, flag);
+    return cudaGetLastError();
+}
+
+}  // namespace zj

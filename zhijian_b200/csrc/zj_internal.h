@@ -1,0 +1,86 @@
+// zj_internal.h -- host-side structures shared by the setup code, the
+// kernels' launchers and the C-ABI.  Not installed; the public boundary is
+// include/zj_fr.h.
+#pragma once
+
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "zj_fr.h"
+
+#ifdef __CUDACC__
+#define ZJ_HD __host__ __device__
+#else
+#define ZJ_HD
+#endif
+
+namespace zj {
+
+constexpr int kMaxP = 5;          // reference MAX_POLY_ORDER (types.hpp:27)
+
+// Per-element, per-edge face record read by the stage kernels.  One record
+// per (element, local edge) lets every element evaluate its own four edges
+// without a face-indexed intermediate array.
+struct EdgeRec {
+    int32_t nbr;        // neighbour element, or -1 on a boundary / orphan edge
+    int32_t nbr_edge;   // neighbour's local edge, or the boundary data slot
+    int32_t flags;      // kEdge* bits, boundary type in bits 8..11
+    int32_t pad;
+};
+constexpr int32_t kEdgeRight = 1;    // this element is the face's right side
+constexpr int32_t kEdgeBoundary = 2; // boundary face (ghost state)
+constexpr int32_t kEdgeOrphan = 4;   // edge on no face (non-manifold): no correction
+ZJ_HD inline int32_t edge_bc_type(int32_t flags) { return (flags >> 8) & 0xF; }
+
+// 1D operators of one polynomial order.  The 2D tensor-product operators of
+// the reference (diff_xi, diff_eta, interp, corr_deriv) are exact Kronecker
+// products of these with 0/1 factors, so the kernels apply them
+// sum-factorised with the same terms in the same order.
+struct Operators1D {
+    int P = 0, n1 = 0;
+    std::vector<double> pts, wts;   // Gauss-Legendre nodes / weights
+    std::vector<double> D1;         // [n1][n1]  D1[i][k] = l_k'(x_i)
+    std::vector<double> Lm, Lp;     // l_j(-1), l_j(+1)
+    std::vector<double> gL, gR;     // correction derivatives g_L'(x_j), g_R'(x_j)
+};
+
+// Reference-compatible operator construction (basis.cpp:12-104,169-224,
+// 314-379, 464-613): Radau (DG) correction for every flux type.
+void build_operators_compat(int P, Operators1D& ops);
+// Physics mode: VCJH correction with the c parameter of the flux type.
+void build_operators_vcjh(int P, int flux_type, Operators1D& ops);
+double lagrange_eval(const std::vector<double>& nodes, int j, double x);
+double lagrange_deriv(const std::vector<double>& nodes, int j, double x);
+void gauss_legendre(int n, std::vector<double>& x, std::vector<double>& w);
+
+// Topology and geometry of a quad mesh, built on the host once.
+struct HostMesh {
+    int64_t n_nodes = 0, n_elem = 0, n_faces = 0;
+    int nn = 4, order = 1;                 // nodes per element, geometric order
+    std::vector<double> xy;                // [n_nodes][2]
+    std::vector<int64_t> conn;             // [E][nn]
+    // faces in the reference order (sorted vertex pair)
+    std::vector<int32_t> fle, fll, fre, frl, fbct, ftag, fslot;
+    std::vector<double> fnx, fny, flen;
+    int64_t n_bnd_faces = 0;
+    int64_t n_orphan_edges = 0;
+};
+
+// Builds faces exactly as Mesh::buildFaces + GmshReader::applyBoundaryTags
+// (mesh.cpp:18-83, gmsh_reader.cpp:720-758) and normals as Mesh::faceNormal
+// (mesh.cpp:159-183).  Returns false with msg on a bad mesh.
+bool build_mesh(const zj_mesh_desc* d, const zj_params* p, HostMesh& m, std::string& msg);
+
+// Metric terms at the solution points, [E][n_sp] J and [E][n_sp][4] Jinv =
+// (xi_x, xi_y, eta_x, eta_y), as fr_solver.cpp:85-129.
+bool build_metrics(const HostMesh& m, const Operators1D& ops, std::vector<double>& J,
+                   std::vector<double>& Jinv, std::string& msg);
+void sp_coords(const HostMesh& m, const Operators1D& ops, std::vector<double>& xy);
+void element_areas(const HostMesh& m, std::vector<double>& area);
+
+// Boundary data, 8 doubles per boundary slot (fr_solver.cpp:432-482).
+void build_bc_data(const HostMesh& m, const zj_params* p, std::vector<double>& bc);
+void build_edge_records(const HostMesh& m, std::vector<EdgeRec>& rec, std::vector<double>& nrm);
+
+}  // namespace zj

@@ -1,0 +1,50 @@
+// zj_kernels.h -- launch interface between the C-ABI and the CUDA kernels.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "zj_internal.h"
+
+namespace zj {
+
+// Arguments of one fused residual / RK-stage launch.  Device pointers.
+struct StageArgs {
+    const double* U;        // stage input state, AoS [E][n_sp][4]
+    const double* U0;       // RK base state (stages 2, 3)
+    double* Uout;           // stage output state
+    const double* Tin;      // traces of U, [E][4 edges][n1][4]
+    double* Tout;           // traces of Uout
+    double* R;              // residual output (stage 0 only)
+    const double* Jinv;     // [E][n_sp][4] = (xi_x, xi_y, eta_x, eta_y)
+    const double* J;        // [E][n_sp]
+    const EdgeRec* edges;   // [E][4]
+    const double4* enrm;    // [E][4] = (face nx, face ny, edge length, 0)
+    const double* bc;       // [slots][8]
+    const double* ops;      // packed 1D operators, see OpsLayout
+    const double* dt;       // device scalar: step size
+    double* partials;       // [grid] per-CTA sum of R^2 (stage 3 and stage 0)
+    long long n_elem;
+    double gamma;
+    int stage;              // 0: residual only; 1..3: SSP-RK3 stage
+};
+
+// Packed operator block: D1[n1*n1], Lm[n1], Lp[n1], gL[n1], gR[n1].
+inline int ops_size(int n1) { return n1 * n1 + 4 * n1; }
+void pack_ops(const Operators1D& o, std::vector<double>& out);
+
+// Compat-mode FP64 launches (reference residual semantics).
+cudaError_t launch_compat_stage(int P, const StageArgs& a, cudaStream_t s, int* grid_out);
+cudaError_t launch_traces(int P, const double* U, double* T, const double* ops,
+                          long long n_elem, cudaStream_t s);
+int stage_grid(int P, long long n_elem);
+
+// Deterministic reduction of per-CTA partial sums into out[0].
+cudaError_t launch_reduce_sum(const double* partials, int n, double* out, cudaStream_t s);
+// out[0] = min over states of CFL*h/(ws*(2P+1)); h per element.
+cudaError_t launch_compute_dt(const double* U, const double* h, long long n_elem, int n_sp,
+                              double gamma, double cfl, int P, double* scratch, int scratch_n,
+                              double* out, cudaStream_t s);
+// flag[0] = 1 if any value of x[0..n) is NaN/Inf.
+cudaError_t launch_check_finite(const double* x, long long n, int* flag, cudaStream_t s);
+
+}  // namespace zj

@@ -1,0 +1,177 @@
+"""Python view of the C-ABI with the reference's FRSolver method names
+(include/solver/fr_solver.hpp:77-180): initialize, setInitialCondition,
+advance, computeTimeStep, computeResidual, copyToHost, copyToDevice.
+
+Everything runs in libzj_fr.so; this module only marshals arguments.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import _lib as L
+from .meshgen import QuadMesh
+
+
+def make_params(poly_order=3, gamma=1.4, rho_inf=1.0, p_inf=1.0 / 1.4, Mach=0.5, AoA=0.0,
+                flux_type="HU", riemann="Rusanov", CFL=0.5, viscous=False, Re=1000.0,
+                Pr=0.72, compat=True, precision="fp64", bcs=(), config_text=None):
+    """A zj_params with the reference defaults, then the given values.
+    bcs: iterable of (tag, type name[, p_static]).  config_text is parsed
+    with the reference grammar after the keyword values."""
+    p = L.Params()
+    lib = L.lib()
+    lib.zj_params_default(C.byref(p))
+    p.poly_order = poly_order
+    p.gamma = gamma
+    p.rho_inf = rho_inf
+    p.p_inf = p_inf
+    p.Mach = Mach
+    p.AoA = AoA
+    p.flux_type = L.FLUX_TYPES[flux_type] if isinstance(flux_type, str) else int(flux_type)
+    p.riemann = L.RIEMANN[riemann] if isinstance(riemann, str) else int(riemann)
+    p.CFL = CFL
+    p.viscous = int(bool(viscous))
+    p.Re = Re
+    p.Pr = Pr
+    p.compat = int(bool(compat))
+    p.precision = L.FP64 if precision == "fp64" else L.MIXED
+    p.n_bc = 0
+    for b in bcs:
+        tag, name = b[0], b[1]
+        s = p.bc[p.n_bc]
+        s.tag = int(tag)
+        s.type = L.BC_TYPES[name] if isinstance(name, str) else int(name)
+        s.p_static = float(b[2]) if len(b) > 2 else 0.0
+        s.dir_x, s.dir_y = 1.0, 0.0
+        p.n_bc += 1
+    if config_text is not None:
+        L.check(lib.zj_params_parse_string(config_text.encode(), C.byref(p)))
+    return p
+
+
+def _dptr(a: np.ndarray):
+    return a.ctypes.data_as(C.POINTER(C.c_double))
+
+
+class FRSolver:
+    """One zj_solver handle."""
+
+    def __init__(self, mesh: QuadMesh, params: L.Params):
+        lib = L.lib()
+        self._keep = []
+        xy = np.ascontiguousarray(mesh.xy, dtype=np.float64)
+        conn = np.ascontiguousarray(mesh.conn, dtype=np.int64)
+        ne, nn = conn.shape
+        et = np.ones(ne, dtype=np.int32)
+        eo = np.full(ne, {4: 1, 9: 2, 25: 4}[nn], dtype=np.int32)
+        off = (np.arange(ne + 1, dtype=np.int64) * nn)
+        bnd = np.ascontiguousarray(mesh.bnd, dtype=np.int64)
+        d = L.MeshDesc()
+        d.n_nodes = xy.shape[0]
+        d.xy = _dptr(xy)
+        d.n_elem = ne
+        d.elem_type = et.ctypes.data_as(C.POINTER(C.c_int32))
+        d.elem_order = eo.ctypes.data_as(C.POINTER(C.c_int32))
+        d.conn_offsets = off.ctypes.data_as(C.POINTER(C.c_int64))
+        d.conn = conn.ctypes.data_as(C.POINTER(C.c_int64))
+        d.n_bnd_edges = bnd.shape[0]
+        d.bnd_edges = bnd.ctypes.data_as(C.POINTER(C.c_int64))
+        h = C.c_void_p()
+        L.check(lib.zj_solver_create(C.byref(d), C.byref(params), C.byref(h)))
+        self.h = h
+        self.params = params
+        self.n_elem = lib.zj_num_elements(h)
+        self.n_sp = lib.zj_num_solution_points(h)
+        self.n_faces = lib.zj_num_faces(h)
+        self.shape = (self.n_elem, self.n_sp, 4)
+        self._host = np.zeros(self.shape)
+
+    def close(self):
+        if getattr(self, "h", None):
+            L.lib().zj_solver_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def _ck(self, code):
+        L.check(code, self.h)
+
+    # -- reference method names ------------------------------------------
+    def solution_point_coords(self) -> np.ndarray:
+        xy = np.zeros((self.n_elem, self.n_sp, 2))
+        self._ck(L.lib().zj_solution_point_coords(self.h, _dptr(xy)))
+        return xy
+
+    def setInitialCondition(self, ic):
+        """ic maps an [..., 2] coordinate array to an [..., 4] state array."""
+        self.copyToDevice(np.asarray(ic(self.solution_point_coords()), dtype=np.float64))
+
+    def copyToDevice(self, U: np.ndarray):
+        U = np.ascontiguousarray(U, dtype=np.float64).reshape(self.shape)
+        self._ck(L.lib().zj_set_state(self.h, _dptr(U)))
+
+    def copyToHost(self, out: np.ndarray = None) -> np.ndarray:
+        """The current state; into ``out`` (C-contiguous float64) when given."""
+        if out is None:
+            out = np.empty(self.shape)
+        assert out.dtype == np.float64 and out.flags.c_contiguous and out.size == np.prod(self.shape)
+        self._ck(L.lib().zj_get_state(self.h, _dptr(out)))
+        return out
+
+    solution = copyToHost
+
+    def advance(self, dt: float, nsteps: int = 1, sync: bool = True):
+        self._ck(L.lib().zj_step(self.h, float(dt), int(nsteps)))
+        if sync:
+            self.synchronize()
+
+    def synchronize(self):
+        self._ck(L.lib().zj_synchronize(self.h))
+
+    def computeTimeStep(self) -> float:
+        v = C.c_double()
+        self._ck(L.lib().zj_compute_dt(self.h, C.byref(v)))
+        return v.value
+
+    def computeResidual(self) -> float:
+        v = C.c_double()
+        self._ck(L.lib().zj_residual_norm(self.h, C.byref(v)))
+        return v.value
+
+    def check_state(self):
+        self._ck(L.lib().zj_check_state(self.h))
+
+    # -- residual entry points ------------------------------------------
+    def rhs(self, U: np.ndarray) -> np.ndarray:
+        """R(U) through host buffers."""
+        U = np.ascontiguousarray(U, dtype=np.float64).reshape(self.shape)
+        R = np.empty(self.shape)
+        self._ck(L.lib().zj_rhs_host(self.h, _dptr(U), _dptr(R)))
+        return R
+
+    def rhs_device(self, U_ptr: int, R_ptr: int):
+        """R(U) on device pointers (e.g. torch tensors' data_ptr())."""
+        self._ck(L.lib().zj_rhs(self.h, C.c_void_p(U_ptr), C.c_void_p(R_ptr)))
+
+    def set_stream(self, stream_ptr: int):
+        self._ck(L.lib().zj_set_stream(self.h, C.c_void_p(stream_ptr)))
+
+    @property
+    def time(self) -> float:
+        return L.lib().zj_time(self.h)
+
+    @property
+    def iteration(self) -> int:
+        return L.lib().zj_iteration(self.h)
