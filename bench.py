@@ -224,17 +224,16 @@ def run_ours(args):
     from zhijian_b200 import meshgen as M
     mesh = build_case()
     s = make_solver(mesh)
-    stream = torch.cuda.current_stream(dev)
+    stream = torch.cuda.Stream(dev)        # a real stream: events and kernels share it
     s.set_stream(stream.cuda_stream)
     U0 = M.taylor_green(s.solution_point_coords())
     s.copyToDevice(U0)
     dof = s.n_elem * s.n_sp
+    sampler = ClockSampler(local)   # sampled from warm-up through the timed region
+    sampler.start()
+    time.sleep(0.2)
     s.advance(DT, args.warmup)
     barrier_sync()
-
-    sampler = ClockSampler(local)
-    sampler.start()
-    time.sleep(0.3)
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     barrier_sync()
     e0.record(stream)
@@ -303,8 +302,8 @@ def run_ours(args):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=300)
-    ap.add_argument("--warmup", type=int, default=10)
+    ap.add_argument("--steps", type=int, default=1000)
+    ap.add_argument("--warmup", type=int, default=20)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=10.0)

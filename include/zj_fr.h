@@ -168,8 +168,10 @@ zj_status zj_check_state(zj_solver* s);
 double zj_time(const zj_solver* s);
 int zj_iteration(const zj_solver* s);
 
-/* Stream: the handle owns a stream; a caller stream may be set instead
- * (NULL restores the owned one).  cudaStream_t passed as void*. */
+/* Stream: the handle creates its own non-blocking stream and uses it until a
+ * caller stream is set; NULL selects the CUDA legacy default stream.  To go
+ * back to the handle's own stream pass the value zj_get_stream returned before
+ * the first zj_set_stream.  cudaStream_t passed as void*. */
 zj_status zj_set_stream(zj_solver* s, void* stream);
 void* zj_get_stream(const zj_solver* s);
 

@@ -53,11 +53,11 @@ def case_defs():
                                   state=("vortex", 1.0, 1.0), dt=0.01, nsteps=3)
     cases["vortex_dim_p3"] = dict(mesh=vm, tags=None, P=3,
                                   prm=(RHO_S, P_S / GAMMA, 0.5, 0.0),
-                                  state=("vortex", RHO_S, P_S), dt=1e-4, nsteps=5)
+                                  state=("vortex", RHO_S, P_S), dt=1e-6, nsteps=5)
     for P in range(1, 6):
         cases[f"mixed_p{P}"] = dict(mesh=mixed_mesh(), tags=mixed_tags(0.9e5), P=P,
                                     prm=(1.2, 1.0e5, 0.4, 10.0),
-                                    state=("random", 1.2, 1.0e5, 11 + P), dt=2e-5, nsteps=2)
+                                    state=("random", 1.2, 1.0e5, 11 + P), dt=1e-8, nsteps=3)
     cases["tgv16_p3"] = dict(mesh=M.tgv_mesh(16, seed=1), tags=None, P=3,
                              prm=(1.0, 1.0 / (GAMMA * 0.09), 0.3, 0.0), state=("tgv",),
                              dt=1e-3, nsteps=2)

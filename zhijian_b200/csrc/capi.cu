@@ -249,7 +249,7 @@ zj_status zj_solution_point_coords(const zj_solver* s, double* xy) {
 
 zj_status zj_set_stream(zj_solver* s, void* stream) {
     if (!s) return ZJ_ERR_ARG;
-    s->stream = stream ? static_cast<cudaStream_t>(stream) : s->own;
+    s->stream = static_cast<cudaStream_t>(stream);
     return ZJ_OK;
 }
 

@@ -21,6 +21,7 @@
 #include <cuda_runtime.h>
 
 #include "zj_kernels.h"
+#include "zj_math.h"
 
 namespace zj {
 
@@ -50,19 +51,83 @@ struct Shape {
 };
 
 // ---------------------------------------------------------------- physics --
+//
+// FP64 division and square root run on the XU pipe, which these kernels
+// saturate first.  The reference divides by rho up to ten times per state;
+// here every state takes one reciprocal and multiplies, and reciprocals and
+// square roots come from zj_math.h (Newton-Raphson on the FMA pipe, within
+// 2 ulp).  Each quotient moves by a few ulp; the residual stays within 1e-12
+// of the reference's.
 
-// IdealGas::pressure (euler.hpp:16-23)
-__device__ __forceinline__ double pressure(const double* U, double g) {
-    const double rho = U[0], u = U[1] / rho, v = U[2] / rho, E = U[3] / rho;
-    const double ke = 0.5 * (u * u + v * v);
-    return (g - 1.0) * rho * (E - ke);
+// 1/x: Newton-Raphson for positive normal x, IEEE division otherwise (zero,
+// negative or non-finite densities, which the reference also divides by).
+__device__ __forceinline__ double rcp_any(double x) {
+    return (x > 1e-300 && x < 1e300) ? zj_rcp(x) : 1.0 / x;
 }
 
-// IdealGas::fluxX / fluxY (euler.hpp:101-129)
-__device__ __forceinline__ void flux_xy(const double* U, double g, double* F, double* G) {
-    const double rho = U[0], u = U[1] / rho, v = U[2] / rho, p = pressure(U, g);
-    F[0] = U[1]; F[1] = U[1] * u + p; F[2] = U[1] * v; F[3] = (U[3] + p) * u;
-    G[0] = U[2]; G[1] = U[2] * u; G[2] = U[2] * v + p; G[3] = (U[3] + p) * v;
+// Primitive quantities of one trace state in the form the reference's
+// Rusanov flux uses them (kernels.cu:601-630): floored density and pressure,
+// velocities, total enthalpy and the wave speed |u| + c.  praw is the
+// pressure of IdealGas::pressure (euler.hpp:16-23) from the unfloored
+// density, used by the interior flux and the wall ghost states; it differs
+// from the floored form only when the trace density is below 1e-10.
+struct Prim {
+    double q[4];
+    double rho, u, v, p, s, H, praw;
+};
+
+__device__ __forceinline__ void raw_velocity(const Prim& w, double& u, double& v) {
+    if (w.q[0] >= 1e-10) { u = w.u; v = w.v; }
+    else { const double ir = 1.0 / w.q[0]; u = w.q[1] * ir; v = w.q[2] * ir; }
+}
+
+__device__ __forceinline__ void make_prim(const double* q, double g, Prim& w) {
+    w.q[0] = q[0]; w.q[1] = q[1]; w.q[2] = q[2]; w.q[3] = q[3];
+    w.rho = fmax(q[0], 1e-10);
+    const double ir = rcp_any(w.rho);
+    w.u = q[1] * ir;
+    w.v = q[2] * ir;
+    const double E = q[3] * ir;
+    const double pf = (g - 1.0) * w.rho * (E - 0.5 * (w.u * w.u + w.v * w.v));
+    if (q[0] >= 1e-10) {
+        w.praw = pf;
+    } else {
+        const double irr = 1.0 / q[0];
+        const double ur = q[1] * irr, vr = q[2] * irr;
+        w.praw = (g - 1.0) * q[0] * (q[3] * irr - 0.5 * (ur * ur + vr * vr));
+    }
+    w.p = fmax(pf, 1e-10);
+    const double c = zj_sqrt(fmax(g * w.p * ir, 1e-10));
+    w.s = zj_sqrt(w.u * w.u + w.v * w.v) + c;
+    w.H = E + w.p * ir;
+}
+
+// Normal component of the Euler flux (IdealGas::fluxX/fluxY, euler.hpp:101-129).
+__device__ __forceinline__ void flux_normal(const Prim& w, double nx, double ny, double* Fn) {
+    const double pr = w.praw;
+    double u, v;
+    raw_velocity(w, u, v);
+    Fn[0] = w.q[1] * nx + w.q[2] * ny;
+    Fn[1] = (w.q[1] * u + pr) * nx + (w.q[2] * u) * ny;
+    Fn[2] = (w.q[1] * v) * nx + (w.q[2] * v + pr) * ny;
+    Fn[3] = ((w.q[3] + pr) * u) * nx + ((w.q[3] + pr) * v) * ny;
+}
+
+// The reference's hard-coded Rusanov with floors (kernels.cu:597-669):
+// s_max from the full speed |u| + c, NaN/Inf -> 0.
+__device__ __forceinline__ void rusanov_compat(const Prim& L, const Prim& R, double nx, double ny,
+                                               double* F) {
+    const double vnL = L.u * nx + L.v * ny, vnR = R.u * nx + R.v * ny;
+    const double smax = fmax(L.s, R.s);
+    const double FL[4] = {L.rho * vnL, L.rho * L.u * vnL + L.p * nx, L.rho * L.v * vnL + L.p * ny,
+                          L.rho * L.H * vnL};
+    const double FR[4] = {R.rho * vnR, R.rho * R.u * vnR + R.p * nx, R.rho * R.v * vnR + R.p * ny,
+                          R.rho * R.H * vnR};
+#pragma unroll
+    for (int v = 0; v < 4; ++v) {
+        const double f = 0.5 * (FL[v] + FR[v]) - 0.5 * smax * (R.q[v] - L.q[v]);
+        F[v] = isfinite(f) ? f : 0.0;
+    }
 }
 
 __device__ __forceinline__ void prim2cons(double rho, double u, double v, double p, double g,
@@ -71,27 +136,24 @@ __device__ __forceinline__ void prim2cons(double rho, double u, double v, double
     U[3] = p / (g - 1.0) + 0.5 * rho * (u * u + v * v);
 }
 
-// computeGhostState (kernels.cu:453-525)
-__device__ void ghost_compat(const double* Ui, double nx, double ny, int bct,
+// computeGhostState (kernels.cu:453-525), from the interior primitives.
+__device__ void ghost_compat(const Prim& w, double nx, double ny, int bct,
                              const double* __restrict__ bcd, double g, double* Ug) {
     switch (bct) {
         case ZJ_BC_WALL: case ZJ_BC_SLIPWALL: case ZJ_BC_SYMMETRY: {
-            const double rho = Ui[0], u = Ui[1] / rho, v = Ui[2] / rho;
-            const double p = pressure(Ui, g);
+            double u, v;
+            raw_velocity(w, u, v);
             const double vn = u * nx + v * ny;
-            prim2cons(rho, u - 2.0 * vn * nx, v - 2.0 * vn * ny, p, g, Ug);
+            prim2cons(w.q[0], u - 2.0 * vn * nx, v - 2.0 * vn * ny, w.praw, g, Ug);
             break;
         }
         case ZJ_BC_FARFIELD: {
             const double rho_inf = bcd[0], u_inf = bcd[1], v_inf = bcd[2], p_inf = bcd[3];
-            const double rho_i = fmax(Ui[0], 1e-10);
-            const double u_i = Ui[1] / rho_i, v_i = Ui[2] / rho_i;
-            const double p_i = fmax((g - 1.0) * (Ui[3] - 0.5 * rho_i * (u_i * u_i + v_i * v_i)), 1e-10);
             const double vn_inf = u_inf * nx + v_inf * ny;
             double rb, ub, vb;
             if (vn_inf > 0) { rb = rho_inf; ub = u_inf; vb = v_inf; }
-            else { rb = rho_i; ub = u_i; vb = v_i; }
-            double pb = 0.5 * (p_inf + p_i);
+            else { rb = w.rho; ub = w.u; vb = w.v; }
+            double pb = 0.5 * (p_inf + w.p);
             rb = fmax(fmin(rb, 100.0), 0.01);
             ub = fmax(fmin(ub, 1000.0), -1000.0);
             vb = fmax(fmin(vb, 1000.0), -1000.0);
@@ -100,46 +162,34 @@ __device__ void ghost_compat(const double* Ui, double nx, double ny, int bct,
             break;
         }
         case ZJ_BC_OUTFLOW: {
-            const double rho = Ui[0], u = Ui[1] / rho, v = Ui[2] / rho;
-            prim2cons(rho, u, v, bcd[0], g, Ug);
+            double u, v;
+            raw_velocity(w, u, v);
+            prim2cons(w.q[0], u, v, bcd[0], g, Ug);
             break;
         }
         default:
-            Ug[0] = Ui[0]; Ug[1] = Ui[1]; Ug[2] = Ui[2]; Ug[3] = Ui[3];
+            Ug[0] = w.q[0]; Ug[1] = w.q[1]; Ug[2] = w.q[2]; Ug[3] = w.q[3];
     }
 }
 
-// The reference's hard-coded Rusanov with floors (kernels.cu:597-669).
-__device__ void rusanov_compat(const double* UL, const double* UR, double nx, double ny,
-                               double g, double* F) {
-    const double rhoL = fmax(UL[0], 1e-10), rhoR = fmax(UR[0], 1e-10);
-    const double uL = UL[1] / rhoL, vL = UL[2] / rhoL, uR = UR[1] / rhoR, vR = UR[2] / rhoR;
-    const double EL = UL[3] / rhoL, ER = UR[3] / rhoR;
-    const double pL = fmax((g - 1.0) * rhoL * (EL - 0.5 * (uL * uL + vL * vL)), 1e-10);
-    const double pR = fmax((g - 1.0) * rhoR * (ER - 0.5 * (uR * uR + vR * vR)), 1e-10);
-    const double cL = sqrt(fmax(g * pL / rhoL, 1e-10)), cR = sqrt(fmax(g * pR / rhoR, 1e-10));
-    const double vnL = uL * nx + vL * ny, vnR = uR * nx + vR * ny;
-    const double smax = fmax(sqrt(uL * uL + vL * vL) + cL, sqrt(uR * uR + vR * vR) + cR);
-    const double HL = EL + pL / rhoL, HR = ER + pR / rhoR;
-    const double FL[4] = {rhoL * vnL, rhoL * uL * vnL + pL * nx, rhoL * vL * vnL + pL * ny, rhoL * HL * vnL};
-    const double FR[4] = {rhoR * vnR, rhoR * uR * vnR + pR * nx, rhoR * vR * vnR + pR * ny, rhoR * HR * vnR};
-#pragma unroll
-    for (int v = 0; v < 4; ++v) {
-        double f = 0.5 * (FL[v] + FR[v]) - 0.5 * smax * (UR[v] - UL[v]);
-        F[v] = isfinite(f) ? f : 0.0;
-    }
+// IdealGas::pressure (euler.hpp:16-23)
+__device__ __forceinline__ double pressure(const double* U, double g) {
+    const double rho = U[0], u = U[1] / rho, v = U[2] / rho, E = U[3] / rho;
+    return (g - 1.0) * rho * (E - 0.5 * (u * u + v * v));
 }
 
-// enforcePositivityKernel (kernels.cu:1236-1288): gamma fixed at 1.4.
+// enforcePositivityKernel (kernels.cu:1236-1288): gamma fixed at 1.4; the
+// clamped density is >= 0.01, so its 1e-10 floor never binds.
 __device__ __forceinline__ void positivity(double* U) {
     const double rn = fmax(0.01, fmin(100.0, U[0]));
-    double u = U[1] / fmax(rn, 1e-10), v = U[2] / fmax(rn, 1e-10);
-    const double vm = sqrt(u * u + v * v);
+    const double ir = zj_rcp(rn);   // rn is in [0.01, 100]
+    double u = U[1] * ir, v = U[2] * ir;
+    const double vm = zj_sqrt(u * u + v * v);
     if (vm > 2000.0) { const double s = 2000.0 / vm; u *= s; v *= s; }
     const double ke = 0.5 * rn * (u * u + v * v);
     double p = (1.4 - 1.0) * (U[3] - ke);
     p = fmax(100.0, fmin(1e8, p));
-    U[0] = rn; U[1] = rn * u; U[2] = rn * v; U[3] = p / (1.4 - 1.0) + ke;
+    U[0] = rn; U[1] = rn * u; U[2] = rn * v; U[3] = p * (1.0 / (1.4 - 1.0)) + ke;
 }
 
 __device__ __forceinline__ void load4(const double* p, double* v) {
@@ -202,8 +252,11 @@ __device__ double block_sum(double x, double* red) {
 
 // -------------------------------------------------------------- kernels --
 
+// Minimum resident CTAs per SM requested from the register allocator.
+constexpr int kMinBlocks = 4;
+
 template <int P>
-__global__ void __launch_bounds__(Shape<P>::THREADS)
+__global__ void __launch_bounds__(Shape<P>::THREADS, kMinBlocks)
 k_compat_stage(const StageArgs a) {
     using S = Shape<P>;
     constexpr int N1 = S::N1, NSP = S::NSP, NFT = S::NFT, TPE = S::TPE, EB = S::EB;
@@ -211,7 +264,14 @@ k_compat_stage(const StageArgs a) {
     __shared__ double sF[EB][4][NSP];
     __shared__ double sG[EB][4][NSP];
     __shared__ double sD[EB][NFT][4];
-    __shared__ double sU[EB][4][NSP];
+    // The trace primitives are dead after phase B and the new state is first
+    // written in phase C, after a barrier: one buffer serves both.
+    __shared__ union {
+        Prim w[EB][NFT];
+        double u[EB][4][NSP];
+    } sBW;
+    auto& sW = sBW.w;
+    auto& sU = sBW.u;
     __shared__ double sRed[32];
 
     const int tid = threadIdx.x;
@@ -227,20 +287,24 @@ k_compat_stage(const StageArgs a) {
     const bool valid = (el < EB) && (e < a.n_elem);
     const double g = a.gamma;
 
-    // ---- A: fluxes at the solution points
-    double u[4], ji[4], u0[4];
+    // ---- A: Euler fluxes at the solution points; own trace primitives
+    double u[4];
     if (valid && k < NSP) {
-        const long long idx = e * NSP + k;
-        load4(a.U + idx * 4, u);
-        double F[4], G[4];
-        flux_xy(u, g, F, G);
-#pragma unroll
-        for (int v = 0; v < 4; ++v) { sF[el][v][k] = F[v]; sG[el][v][k] = G[v]; }
-        load4_nc(a.Jinv + idx * 4, ji);
-        if (a.stage >= 2) load4(a.U0 + idx * 4, u0);
-        else { u0[0] = u[0]; u0[1] = u[1]; u0[2] = u[2]; u0[3] = u[3]; }
+        load4(a.U + (e * NSP + k) * 4, u);
+        const double ir = rcp_any(u[0]);
+        const double uu = u[1] * ir, vv = u[2] * ir, E = u[3] * ir;
+        const double p = (g - 1.0) * u[0] * (E - 0.5 * (uu * uu + vv * vv));
+        sF[el][0][k] = u[1]; sF[el][1][k] = u[1] * uu + p;
+        sF[el][2][k] = u[1] * vv; sF[el][3][k] = (u[3] + p) * uu;
+        sG[el][0][k] = u[2]; sG[el][1][k] = u[2] * uu;
+        sG[el][2][k] = u[2] * vv + p; sG[el][3][k] = (u[3] + p) * vv;
     }
-    __syncthreads();   // sOps ready
+    if (valid && k < NFT) {
+        double q[4];
+        load4_nc(a.Tin + (e * NFT + k) * 4, q);
+        make_prim(q, g, sW[el][k]);
+    }
+    __syncthreads();   // sOps, sF, sG, sW ready
 
     // ---- B: interface fluxes, this element's side
     if (valid && k < NFT) {
@@ -250,30 +314,31 @@ k_compat_stage(const StageArgs a) {
         const double nx = nr.x, ny = nr.y;
         double Fd[4] = {0.0, 0.0, 0.0, 0.0};
         if (!(r.flags & kEdgeOrphan)) {
-            const double* own = a.Tin + (e * 4 + edge) * N1 * 4;
-            double UL[4], UR[4], Fc[4], Fx[4], Fy[4], Uo[4];
+            Prim X;
+            double Fc[4], Fi[4];
             if (!(r.flags & kEdgeRight)) {
-                load4_nc(own + fp * 4, UL);
-                if (r.nbr >= 0) {
-                    load4_nc(a.Tin + ((long long)r.nbr * 4 + r.nbr_edge) * N1 * 4 + (N1 - 1 - fp) * 4, UR);
-                } else {
-                    ghost_compat(UL, nx, ny, edge_bc_type(r.flags), a.bc + (long long)r.nbr_edge * 8, g, UR);
-                }
-                rusanov_compat(UL, UR, nx, ny, g, Fc);
-                flux_xy(UL, g, Fx, Fy);
+                const Prim& L = sW[el][k];
+                double q[4];
+                if (r.nbr >= 0)
+                    load4_nc(a.Tin + (((long long)r.nbr * 4 + r.nbr_edge) * N1 + (N1 - 1 - fp)) * 4, q);
+                else
+                    ghost_compat(L, nx, ny, edge_bc_type(r.flags), a.bc + (long long)r.nbr_edge * 8, g, q);
+                make_prim(q, g, X);
+                rusanov_compat(L, X, nx, ny, Fc);
+                flux_normal(L, nx, ny, Fi);
 #pragma unroll
-                for (int v = 0; v < 4; ++v) Fd[v] = Fc[v] - (Fx[v] * nx + Fy[v] * ny);
+                for (int v = 0; v < 4; ++v) Fd[v] = Fc[v] - Fi[v];
             } else {
                 // Right side: the common flux at fp pairs the left trace at fp
                 // with this trace at N1-1-fp (kernels.cu:577), while the
                 // interior flux uses this trace at fp (kernels.cu:402-425).
-                load4_nc(a.Tin + ((long long)r.nbr * 4 + r.nbr_edge) * N1 * 4 + fp * 4, UL);
-                load4_nc(own + (N1 - 1 - fp) * 4, UR);
-                rusanov_compat(UL, UR, nx, ny, g, Fc);
-                load4_nc(own + fp * 4, Uo);
-                flux_xy(Uo, g, Fx, Fy);
+                double q[4];
+                load4_nc(a.Tin + (((long long)r.nbr * 4 + r.nbr_edge) * N1 + fp) * 4, q);
+                make_prim(q, g, X);
+                rusanov_compat(X, sW[el][edge * N1 + (N1 - 1 - fp)], nx, ny, Fc);
+                flux_normal(sW[el][k], nx, ny, Fi);
 #pragma unroll
-                for (int v = 0; v < 4; ++v) Fd[v] = -Fc[v] + (Fx[v] * nx + Fy[v] * ny);
+                for (int v = 0; v < 4; ++v) Fd[v] = -Fc[v] + Fi[v];
             }
         }
 #pragma unroll
@@ -286,6 +351,9 @@ k_compat_stage(const StageArgs a) {
     if (valid && k < NSP) {
         const int i = k % N1, j = k / N1;   // xi index, eta index
         const long long idx = e * NSP + k;
+        double ji[4], u0[4];
+        load4_nc(a.Jinv + idx * 4, ji);
+        if (a.stage >= 2) load4(a.U0 + idx * 4, u0);
         double res[4];
 #pragma unroll
         for (int v = 0; v < 4; ++v) {
@@ -317,7 +385,7 @@ k_compat_stage(const StageArgs a) {
             double uo[4];
 #pragma unroll
             for (int v = 0; v < 4; ++v) {
-                if (a.stage == 1) uo[v] = u0[v] + dt * res[v];
+                if (a.stage == 1) uo[v] = u[v] + dt * res[v];
                 else if (a.stage == 2) uo[v] = 0.75 * u0[v] + 0.25 * u[v] + 0.25 * dt * res[v];
                 else uo[v] = (1.0 / 3.0) * u0[v] + (2.0 / 3.0) * u[v] + (2.0 / 3.0) * dt * res[v];
             }
@@ -439,6 +507,13 @@ cudaError_t launch_stage_t(const StageArgs& a, cudaStream_t s, int* grid_out) {
     const long long grid = (a.n_elem + S::EB - 1) / S::EB;
     if (grid_out) *grid_out = (int)grid;
     if (grid <= 0) return cudaSuccess;
+    // Prefer the largest shared-memory carveout so kMinBlocks CTAs fit per SM.
+    static bool carveout_set = false;
+    if (!carveout_set) {
+        cudaFuncSetAttribute(k_compat_stage<P>, cudaFuncAttributePreferredSharedMemoryCarveout,
+                             cudaSharedmemCarveoutMaxShared);
+        carveout_set = true;
+    }
     k_compat_stage<P><<<(unsigned)grid, S::THREADS, 0, s>>>(a);
     return cudaGetLastError();
 }
