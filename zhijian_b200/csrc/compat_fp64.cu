@@ -48,6 +48,15 @@ struct Shape {
     static constexpr int EB = (256 / TPE) > 0 ? (256 / TPE) : 1;
     static constexpr int THREADS = EB * TPE;
     static constexpr int NOPS = N1 * N1 + 4 * N1;
+    // Shared-memory layout of per-element fields (doubles): [var][eta row][xi]
+    // with rows padded to an even length so every row starts 16-byte aligned
+    // (vector loads), and a per-element stride of 6 mod 16 so the elements
+    // that share a warp start on different banks.  Flux differences use
+    // [flux point][var] with a per-element stride of 2 mod 16.
+    static constexpr int RS = (N1 + 1) & ~1;
+    static constexpr int VS = N1 * RS;
+    static constexpr int FS = 4 * VS + (6 - (4 * VS) % 16 + 16) % 16;
+    static constexpr int DS = 4 * NFT + 2;
 };
 
 // ---------------------------------------------------------------- physics --
@@ -113,19 +122,23 @@ __device__ __forceinline__ void flux_normal(const Prim& w, double nx, double ny,
     Fn[3] = ((w.q[3] + pr) * u) * nx + ((w.q[3] + pr) * v) * ny;
 }
 
-// The reference's hard-coded Rusanov with floors (kernels.cu:597-669):
-// s_max from the full speed |u| + c, NaN/Inf -> 0.
-__device__ __forceinline__ void rusanov_compat(const Prim& L, const Prim& R, double nx, double ny,
-                                               double* F) {
-    const double vnL = L.u * nx + L.v * ny, vnR = R.u * nx + R.v * ny;
-    const double smax = fmax(L.s, R.s);
-    const double FL[4] = {L.rho * vnL, L.rho * L.u * vnL + L.p * nx, L.rho * L.v * vnL + L.p * ny,
-                          L.rho * L.H * vnL};
-    const double FR[4] = {R.rho * vnR, R.rho * R.u * vnR + R.p * nx, R.rho * R.v * vnR + R.p * ny,
-                          R.rho * R.H * vnR};
+// The reference's hard-coded Rusanov flux with floors (kernels.cu:597-669):
+// s_max = max(|u|+c) over both sides, F = (F_L+F_R)/2 - s_max (U_R-U_L)/2,
+// NaN/Inf -> 0.  Evaluated for (L, R) = (O, X), or (X, O) when swap: the
+// central part and s_max are symmetric and IEEE addition commutes, while
+// U_R - U_L only changes sign exactly, so both orders need one code path.
+__device__ __forceinline__ void rusanov_pair(const Prim& O, const Prim& X, bool swap, double nx,
+                                             double ny, double* F) {
+    const double vnO = O.u * nx + O.v * ny, vnX = X.u * nx + X.v * ny;
+    const double smax = fmax(O.s, X.s);
+    const double FO[4] = {O.rho * vnO, O.rho * O.u * vnO + O.p * nx, O.rho * O.v * vnO + O.p * ny,
+                          O.rho * O.H * vnO};
+    const double FX[4] = {X.rho * vnX, X.rho * X.u * vnX + X.p * nx, X.rho * X.v * vnX + X.p * ny,
+                          X.rho * X.H * vnX};
 #pragma unroll
     for (int v = 0; v < 4; ++v) {
-        const double f = 0.5 * (FL[v] + FR[v]) - 0.5 * smax * (R.q[v] - L.q[v]);
+        const double jump = swap ? (O.q[v] - X.q[v]) : (X.q[v] - O.q[v]);
+        const double f = 0.5 * (FO[v] + FX[v]) - 0.5 * smax * jump;
         F[v] = isfinite(f) ? f : 0.0;
     }
 }
@@ -208,29 +221,30 @@ __device__ __forceinline__ void store4(double* p, const double* v) {
 }
 
 // Trace of one flux point from a state held in shared memory as
-// s[var][j*N1 + i] (i: xi index, j: eta index).  Edge parametrisations follow
-// FROperators::initQuad (basis.cpp:540-552): edges 0,1 run with +s, edges 2,3
-// with -s, so fp on edges 2,3 meets xi/eta index N1-1-fp.  Sums run over the
-// index the reference's dense row has nonzero weights on, ascending.
-template <int N1>
-__device__ __forceinline__ void trace_point(const double (*s)[N1 * N1], const double* Lm,
-                                            const double* Lp, int edge, int fp, double* out) {
+// s[var*VS + j*RS + i] (i: xi index, j: eta index).  Edge parametrisations
+// follow FROperators::initQuad (basis.cpp:540-552): edges 0,1 run with +s,
+// edges 2,3 with -s, so fp on edges 2,3 meets xi/eta index N1-1-fp.  The sum
+// runs over the index the reference's dense row has nonzero weights on,
+// ascending:  edge 0: sum_j l_j(-1) s[j][fp]     edge 1: sum_i l_i(1) s[fp][i]
+//             edge 2: sum_j l_j(1) s[j][N1-1-fp] edge 3: sum_i l_i(-1) s[N1-1-fp][i]
+// Written without branches on the edge (the four edges share a warp).
+template <int N1, int RS, int VS>
+__device__ __forceinline__ void trace_point(const double* s, const double* Lm, const double* Lp,
+                                            int edge, int fp, double* out) {
+    const int line = (edge >= 2) ? (N1 - 1 - fp) : fp;
+    const bool along_eta = (edge == 0 || edge == 2);
+    const int base = along_eta ? line : line * RS;
+    const int stride = along_eta ? RS : 1;
+    const double* W = (edge == 0 || edge == 3) ? Lm : Lp;
+    double w[N1];
+#pragma unroll
+    for (int m = 0; m < N1; ++m) w[m] = W[m];
 #pragma unroll
     for (int v = 0; v < 4; ++v) {
+        const double* sv = s + v * VS + base;
         double t = 0.0;
-        if (edge == 0) {
 #pragma unroll
-            for (int j = 0; j < N1; ++j) t = fma(Lm[j], s[v][j * N1 + fp], t);
-        } else if (edge == 1) {
-#pragma unroll
-            for (int i = 0; i < N1; ++i) t = fma(Lp[i], s[v][fp * N1 + i], t);
-        } else if (edge == 2) {
-#pragma unroll
-            for (int j = 0; j < N1; ++j) t = fma(Lp[j], s[v][j * N1 + (N1 - 1 - fp)], t);
-        } else {
-#pragma unroll
-            for (int i = 0; i < N1; ++i) t = fma(Lm[i], s[v][(N1 - 1 - fp) * N1 + i], t);
-        }
+        for (int m = 0; m < N1; ++m) t = fma(w[m], sv[m * stride], t);
         out[v] = t;
     }
 }
@@ -253,126 +267,165 @@ __device__ double block_sum(double x, double* red) {
 // -------------------------------------------------------------- kernels --
 
 // Minimum resident CTAs per SM requested from the register allocator.
-constexpr int kMinBlocks = 4;
+#ifndef ZJ_MIN_BLOCKS
+#define ZJ_MIN_BLOCKS 3
+#endif
+constexpr int kMinBlocks = ZJ_MIN_BLOCKS;
+
+__device__ __forceinline__ void prefetch_l2(const void* p) {
+    asm volatile("prefetch.global.L2 [%0];" ::"l"(p));
+}
+
+// N values of a 16-byte aligned shared-memory row, with 16-byte loads.
+template <int N>
+__device__ __forceinline__ void load_row(const double* row, double* out) {
+#pragma unroll
+    for (int m = 0; m + 1 < N; m += 2) {
+        const double2 t = *reinterpret_cast<const double2*>(row + m);
+        out[m] = t.x;
+        out[m + 1] = t.y;
+    }
+    if (N & 1) out[N - 1] = row[N - 1];
+}
 
 template <int P>
 __global__ void __launch_bounds__(Shape<P>::THREADS, kMinBlocks)
 k_compat_stage(const StageArgs a) {
     using S = Shape<P>;
     constexpr int N1 = S::N1, NSP = S::NSP, NFT = S::NFT, TPE = S::TPE, EB = S::EB;
+    constexpr int RS = S::RS, VS = S::VS, FS = S::FS, DS = S::DS;
     __shared__ double sOps[S::NOPS];
-    __shared__ double sF[EB][4][NSP];
-    __shared__ double sG[EB][4][NSP];
-    __shared__ double sD[EB][NFT][4];
-    // The trace primitives are dead after phase B and the new state is first
-    // written in phase C, after a barrier: one buffer serves both.
-    __shared__ union {
-        Prim w[EB][NFT];
-        double u[EB][4][NSP];
-    } sBW;
-    auto& sW = sBW.w;
-    auto& sU = sBW.u;
+    __shared__ __align__(16) double sF[EB * FS];
+    __shared__ __align__(16) double sG[EB * FS];
+    __shared__ __align__(16) double sD[EB * DS];
+    __shared__ __align__(16) double sU[EB * FS];
     __shared__ double sRed[32];
 
     const int tid = threadIdx.x;
     for (int i = tid; i < S::NOPS; i += blockDim.x) sOps[i] = a.ops[i];
-    const double* D1 = sOps;
-    const double* Lm = sOps + N1 * N1;
-    const double* Lp = Lm + N1;
-    const double* gL = Lp + N1;
-    const double* gR = gL + N1;
 
     const int el = tid / TPE, k = tid - el * TPE;
     const long long e = (long long)blockIdx.x * EB + el;
     const bool valid = (el < EB) && (e < a.n_elem);
+    const bool is_sp = valid && k < NSP;
+    const bool is_fp = valid && k < NFT;
     const double g = a.gamma;
+    const int edge = k / N1, fp = k - edge * N1;   // flux-point role
+    const int i = k % N1, j = k / N1;              // solution-point role (xi, eta)
 
-    // ---- A: Euler fluxes at the solution points; own trace primitives
-    double u[4];
-    if (valid && k < NSP) {
-        load4(a.U + (e * NSP + k) * 4, u);
+    // ---- A: independent global loads first; Euler fluxes into shared memory
+    EdgeRec r{-1, 0, kEdgeOrphan, 0};
+    double2 nr = make_double2(0.0, 0.0);
+    double qo[4], qn[4] = {0.0, 0.0, 0.0, 0.0}, u[4];
+    if (is_fp) {
+        r = a.edges[e * 4 + edge];
+        nr = __ldg(reinterpret_cast<const double2*>(a.enrm + e * 4 + edge));
+        load4_nc(a.Tin + (e * NFT + k) * 4, qo);
+    }
+    if (is_sp) {
+        const long long idx = e * NSP + k;
+        load4(a.U + idx * 4, u);
+        if ((k & 3) == 0) {
+            prefetch_l2(a.Jinv + idx * 4);
+            if (a.stage >= 2) prefetch_l2(a.U0 + idx * 4);
+        }
+    }
+    // Every flux point meets the neighbour's mirrored point N1-1-fp: both
+    // elements run their shared edge counter-clockwise (kernels.cu:577).
+    if (is_fp && !(r.flags & (kEdgeOrphan | kEdgeBoundary)))
+        load4_nc(a.Tin + (((long long)r.nbr * 4 + r.nbr_edge) * N1 + (N1 - 1 - fp)) * 4, qn);
+    if (is_sp) {
         const double ir = rcp_any(u[0]);
         const double uu = u[1] * ir, vv = u[2] * ir, E = u[3] * ir;
         const double p = (g - 1.0) * u[0] * (E - 0.5 * (uu * uu + vv * vv));
-        sF[el][0][k] = u[1]; sF[el][1][k] = u[1] * uu + p;
-        sF[el][2][k] = u[1] * vv; sF[el][3][k] = (u[3] + p) * uu;
-        sG[el][0][k] = u[2]; sG[el][1][k] = u[2] * uu;
-        sG[el][2][k] = u[2] * vv + p; sG[el][3][k] = (u[3] + p) * vv;
+        double* f = sF + el * FS + j * RS + i;
+        double* h = sG + el * FS + j * RS + i;
+        f[0] = u[1]; f[VS] = u[1] * uu + p; f[2 * VS] = u[1] * vv; f[3 * VS] = (u[3] + p) * uu;
+        h[0] = u[2]; h[VS] = u[2] * uu; h[2 * VS] = u[2] * vv + p; h[3 * VS] = (u[3] + p) * vv;
     }
-    if (valid && k < NFT) {
-        double q[4];
-        load4_nc(a.Tin + (e * NFT + k) * 4, q);
-        make_prim(q, g, sW[el][k]);
-    }
-    __syncthreads();   // sOps, sF, sG, sW ready
 
-    // ---- B: interface fluxes, this element's side
-    if (valid && k < NFT) {
-        const int edge = k / N1, fp = k - edge * N1;
-        const EdgeRec r = a.edges[e * 4 + edge];
-        const double2 nr = __ldg(reinterpret_cast<const double2*>(a.enrm + e * 4 + edge));
+    // ---- B: common flux of each face point, computed once per side.  A left
+    // (or boundary) side owns the slot of its own point; a right side's point
+    // fp produces the common flux of slot N1-1-fp (reference pairing: the left
+    // trace at fp' with the right trace at N1-1-fp', used by the right side
+    // at fp').  Slots hold sigma * Fc, sigma = +1 left, -1 right.
+    double sig = 1.0, Fi[4] = {0.0, 0.0, 0.0, 0.0};
+    if (is_fp) {
         const double nx = nr.x, ny = nr.y;
-        double Fd[4] = {0.0, 0.0, 0.0, 0.0};
+        double Fc[4] = {0.0, 0.0, 0.0, 0.0};
+        int target = k;
         if (!(r.flags & kEdgeOrphan)) {
-            Prim X;
-            double Fc[4], Fi[4];
-            if (!(r.flags & kEdgeRight)) {
-                const Prim& L = sW[el][k];
-                double q[4];
-                if (r.nbr >= 0)
-                    load4_nc(a.Tin + (((long long)r.nbr * 4 + r.nbr_edge) * N1 + (N1 - 1 - fp)) * 4, q);
-                else
-                    ghost_compat(L, nx, ny, edge_bc_type(r.flags), a.bc + (long long)r.nbr_edge * 8, g, q);
-                make_prim(q, g, X);
-                rusanov_compat(L, X, nx, ny, Fc);
-                flux_normal(L, nx, ny, Fi);
-#pragma unroll
-                for (int v = 0; v < 4; ++v) Fd[v] = Fc[v] - Fi[v];
-            } else {
-                // Right side: the common flux at fp pairs the left trace at fp
-                // with this trace at N1-1-fp (kernels.cu:577), while the
-                // interior flux uses this trace at fp (kernels.cu:402-425).
-                double q[4];
-                load4_nc(a.Tin + (((long long)r.nbr * 4 + r.nbr_edge) * N1 + fp) * 4, q);
-                make_prim(q, g, X);
-                rusanov_compat(X, sW[el][edge * N1 + (N1 - 1 - fp)], nx, ny, Fc);
-                flux_normal(sW[el][k], nx, ny, Fi);
-#pragma unroll
-                for (int v = 0; v < 4; ++v) Fd[v] = -Fc[v] + Fi[v];
-            }
+            Prim O, X;
+            make_prim(qo, g, O);
+            if (r.flags & kEdgeBoundary)
+                ghost_compat(O, nx, ny, edge_bc_type(r.flags), a.bc + (long long)r.nbr_edge * 8, g, qn);
+            make_prim(qn, g, X);
+            // Left side: Rusanov(own, neighbour); right side: Rusanov(neighbour, own).
+            const bool right = (r.flags & kEdgeRight) != 0;
+            rusanov_pair(O, X, right, nx, ny, Fc);
+            flux_normal(O, nx, ny, Fi);   // interior flux of this point (kernels.cu:389-424)
+            sig = right ? -1.0 : 1.0;
+            target = right ? edge * N1 + (N1 - 1 - fp) : k;
         }
+        double c[4];
 #pragma unroll
-        for (int v = 0; v < 4; ++v) sD[el][k][v] = Fd[v];
+        for (int v = 0; v < 4; ++v) c[v] = sig * Fc[v];
+        store4(sD + el * DS + target * 4, c);
+    }
+    __syncthreads();   // sOps, sF, sG, common fluxes ready
+    // Flux difference of this point: left Fc - Fi, right -Fc + Fi (kernels.cu:393-424).
+    if (is_fp) {
+        double* d = sD + el * DS + k * 4;
+        double t[4];
+        load4(d, t);
+#pragma unroll
+        for (int v = 0; v < 4; ++v) t[v] = t[v] - sig * Fi[v];
+        store4(d, t);
     }
     __syncthreads();
 
     // ---- C: divergence, correction, stage update
     double rsq = 0.0;
-    if (valid && k < NSP) {
-        const int i = k % N1, j = k / N1;   // xi index, eta index
+    if (is_sp) {
         const long long idx = e * NSP + k;
         double ji[4], u0[4];
         load4_nc(a.Jinv + idx * 4, ji);
         if (a.stage >= 2) load4(a.U0 + idx * 4, u0);
+        double Di[N1], Dj[N1];
+#pragma unroll
+        for (int m = 0; m < N1; ++m) { Di[m] = sOps[i * N1 + m]; Dj[m] = sOps[j * N1 + m]; }
+        const double* gL = sOps + N1 * N1 + 2 * N1;
+        const double* gR = gL + N1;
+        const double gLj = gL[j], gRi = gR[i], gRj = gR[j], gLi = gL[i];
+        const double* f = sF + el * FS;
+        const double* h = sG + el * FS;
+        const double* d = sD + el * DS;
+        double c0[4], c1[4], c2[4], c3[4];
+        load4(d + (0 * N1 + i) * 4, c0);
+        load4(d + (1 * N1 + j) * 4, c1);
+        load4(d + (2 * N1 + i) * 4, c2);
+        load4(d + (3 * N1 + j) * 4, c3);
         double res[4];
 #pragma unroll
         for (int v = 0; v < 4; ++v) {
+            double fr[N1], gr[N1];
+            load_row<N1>(f + v * VS + j * RS, fr);
+            load_row<N1>(h + v * VS + j * RS, gr);
             double dFdxi = 0.0, dFdeta = 0.0, dGdxi = 0.0, dGdeta = 0.0;
 #pragma unroll
             for (int m = 0; m < N1; ++m) {
-                const double dxi = D1[i * N1 + m], deta = D1[j * N1 + m];
-                dFdxi = fma(dxi, sF[el][v][j * N1 + m], dFdxi);
-                dFdeta = fma(deta, sF[el][v][m * N1 + i], dFdeta);
-                dGdxi = fma(dxi, sG[el][v][j * N1 + m], dGdxi);
-                dGdeta = fma(deta, sG[el][v][m * N1 + i], dGdeta);
+                dFdxi = fma(Di[m], fr[m], dFdxi);
+                dFdeta = fma(Dj[m], f[v * VS + m * RS + i], dFdeta);
+                dGdxi = fma(Di[m], gr[m], dGdxi);
+                dGdeta = fma(Dj[m], h[v * VS + m * RS + i], dGdeta);
             }
             const double div = (dFdxi * ji[0] + dFdeta * ji[2]) + (dGdxi * ji[1] + dGdeta * ji[3]);
             double rr = -div;
             double corr = 0.0;
-            corr += sD[el][0 * N1 + i][v] * gL[j];
-            corr += sD[el][1 * N1 + j][v] * gR[i];
-            corr += sD[el][2 * N1 + i][v] * gR[j];
-            corr += sD[el][3 * N1 + j][v] * gL[i];
+            corr += c0[v] * gLj;
+            corr += c1[v] * gRi;
+            corr += c2[v] * gRj;
+            corr += c3[v] * gLi;
             rr -= corr;
             res[v] = rr;
         }
@@ -391,8 +444,9 @@ k_compat_stage(const StageArgs a) {
             }
             positivity(uo);
             store4(a.Uout + idx * 4, uo);
+            double* su = sU + el * FS + j * RS + i;
 #pragma unroll
-            for (int v = 0; v < 4; ++v) sU[el][v][k] = uo[v];
+            for (int v = 0; v < 4; ++v) su[v * VS] = uo[v];
             if (a.stage == 3) {
 #pragma unroll
                 for (int v = 0; v < 4; ++v) rsq += res[v] * res[v];
@@ -407,10 +461,9 @@ k_compat_stage(const StageArgs a) {
     __syncthreads();
 
     // ---- D: traces of the new state
-    if (valid && k < NFT) {
-        const int edge = k / N1, fp = k - edge * N1;
+    if (is_fp) {
         double t[4];
-        trace_point<N1>(sU[el], Lm, Lp, edge, fp, t);
+        trace_point<N1, RS, VS>(sU + el * FS, sOps + N1 * N1, sOps + N1 * N1 + N1, edge, fp, t);
         store4(a.Tout + (e * NFT + k) * 4, t);
     }
 }
@@ -421,8 +474,9 @@ k_traces(const double* __restrict__ U, double* __restrict__ T, const double* __r
          long long n_elem) {
     using S = Shape<P>;
     constexpr int N1 = S::N1, NSP = S::NSP, NFT = S::NFT, TPE = S::TPE, EB = S::EB;
+    constexpr int RS = S::RS, VS = S::VS, FS = S::FS;
     __shared__ double sOps[S::NOPS];
-    __shared__ double sU[EB][4][NSP];
+    __shared__ double sU[EB * FS];
     const int tid = threadIdx.x;
     for (int i = tid; i < S::NOPS; i += blockDim.x) sOps[i] = ops[i];
     const int el = tid / TPE, k = tid - el * TPE;
@@ -431,14 +485,15 @@ k_traces(const double* __restrict__ U, double* __restrict__ T, const double* __r
     if (valid && k < NSP) {
         double u[4];
         load4_nc(U + (e * NSP + k) * 4, u);
+        double* su = sU + el * FS + (k / N1) * RS + (k % N1);
 #pragma unroll
-        for (int v = 0; v < 4; ++v) sU[el][v][k] = u[v];
+        for (int v = 0; v < 4; ++v) su[v * VS] = u[v];
     }
     __syncthreads();
     if (valid && k < NFT) {
         const int edge = k / N1, fp = k - edge * N1;
         double t[4];
-        trace_point<N1>(sU[el], sOps + N1 * N1, sOps + N1 * N1 + N1, edge, fp, t);
+        trace_point<N1, RS, VS>(sU + el * FS, sOps + N1 * N1, sOps + N1 * N1 + N1, edge, fp, t);
         store4(T + (e * NFT + k) * 4, t);
     }
 }
