@@ -48,7 +48,23 @@ def build(force: bool = False, verbose: bool = False, ptxas_v: bool = False) -> 
     if verbose or ptxas_v:
         sys.stdout.write(r.stdout + r.stderr)
     os.replace(LIB + ".tmp", LIB)
+    build_driver()
     return LIB
+
+
+DRIVER = os.path.join(HERE, "zj_run")
+
+
+def build_driver() -> str:
+    """The C++ driver (cpp/zj_run.cpp) over the FRSolver facade, linked to the
+    in-tree library."""
+    cmd = ["g++", "-std=c++17", "-O2", "-I", os.path.join(ROOT, "include"),
+           os.path.join(HERE, "cpp", "zj_run.cpp"), "-L", HERE, "-lzj_fr",
+           "-Wl,-rpath,$ORIGIN", "-o", DRIVER]
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError("driver build failed:\n" + r.stderr)
+    return DRIVER
 
 
 if __name__ == "__main__":
