@@ -175,6 +175,26 @@ int zj_iteration(const zj_solver* s);
 zj_status zj_set_stream(zj_solver* s, void* stream);
 void* zj_get_stream(const zj_solver* s);
 
+/* ---- allocation-free residual ------------------------------------------------
+ * No counterpart in the reference.  The same residual as zj_rhs for callers
+ * that may not allocate device memory when they need it (a host application
+ * whose device memory is reserved up front by its own allocator, a
+ * time-critical loop that must not hit cudaMalloc's implicit synchronisation).
+ * Its per-call scratch -- the trace buffer, E*4*(P+1)*4 doubles, plus one
+ * double per CTA -- lives in one file-scope device array of
+ * ZJ_NOALLOC_SCRATCH_BYTES inside the library, which every GPU that loads the
+ * library holds until the process exits; the call makes no cudaMalloc,
+ * cudaFree or other allocating call.  A mesh whose scratch exceeds the limit
+ * is rejected with ZJ_ERR_ARG (P3: up to 65 000 elements).
+ * The first call on a device looks up the array's device address (once per
+ * device, with that device current); make that first call before any stream
+ * capture.  All calls share the one array: calls that overlap on the GPU
+ * (other streams, other handles, other host threads) race on it.  Inputs and
+ * outputs are the caller's device buffers, 16-byte aligned, on the handle's
+ * stream. */
+#define ZJ_NOALLOC_SCRATCH_BYTES (32u * 1024u * 1024u)
+zj_status zj_rhs_noalloc(zj_solver* s, const double* U_dev, double* R_dev);
+
 /* ---- config-file convenience: parse + mesh from a Gmsh file ---------------- */
 /* Read an ASCII Gmsh MSH v2.2 / v4.1 quad mesh (src/mesh/gmsh_reader.cpp:161)
  * and create a solver.  Physical names map to boundary types as

@@ -84,6 +84,7 @@ def lib():
         "zj_synchronize": (ip, [vp]),
         "zj_rhs": (ip, [vp, vp, vp]),
         "zj_rhs_host": (ip, [vp, dp, dp]),
+        "zj_rhs_noalloc": (ip, [vp, vp, vp]),
         "zj_residual_norm": (ip, [vp, dp]),
         "zj_compute_dt": (ip, [vp, dp]),
         "zj_check_state": (ip, [vp]),

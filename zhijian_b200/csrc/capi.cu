@@ -15,6 +15,7 @@
 #include <cstdio>
 #include <cstring>
 #include <string>
+#include <mutex>
 #include <vector>
 
 #include "zj_internal.h"
@@ -368,6 +369,74 @@ zj_status zj_check_state(zj_solver* s) {
     ZJ_CK(s, cudaMemcpyAsync(&flag, s->dFlag, sizeof(int), cudaMemcpyDeviceToHost, s->stream), "check copy");
     ZJ_CK(s, cudaStreamSynchronize(s->stream), "check sync");
     if (flag) return fail(s, ZJ_ERR_NAN, "state holds NaN or Inf");
+    return ZJ_OK;
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Allocation-free residual.  Some callers may not allocate device memory at
+// the point where they need a residual: a host application whose device
+// memory is reserved up front by its own pool allocator, or a time-critical
+// loop where the implicit synchronisation of cudaMalloc/cudaFree is not
+// allowed.  zj_rhs_noalloc serves them: its per-call scratch (the trace buffer
+// of the residual and the per-CTA partial sums) lives in this file-scope
+// array instead of the handle's buffers, so the call allocates and frees
+// nothing.  The array is a fixed ZJ_NOALLOC_SCRATCH_BYTES that every GPU which
+// loads this library holds until the process exits.
+static __device__ __align__(256) double g_noalloc_scratch[ZJ_NOALLOC_SCRATCH_BYTES / sizeof(double)];
+
+namespace {
+
+// Device address of g_noalloc_scratch per device.  In host code the array's
+// name only stands in for the symbol; a kernel must be given the address
+// cudaGetSymbolAddress returns with that device current.
+constexpr int kMaxDevices = 64;
+double* g_noalloc_ptr[kMaxDevices] = {};
+std::mutex g_noalloc_mutex;
+
+cudaError_t noalloc_scratch(double** out) {
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    if (dev < 0 || dev >= kMaxDevices) return cudaErrorInvalidDevice;
+    std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+    if (!g_noalloc_ptr[dev]) {
+        void* p = nullptr;
+        e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+        if (e != cudaSuccess) return e;
+        g_noalloc_ptr[dev] = static_cast<double*>(p);
+    }
+    *out = g_noalloc_ptr[dev];
+    return cudaSuccess;
+}
+
+}  // namespace
+
+extern "C" {
+
+zj_status zj_rhs_noalloc(zj_solver* s, const double* U_dev, double* R_dev) {
+    if (!s || !U_dev || !R_dev) return ZJ_ERR_ARG;
+    if ((reinterpret_cast<uintptr_t>(U_dev) | reinterpret_cast<uintptr_t>(R_dev)) & 15u)
+        return fail(s, ZJ_ERR_ARG, "U_dev and R_dev must be 16-byte aligned");
+    const size_t trace_bytes = s->trace_n * sizeof(double);
+    const size_t part_bytes = (size_t)s->grid * sizeof(double);
+    if (trace_bytes + part_bytes > ZJ_NOALLOC_SCRATCH_BYTES)
+        return fail(s, ZJ_ERR_ARG,
+                    "mesh too large for zj_rhs_noalloc: needs " + std::to_string(trace_bytes + part_bytes) +
+                        " bytes of scratch, the static limit is " +
+                        std::to_string((size_t)ZJ_NOALLOC_SCRATCH_BYTES) + " bytes");
+    double* scratch = nullptr;
+    ZJ_CK(s, noalloc_scratch(&scratch), "static scratch address");
+    // Every scratch value is written before it is read (all traces by the
+    // trace launch, one partial per CTA), so nothing needs clearing.
+    double* traces = scratch;
+    double* partials = scratch + s->trace_n;
+    ZJ_CK(s, launch_traces(s->P, U_dev, traces, s->dOps, s->E, s->stream), "trace launch");
+    StageArgs a = base_args(s);
+    a.U = U_dev; a.U0 = U_dev; a.Uout = nullptr; a.Tin = traces; a.Tout = nullptr;
+    a.R = R_dev; a.partials = partials; a.stage = 0;
+    ZJ_CK(s, launch_compat_stage(s->P, a, s->stream, nullptr), "residual launch");
     return ZJ_OK;
 }
 
