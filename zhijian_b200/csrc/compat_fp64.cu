@@ -61,11 +61,10 @@ struct Shape {
 
 // ---------------------------------------------------------------- physics --
 //
-// FP64 division and square root run on the XU pipe, which these kernels
-// saturate first.  The reference divides by rho up to ten times per state;
-// here every state takes one reciprocal and multiplies, and reciprocals and
-// square roots come from zj_math.h (Newton-Raphson on the FMA pipe, within
-// 2 ulp).  Each quotient moves by a few ulp; the residual stays within 1e-12
+// The reference divides by rho up to ten times per state; here every state
+// takes one reciprocal and multiplies, and reciprocals and square roots come
+// from zj_math.h (Newton-Raphson FMA chains, within 2 ulp) instead of the
+// long FP64 divide/sqrt sequences.  Each quotient moves by a few ulp; the residual stays within 1e-12
 // of the reference's.
 
 // 1/x: Newton-Raphson for positive normal x, IEEE division otherwise (zero,

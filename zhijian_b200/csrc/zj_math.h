@@ -1,9 +1,9 @@
 // zj_math.h -- FP64 reciprocal and square root on the FMA pipe.
 //
-// On sm_100a an FP64 division or square root issues to the XU pipe, which the
-// residual kernels saturate long before HBM or the FP64 FMA pipe.  These two
-// functions use Newton-Raphson iterations from integer-arithmetic seeds, so
-// they only issue FP64 FMAs and integer ops:
+// An FP64 division or square root is a long dependent instruction sequence
+// with a special-case path; the residual kernels take several per state.
+// These two functions use Newton-Raphson iterations from integer-arithmetic
+// seeds, so they are short branch-free chains of FP64 FMAs and integer ops:
 //   reciprocal: seed = bits(0x7FDE623822FC16E6 - bits(x)) (relative error
 //     below 1/8 for normal x), then e = 1 - x*y, y += y*e five times
 //     (error squares each step: 2^-3 -> below 2^-60);
