@@ -49,6 +49,14 @@ struct orc_ctx {
     /* work */
     double *Fx, *Fy, *Ufp, *Fcom, *Fdiff, *U0, *U1;
     int nthreads;
+    /* physics mode */
+    int flux_type, riemann, viscous;
+    double Re, Pr, T_inf;
+    double gLp[16], gRp[16];
+    int n_tags;
+    int tag_ids[64];
+    double tag_pt[64], tag_Tt[64], tag_dx[64], tag_dy[64], tag_Tw[64], tag_ps[64];
+    double *flen;
 };
 
 /* ---------------------------------------------------------------- basis -- */
@@ -363,6 +371,7 @@ static int build_faces(orc_ctx* c, int64_t n_bnd, const int64_t* bnd,
     c->fbct = (int*)malloc(sizeof(int) * cap); c->ftag = (int*)malloc(sizeof(int) * cap);
     c->fbcmap = (int*)malloc(sizeof(int) * cap);
     c->fn = (double*)malloc(sizeof(double) * 2 * cap);
+    c->flen = (double*)malloc(sizeof(double) * cap);
     c->bc_data = (double*)calloc((size_t)(cap * 8 + 8), sizeof(double));
     double c_inf = sqrt(c->gamma * c->p_inf / c->rho_inf);
     (void)c_inf;
@@ -392,6 +401,13 @@ static int build_faces(orc_ctx* c, int64_t n_bnd, const int64_t* bnd,
                 c->fbct[f] = BC_INTERIOR; c->ftag[f] = -1;
             }
             face_normal(c, c->fle[f], c->fll[f], c->fn + 2 * f);
+            {   /* mesh.cpp:148-157 */
+                const int64_t* nd = c->conn + (int64_t)c->fle[f] * c->nn;
+                const double* v0 = c->xy + 2 * nd[c->fll[f]];
+                const double* v1 = c->xy + 2 * nd[(c->fll[f] + 1) % 4];
+                double tx = v1[0] - v0[0], ty = v1[1] - v0[1];
+                c->flen[f] = sqrt(tx * tx + ty * ty);
+            }
             /* fr_solver.cpp:432-482 BC packing, 8 values per boundary face */
             if (cnt == 1) {
                 c->fbcmap[f] = (int)nbc;
@@ -457,6 +473,12 @@ orc_ctx* orc_create(int P, double gamma, double rho_inf, double p_inf,
     c->Jinv = (double*)malloc(sizeof(double) * n_elem * nsp * 4);
     c->area = (double*)malloc(sizeof(double) * n_elem);
     build_geometry(c);
+    c->n_tags = n_tags < 64 ? n_tags : 64;
+    for (int t = 0; t < c->n_tags; ++t) {
+        c->tag_ids[t] = tag_ids[t]; c->tag_ps[t] = tag_pstatic[t];
+        c->tag_pt[t] = 0.0; c->tag_Tt[t] = 0.0; c->tag_dx[t] = 1.0; c->tag_dy[t] = 0.0; c->tag_Tw[t] = 0.0;
+    }
+    c->flux_type = 2; c->riemann = 0; c->viscous = 0; c->Re = 1000.0; c->Pr = 0.72; c->T_inf = 300.0;
     if (build_faces(c, n_bnd, bnd, n_tags, tag_ids, tag_types, tag_pstatic) != 0) {
         orc_destroy(c); return NULL;
     }
@@ -477,7 +499,7 @@ void orc_destroy(orc_ctx* c) {
     void* ps[] = {c->xy, c->conn, c->J, c->Jinv, c->area, c->fle, c->fll, c->fre, c->frl,
                   c->fbct, c->ftag, c->fbcmap, c->fn, c->bc_data, c->pts, c->D1, c->dxi,
                   c->deta, c->interp, c->corr, c->Fx, c->Fy, c->Ufp, c->Fcom, c->Fdiff,
-                  c->U0, c->U1};
+                  c->U0, c->U1, c->flen};
     for (size_t i = 0; i < sizeof(ps) / sizeof(ps[0]); ++i) free(ps[i]);
     free(c);
 }
@@ -768,4 +790,363 @@ double orc_l2(const double* R, int64_t n) {
     double s = 0.0;
     for (int64_t i = 0; i < n; ++i) s += R[i] * R[i];
     return sqrt(s);
+}
+
+
+/* ======================================================================= */
+/* Physics mode: the conservative FR scheme the parameters ask for, restated  */
+/* from the reference's formula sources (no reference residual exists):      */
+/*   Riemann solvers      include/physics/euler.hpp:184-375                  */
+/*   ghost states         include/bc/boundary_condition.hpp:42-311           */
+/*   BC defaults          src/bc/boundary_condition.cpp:32-64                */
+/*   VCJH corrections     Vincent, Castonguay & Jameson 2011 (README refs)   */
+/* ======================================================================= */
+
+static double pressure_raw(const double* U, double g) { return pressure(U, g); }
+
+/* IdealGas::soundSpeed (euler.hpp:34-41) */
+static double sound_speed(const double* U, double g) {
+    double p = fmax(pressure_raw(U, g), 1e-10), rho = fmax(U[0], 1e-10);
+    return sqrt(g * p / rho);
+}
+
+/* IdealGas::fluxNormal (euler.hpp:133-147) */
+static void flux_normal_phys(const double* U, double nx, double ny, double g, double* Fn) {
+    double rho = fmax(U[0], 1e-10);
+    double u = U[1] / rho, v = U[2] / rho;
+    double p = fmax(pressure_raw(U, g), 1e-10);
+    double H = U[3] + pressure_raw(U, g);
+    double vn = u * nx + v * ny;
+    Fn[0] = rho * vn; Fn[1] = rho * u * vn + p * nx; Fn[2] = rho * v * vn + p * ny; Fn[3] = H * vn;
+}
+
+/* IdealGas::maxWaveSpeed (euler.hpp:166-171) */
+static double max_wave_speed(const double* U, double g) {
+    double u = U[1] / U[0], v = U[2] / U[0];
+    return sqrt(u * u + v * v) + sound_speed(U, g);
+}
+
+/* RiemannSolvers::rusanov (euler.hpp:184-200) */
+static void riemann_rusanov(const double* UL, const double* UR, double nx, double ny, double g, double* F) {
+    double FL[4], FR[4];
+    flux_normal_phys(UL, nx, ny, g, FL);
+    flux_normal_phys(UR, nx, ny, g, FR);
+    double smax = fmax(max_wave_speed(UL, g), max_wave_speed(UR, g));
+    for (int i = 0; i < 4; ++i) F[i] = 0.5 * (FL[i] + FR[i]) - 0.5 * smax * (UR[i] - UL[i]);
+}
+
+/* RiemannSolvers::roe with Harten's entropy fix (euler.hpp:204-294) */
+static void riemann_roe(const double* UL, const double* UR, double nx, double ny, double g, double* F) {
+    double rhoL = fmax(UL[0], 1e-10), rhoR = fmax(UR[0], 1e-10);
+    double uL = UL[1] / rhoL, vL = UL[2] / rhoL, uR = UR[1] / rhoR, vR = UR[2] / rhoR;
+    double HL = (UL[3] + pressure_raw(UL, g)) / rhoL, HR = (UR[3] + pressure_raw(UR, g)) / rhoR;
+    double sL = sqrt(rhoL), sR = sqrt(rhoR);
+    double den = fmax(sL + sR, 1e-10);
+    double rhoRoe = sL * sR;
+    double uRoe = (sL * uL + sR * uR) / den, vRoe = (sL * vL + sR * vR) / den;
+    double HRoe = (sL * HL + sR * HR) / den;
+    double vnRoe = uRoe * nx + vRoe * ny, qsq = uRoe * uRoe + vRoe * vRoe;
+    double c2 = fmax((g - 1.0) * (HRoe - 0.5 * qsq), 1e-10), cR = sqrt(c2);
+    double l1 = fabs(vnRoe - cR), l2 = fabs(vnRoe), l3 = fabs(vnRoe), l4 = fabs(vnRoe + cR);
+    double eps = 0.1 * cR;
+    if (l1 < eps) l1 = (l1 * l1 + eps * eps) / (2.0 * eps);
+    if (l4 < eps) l4 = (l4 * l4 + eps * eps) / (2.0 * eps);
+    double drho = rhoR - rhoL, du = uR - uL, dv = vR - vL;
+    double dp = pressure_raw(UR, g) - pressure_raw(UL, g);
+    double dvn = du * nx + dv * ny;
+    double cs = fmax(cR * cR, 1e-10);
+    double a1 = (dp - rhoRoe * cR * dvn) / (2.0 * cs);
+    double a2 = drho - dp / cs;
+    double a3 = rhoRoe * (dv * nx - du * ny);
+    double a4 = (dp + rhoRoe * cR * dvn) / (2.0 * cs);
+    double FL[4], FR[4], dF[4];
+    flux_normal_phys(UL, nx, ny, g, FL);
+    flux_normal_phys(UR, nx, ny, g, FR);
+    double tx = -ny, ty = nx;
+    dF[0] = l1 * a1 * 1.0;
+    dF[1] = l1 * a1 * (uRoe - cR * nx);
+    dF[2] = l1 * a1 * (vRoe - cR * ny);
+    dF[3] = l1 * a1 * (HRoe - cR * vnRoe);
+    dF[0] += l2 * a2 * 1.0;
+    dF[1] += l2 * a2 * uRoe;
+    dF[2] += l2 * a2 * vRoe;
+    dF[3] += l2 * a2 * 0.5 * qsq;
+    dF[0] += l3 * a3 * 0.0;
+    dF[1] += l3 * a3 * tx;
+    dF[2] += l3 * a3 * ty;
+    dF[3] += l3 * a3 * (uRoe * tx + vRoe * ty);
+    dF[0] += l4 * a4 * 1.0;
+    dF[1] += l4 * a4 * (uRoe + cR * nx);
+    dF[2] += l4 * a4 * (vRoe + cR * ny);
+    dF[3] += l4 * a4 * (HRoe + cR * vnRoe);
+    for (int i = 0; i < 4; ++i) F[i] = 0.5 * (FL[i] + FR[i]) - 0.5 * dF[i];
+}
+
+static double clamp_away(double d) { return (fabs(d) < 1e-10) ? ((d >= 0) ? 1e-10 : -1e-10) : d; }
+
+/* RiemannSolvers::hllc (euler.hpp:298-375) */
+static void riemann_hllc(const double* UL, const double* UR, double nx, double ny, double g, double* F) {
+    double rhoL = fmax(UL[0], 1e-10), rhoR = fmax(UR[0], 1e-10);
+    double uL = UL[1] / rhoL, vL = UL[2] / rhoL, uR = UR[1] / rhoR, vR = UR[2] / rhoR;
+    double pL = fmax(pressure_raw(UL, g), 1e-10), pR = fmax(pressure_raw(UR, g), 1e-10);
+    double cL = sound_speed(UL, g), cR = sound_speed(UR, g);
+    double vnL = uL * nx + vL * ny, vnR = uR * nx + vR * ny;
+    double ps = 0.5 * (pL + pR) - 0.5 * (vnR - vnL) * 0.5 * (rhoL + rhoR) * 0.5 * (cL + cR);
+    ps = fmax(ps, 1e-10);
+    double qL = (ps <= pL) ? 1.0 : sqrt(1.0 + (g + 1.0) / (2.0 * g) * (ps / pL - 1.0));
+    double qR = (ps <= pR) ? 1.0 : sqrt(1.0 + (g + 1.0) / (2.0 * g) * (ps / pR - 1.0));
+    double SL = vnL - cL * qL, SR = vnR + cR * qR;
+    double dSM = clamp_away(rhoL * (SL - vnL) - rhoR * (SR - vnR));
+    double SM = (pR - pL + rhoL * vnL * (SL - vnL) - rhoR * vnR * (SR - vnR)) / dSM;
+    if (SL >= 0.0) { flux_normal_phys(UL, nx, ny, g, F); return; }
+    if (SR <= 0.0) { flux_normal_phys(UR, nx, ny, g, F); return; }
+    const double *Uk; double rk, uk, vk, vnk, pk, Sk;
+    if (SM >= 0.0) { Uk = UL; rk = rhoL; uk = uL; vk = vL; vnk = vnL; pk = pL; Sk = SL; }
+    else { Uk = UR; rk = rhoR; uk = uR; vk = vR; vnk = vnR; pk = pR; Sk = SR; }
+    double dK = clamp_away(Sk - SM);
+    double dvn = clamp_away(Sk - vnk);
+    double fac = rk * dvn / dK;
+    double Us[4];
+    Us[0] = fac;
+    Us[1] = fac * (uk + (SM - vnk) * nx);
+    Us[2] = fac * (vk + (SM - vnk) * ny);
+    Us[3] = fac * (Uk[3] / rk + (SM - vnk) * (SM + pk / (rk * dvn)));
+    double Fk[4];
+    flux_normal_phys(Uk, nx, ny, g, Fk);
+    for (int i = 0; i < 4; ++i) F[i] = Fk[i] + Sk * (Us[i] - Uk[i]);
+}
+
+void orc_riemann_point(int which, const double* UL, const double* UR, double nx, double ny,
+                       double g, double* F) {
+    if (which == 1) riemann_roe(UL, UR, nx, ny, g, F);
+    else if (which == 2) riemann_hllc(UL, UR, nx, ny, g, F);
+    else riemann_rusanov(UL, UR, nx, ny, g, F);
+}
+
+static int tag_slot(const orc_ctx* c, int tag) {
+    int hit = -1;
+    for (int t = 0; t < c->n_tags; ++t) if (c->tag_ids[t] == tag) hit = t;
+    return hit;
+}
+
+/* BoundaryCondition::ghostState of each class (boundary_condition.hpp:42-311),
+ * with the parameters createBCFromSpec gives them (boundary_condition.cpp:32-64). */
+void orc_ghost_point(const orc_ctx* c, int bct, int tag, const double* Ui, double nx, double ny,
+                     double* Ug) {
+    const double g = c->gamma;
+    int t = tag > 0 ? tag_slot(c, tag) : -1;
+    switch (bct) {
+    case BC_WALL: {
+        double rho = Ui[0], u = Ui[1] / rho, v = Ui[2] / rho;
+        double Tw = (t >= 0) ? c->tag_Tw[t] : 0.0;
+        double p = (Tw > 0) ? rho * Tw : pressure_raw(Ui, g);
+        prim2cons(rho, -u, -v, p, g, Ug);
+        break;
+    }
+    case BC_SLIPWALL: case BC_SYMMETRY: {
+        double rho = Ui[0], u = Ui[1] / rho, v = Ui[2] / rho, p = pressure_raw(Ui, g);
+        double vn = u * nx + v * ny;
+        prim2cons(rho, u - 2.0 * vn * nx, v - 2.0 * vn * ny, p, g, Ug);
+        break;
+    }
+    case BC_FARFIELD: {
+        double Uinf[4];
+        prim2cons(c->rho_inf, c->u_inf, c->v_inf, c->p_inf, g, Uinf);
+        double c_inf = sound_speed(Uinf, g);
+        double rho_i = Ui[0], u_i = Ui[1] / rho_i, v_i = Ui[2] / rho_i;
+        double p_i = pressure_raw(Ui, g), c_i = sound_speed(Ui, g);
+        double vn_i = u_i * nx + v_i * ny, vn_inf = c->u_inf * nx + c->v_inf * ny;
+        double Rp = vn_i + 2.0 * c_i / (g - 1.0), Rm = vn_inf - 2.0 * c_inf / (g - 1.0);
+        double vn_b = 0.5 * (Rp + Rm), c_b = 0.25 * (g - 1.0) * (Rp - Rm);
+        double rho_b, p_b, u_b, v_b;
+        if (vn_b >= 0) {
+            double vt = u_i * (-ny) + v_i * nx, s_i = p_i / pow(rho_i, g);
+            rho_b = pow(c_b * c_b / (g * s_i), 1.0 / (g - 1.0));
+            p_b = rho_b * c_b * c_b / g;
+            u_b = vn_b * nx - vt * ny; v_b = vn_b * ny + vt * nx;
+        } else {
+            double vt = c->u_inf * (-ny) + c->v_inf * nx, s_inf = c->p_inf / pow(c->rho_inf, g);
+            rho_b = pow(c_b * c_b / (g * s_inf), 1.0 / (g - 1.0));
+            p_b = rho_b * c_b * c_b / g;
+            u_b = vn_b * nx - vt * ny; v_b = vn_b * ny + vt * nx;
+        }
+        prim2cons(rho_b, u_b, v_b, p_b, g, Ug);
+        break;
+    }
+    case BC_INFLOW: {
+        double pt = (t >= 0 && c->tag_pt[t] > 0) ? c->tag_pt[t] : c->p_inf * 1.2;
+        double Tt = (t >= 0 && c->tag_Tt[t] > 0) ? c->tag_Tt[t] : c->T_inf;
+        double dx = (t >= 0) ? c->tag_dx[t] : 1.0, dy = (t >= 0) ? c->tag_dy[t] : 0.0;
+        double mag = sqrt(dx * dx + dy * dy);
+        dx /= mag; dy /= mag;
+        double p_int = pressure_raw(Ui, g);
+        double ratio = p_int / pt;
+        double M2 = 2.0 / (g - 1.0) * (pow(ratio, -(g - 1.0) / g) - 1.0);
+        M2 = fmax(M2, 0.0);
+        double M = sqrt(M2);
+        double T = Tt / (1.0 + 0.5 * (g - 1.0) * M2);
+        double rho = p_int / T;
+        double cc = sqrt(g * p_int / rho);
+        double vel = M * cc;
+        prim2cons(rho, vel * dx, vel * dy, p_int, g, Ug);
+        break;
+    }
+    case BC_OUTFLOW: {
+        double ps = (t >= 0 && c->tag_ps[t] > 0) ? c->tag_ps[t] : c->p_inf;
+        double rho = Ui[0], u = Ui[1] / rho, v = Ui[2] / rho;
+        prim2cons(rho, u, v, ps, g, Ug);
+        break;
+    }
+    default:
+        Ug[0] = Ui[0]; Ug[1] = Ui[1]; Ug[2] = Ui[2]; Ug[3] = Ui[3];
+    }
+}
+
+/* VCJH g_L', g_R' at the solution points, from the reference's Legendre
+ * derivative formula (basis.cpp:332-341) -- an independent evaluation of the
+ * same functions the product builds with a recurrence. */
+void orc_vcjh(int P, int flux_type, const double* x, double* gL, double* gR) {
+    int p = P;
+    double fp = 1.0, f2p = 1.0;
+    for (int i = 2; i <= p; ++i) fp *= i;
+    for (int i = 2; i <= 2 * p; ++i) f2p *= i;
+    double ap = f2p / (pow(2.0, p) * fp);
+    double ap2 = ap * ap, cc = 0.0;
+    if (flux_type == 1) cc = 2.0 * p / ((2.0 * p + 1.0) * (p + 1.0) * ap2);
+    else if (flux_type == 2) cc = 2.0 * (p + 1.0) / ((2.0 * p + 1.0) * p * ap2);
+    else if (flux_type == 3) cc = 2.0 * (p + 1.0) * fp * fp / (f2p * (2.0 * p + 1.0));
+    double eta = cc * (2.0 * p + 1.0) * ap2 / 2.0;
+    for (int j = 0; j <= p; ++j) {
+        double t = x[j];
+        double dR = 0.5 * (legendre_deriv(p, t) + (eta * legendre_deriv(p - 1, t) + legendre_deriv(p + 1, t)) / (1.0 + eta));
+        double tn = -t;
+        double dRm = 0.5 * (legendre_deriv(p, tn) + (eta * legendre_deriv(p - 1, tn) + legendre_deriv(p + 1, tn)) / (1.0 + eta));
+        gR[j] = dR;
+        gL[j] = -dRm;
+    }
+}
+
+void orc_set_physics(orc_ctx* c, int flux_type, int riemann, int viscous, double Re, double Pr,
+                     double T_inf) {
+    c->flux_type = flux_type; c->riemann = riemann; c->viscous = viscous;
+    c->Re = Re; c->Pr = Pr; c->T_inf = T_inf;
+    orc_vcjh(c->P, flux_type, c->pts, c->gLp, c->gRp);
+}
+
+void orc_set_bc_extra(orc_ctx* c, int n, const int* ids, const double* pt, const double* Tt,
+                      const double* dx, const double* dy, const double* Tw) {
+    for (int k = 0; k < n; ++k) {
+        int t = tag_slot(c, ids[k]);
+        if (t < 0) continue;
+        c->tag_pt[t] = pt[k]; c->tag_Tt[t] = Tt[k]; c->tag_dx[t] = dx[k]; c->tag_dy[t] = dy[k];
+        c->tag_Tw[t] = Tw[k];
+    }
+}
+
+void orc_get_vcjh(const orc_ctx* c, double* gL, double* gR) {
+    for (int j = 0; j < c->n1; ++j) { gL[j] = c->gLp[j]; gR[j] = c->gRp[j]; }
+}
+
+void orc_rhs_phys(orc_ctx* c, const double* U, double* R) {
+    const int nsp = c->nsp, n1 = c->n1, nfp = c->nfp;
+    const int64_t ne = c->n_elem, nf = c->n_faces;
+    const double g = c->gamma;
+    int nt = c->nthreads;
+    (void)nt;
+    size_t fpn = (size_t)ne * 4 * nfp * 4;
+    double* Ft = c->Fx; double* Gt = c->Fy;          /* transformed fluxes at sp */
+    double* FnD = (double*)malloc(sizeof(double) * fpn);
+    /* transformed fluxes F~ = J (xi_x F + xi_y G), G~ = J (eta_x F + eta_y G) */
+#pragma omp parallel for num_threads(nt) schedule(static)
+    for (int64_t idx = 0; idx < ne * nsp; ++idx) {
+        double F[4], G[4];
+        flux_xy(U + idx * 4, g, F, G);
+        const double* Ji = c->Jinv + idx * 4;
+        double J = c->J[idx];
+        for (int v = 0; v < 4; ++v) {
+            Ft[idx * 4 + v] = J * (Ji[0] * F[v] + Ji[1] * G[v]);
+            Gt[idx * 4 + v] = J * (Ji[2] * F[v] + Ji[3] * G[v]);
+        }
+    }
+    /* traces of U and outward reference-normal transformed flux, dense interp */
+#pragma omp parallel for num_threads(nt) schedule(static)
+    for (int64_t e = 0; e < ne; ++e)
+        for (int t = 0; t < 4 * nfp; ++t) {
+            int edge = t / nfp, fp = t % nfp;
+            const double* w = c->interp + (edge * nfp + fp) * nsp;
+            for (int v = 0; v < 4; ++v) {
+                double su = 0.0, sf = 0.0, sg = 0.0;
+                for (int sp = 0; sp < nsp; ++sp) {
+                    su += w[sp] * U[(e * nsp + sp) * 4 + v];
+                    sf += w[sp] * Ft[(e * nsp + sp) * 4 + v];
+                    sg += w[sp] * Gt[(e * nsp + sp) * 4 + v];
+                }
+                int64_t o = ((e * 4 + edge) * nfp + fp) * 4 + v;
+                c->Ufp[o] = su;
+                FnD[o] = (edge == 0) ? -sg : (edge == 1) ? sf : (edge == 2) ? sg : -sf;
+            }
+        }
+    memset(c->Fdiff, 0, sizeof(double) * fpn);
+    /* common fluxes, computed once per face from the left side's view */
+#pragma omp parallel for num_threads(nt) schedule(static)
+    for (int64_t f = 0; f < nf; ++f) {
+        int le = c->fle[f], ll = c->fll[f], re = c->fre[f], rl = c->frl[f];
+        double nx = c->fn[2 * f], ny = c->fn[2 * f + 1], s = 0.5 * c->flen[f];
+        for (int fp = 0; fp < nfp; ++fp) {
+            int64_t lo = (((int64_t)le * 4 + ll) * nfp + fp) * 4;
+            const double* UL = c->Ufp + lo;
+            double UR[4], Fc[4];
+            int64_t ro = -1;
+            if (re >= 0) {
+                ro = (((int64_t)re * 4 + rl) * nfp + (nfp - 1 - fp)) * 4;
+                for (int v = 0; v < 4; ++v) UR[v] = c->Ufp[ro + v];
+            } else {
+                orc_ghost_point(c, c->fbct[f], c->ftag[f], UL, nx, ny, UR);
+            }
+            orc_riemann_point(c->riemann, UL, UR, nx, ny, g, Fc);
+            for (int v = 0; v < 4; ++v) c->Fdiff[lo + v] = s * Fc[v] - FnD[lo + v];
+            if (ro >= 0)
+                for (int v = 0; v < 4; ++v) c->Fdiff[ro + v] = s * (-Fc[v]) - FnD[ro + v];
+        }
+    }
+    /* divergence + VCJH correction, divided by J */
+#pragma omp parallel for num_threads(nt) schedule(static)
+    for (int64_t e = 0; e < ne; ++e)
+        for (int sp = 0; sp < nsp; ++sp) {
+            int i = sp % n1, j = sp / n1;
+            const double* D = c->Fdiff + e * 4 * nfp * 4;
+            for (int v = 0; v < 4; ++v) {
+                double div = 0.0;
+                for (int k = 0; k < nsp; ++k)
+                    div += c->dxi[sp * nsp + k] * Ft[(e * nsp + k) * 4 + v] +
+                           c->deta[sp * nsp + k] * Gt[(e * nsp + k) * 4 + v];
+                double corr = c->gRp[i] * D[(1 * nfp + j) * 4 + v] - c->gLp[i] * D[(3 * nfp + (nfp - 1 - j)) * 4 + v] +
+                              c->gRp[j] * D[(2 * nfp + (nfp - 1 - i)) * 4 + v] - c->gLp[j] * D[(0 * nfp + i) * 4 + v];
+                R[(e * nsp + sp) * 4 + v] = -(div + corr) / c->J[e * nsp + sp];
+            }
+        }
+    free(FnD);
+}
+
+void orc_step_phys(orc_ctx* c, double* U, double dt, int nsteps, double* R_last) {
+    int64_t n = c->n_elem * c->nsp * 4;
+    double* R = (double*)malloc(sizeof(double) * (size_t)n);
+    int nt = c->nthreads;
+    (void)nt;
+    for (int st = 0; st < nsteps; ++st) {
+        memcpy(c->U0, U, sizeof(double) * (size_t)n);
+        orc_rhs_phys(c, U, R);
+#pragma omp parallel for num_threads(nt) schedule(static)
+        for (int64_t i = 0; i < n; ++i) U[i] = c->U0[i] + dt * R[i];
+        memcpy(c->U1, U, sizeof(double) * (size_t)n);
+        orc_rhs_phys(c, U, R);
+#pragma omp parallel for num_threads(nt) schedule(static)
+        for (int64_t i = 0; i < n; ++i) U[i] = 0.75 * c->U0[i] + 0.25 * c->U1[i] + 0.25 * dt * R[i];
+        orc_rhs_phys(c, U, R);
+#pragma omp parallel for num_threads(nt) schedule(static)
+        for (int64_t i = 0; i < n; ++i)
+            U[i] = (1.0 / 3.0) * c->U0[i] + (2.0 / 3.0) * U[i] + (2.0 / 3.0) * dt * R[i];
+    }
+    if (R_last) memcpy(R_last, R, sizeof(double) * (size_t)n);
+    free(R);
 }

@@ -63,6 +63,24 @@ double orc_compute_dt(const orc_ctx* c, const double* U, double CFL);
 /* L2 norm over n values, summed in index order. */
 double orc_l2(const double* R, int64_t n);
 
+/* ---- physics mode (compat off): conservative FR, VCJH, reference formula
+ * sources for the Riemann solvers and ghost states. ---------------------- */
+void orc_set_physics(orc_ctx* c, int flux_type, int riemann, int viscous, double Re, double Pr,
+                     double T_inf);
+/* per-tag inflow total pressure/temperature/direction and wall temperature */
+void orc_set_bc_extra(orc_ctx* c, int n, const int* tag_ids, const double* p_total,
+                      const double* T_total, const double* dir_x, const double* dir_y,
+                      const double* T_wall);
+void orc_get_vcjh(const orc_ctx* c, double* gL, double* gR);
+void orc_vcjh(int P, int flux_type, const double* x, double* gL, double* gR);
+void orc_rhs_phys(orc_ctx* c, const double* U, double* R);
+void orc_step_phys(orc_ctx* c, double* U, double dt, int nsteps, double* R_last);
+/* pointwise pins: which = 0 Rusanov, 1 Roe, 2 HLLC */
+void orc_riemann_point(int which, const double* UL, const double* UR, double nx, double ny,
+                       double g, double* F);
+void orc_ghost_point(const orc_ctx* c, int bc_type, int tag, const double* Ui, double nx,
+                     double ny, double* Ug);
+
 #ifdef __cplusplus
 }
 #endif

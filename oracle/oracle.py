@@ -75,6 +75,14 @@ def lib():
         h.orc_compute_dt.argtypes = [C.c_void_p, dp, C.c_double]
         h.orc_l2.restype = C.c_double
         h.orc_l2.argtypes = [dp, i64]
+        h.orc_set_physics.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_double,
+                                      C.c_double, C.c_double]
+        h.orc_set_bc_extra.argtypes = [C.c_void_p, C.c_int, ip, dp, dp, dp, dp, dp]
+        h.orc_get_vcjh.argtypes = [C.c_void_p, dp, dp]
+        h.orc_rhs_phys.argtypes = [C.c_void_p, dp, dp]
+        h.orc_step_phys.argtypes = [C.c_void_p, dp, C.c_double, C.c_int, dp]
+        h.orc_riemann_point.argtypes = [C.c_int, dp, dp, C.c_double, C.c_double, C.c_double, dp]
+        h.orc_ghost_point.argtypes = [C.c_void_p, C.c_int, C.c_int, dp, C.c_double, C.c_double, dp]
         _lib = h
     return _lib
 
@@ -168,6 +176,40 @@ class Oracle:
                                       ("pts", "D1", "diff_xi", "diff_eta", "interp", "corr")])
         return out
 
+    # ---- physics mode ------------------------------------------------
+    def set_physics(self, flux_type=2, riemann=0, viscous=False, Re=1000.0, Pr=0.72, T_inf=300.0):
+        lib().orc_set_physics(self.c, flux_type, riemann, int(viscous), Re, Pr, T_inf)
+
+    def set_bc_extra(self, rows):
+        """rows: (tag, p_total, T_total, dir_x, dir_y, T_wall)"""
+        ids = np.array([r[0] for r in rows], dtype=np.int32)
+        cols = [np.array([r[k] for r in rows], dtype=np.float64) for k in range(1, 6)]
+        self._extra = (ids, cols)
+        lib().orc_set_bc_extra(self.c, len(rows), _i(ids), *[_d(x) for x in cols])
+
+    def vcjh(self):
+        gL, gR = np.empty(self.n1), np.empty(self.n1)
+        lib().orc_get_vcjh(self.c, _d(gL), _d(gR))
+        return gL, gR
+
+    def rhs_phys(self, U):
+        U = np.ascontiguousarray(U, dtype=np.float64).reshape(self.shape)
+        R = np.empty(self.shape)
+        lib().orc_rhs_phys(self.c, _d(U), _d(R))
+        return R
+
+    def step_phys(self, U, dt, nsteps=1):
+        U = np.array(U, dtype=np.float64).reshape(self.shape)
+        R = np.empty(self.shape)
+        lib().orc_step_phys(self.c, _d(U), dt, nsteps, _d(R))
+        return U, R
+
+    def ghost(self, bc_type, tag, Ui, nx, ny):
+        Ui = np.ascontiguousarray(Ui, dtype=np.float64)
+        out = np.empty(4)
+        lib().orc_ghost_point(self.c, bc_type, tag, _d(Ui), nx, ny, _d(out))
+        return out
+
     def sp_coords(self):
         xy = np.empty((self.n_elem, self.nsp, 2))
         lib().orc_sp_coords(self.c, _d(xy))
@@ -223,3 +265,11 @@ def read_mesh_out(path, n_elem, nsp):
     sxy = rest[n_elem * nsp * 5:n_elem * nsp * 7].reshape(n_elem, nsp, 2)
     area = rest[n_elem * nsp * 7:n_elem * nsp * 7 + n_elem]
     return faces, J, Ji, sxy, area
+
+
+def riemann_point(which, UL, UR, nx, ny, g):
+    UL = np.ascontiguousarray(UL, dtype=np.float64)
+    UR = np.ascontiguousarray(UR, dtype=np.float64)
+    out = np.empty(4)
+    lib().orc_riemann_point(which, _d(UL), _d(UR), nx, ny, g, _d(out))
+    return out

@@ -27,6 +27,9 @@
 #include "common/types.hpp"
 #include "mesh/mesh.hpp"
 #include "basis/basis.hpp"
+#include "bc/boundary_condition.hpp"
+#include "physics/euler.hpp"
+#include "physics/navierstokes.hpp"
 
 #ifdef ZJ_REF_GPU
 #include <cuda_runtime.h>
@@ -206,6 +209,44 @@ int cmd_gmsh(const char* path, const char* out) {
     return 0;
 }
 
+// "phys in.bin out.bin gamma Mach AoA rho_inf p_inf p_total T_total dx dy p_static T_wall"
+// in: int64 N, then N x (UL[4], UR[4], nx, ny) f64.  out per record:
+// Rusanov, Roe, HLLC fluxes (euler.hpp:184-375), then ghost states of
+// NoSlipWall, IsothermalWall, SlipWall, Symmetry, FarField (fromMach), SubsonicInflow,
+// SubsonicOutflow (boundary_condition.hpp:42-311) from UL.
+int cmd_phys(char** a) {
+    Reader r(a[0]);
+    const int64_t n = r.get<int64_t>();
+    std::vector<double> in; r.arr(in, n * 10);
+    const double g = std::atof(a[2]), mach = std::atof(a[3]), aoa = std::atof(a[4]);
+    const double rho_inf = std::atof(a[5]), p_inf = std::atof(a[6]);
+    const double pt = std::atof(a[7]), Tt = std::atof(a[8]), dx = std::atof(a[9]), dy = std::atof(a[10]);
+    const double ps = std::atof(a[11]), Tw = std::atof(a[12]);
+    NoSlipWallBC wall(g);
+    IsothermalWallBC iso(Tw, g);
+    SlipWallBC slip(g);
+    SymmetryBC sym(g);
+    auto ff = FarFieldBC::fromMach(mach, aoa, rho_inf, p_inf, g);
+    SubsonicInflowBC inflow(pt, Tt, dx, dy, g);
+    SubsonicOutflowBC outflow(ps, g);
+    const BoundaryCondition* bcs[7] = {&wall, &iso, &slip, &sym, ff.get(), &inflow, &outflow};
+    Writer w(a[1]);
+    for (int64_t k = 0; k < n; ++k) {
+        const double* q = &in[k * 10];
+        State UL, UR;
+        for (int v = 0; v < 4; ++v) { UL[v] = q[v]; UR[v] = q[4 + v]; }
+        const double nx = q[8], ny = q[9];
+        State F[3] = {RiemannSolvers::rusanov(UL, UR, nx, ny, g), RiemannSolvers::roe(UL, UR, nx, ny, g),
+                      RiemannSolvers::hllc(UL, UR, nx, ny, g)};
+        for (auto& f : F) for (int v = 0; v < 4; ++v) w.put(f[v]);
+        for (auto* bc : bcs) {
+            State gs = bc->ghostState(UL, nx, ny);
+            for (int v = 0; v < 4; ++v) w.put(gs[v]);
+        }
+    }
+    return 0;
+}
+
 #ifdef ZJ_REF_GPU
 // params: "P gamma rho_inf p_inf Mach AoA"
 SimParams make_params(char** a) {
@@ -266,6 +307,7 @@ int main(int argc, char** argv) {
     if (cmd == "ops" && argc == 4) return cmd_ops(std::atoi(argv[2]), argv[3]);
     if (cmd == "mesh" && argc == 5) return cmd_mesh(argv[2], std::atoi(argv[3]), argv[4]);
     if (cmd == "gmsh" && argc == 4) return cmd_gmsh(argv[2], argv[3]);
+    if (cmd == "phys" && argc == 15) return cmd_phys(argv + 2);
 #ifdef ZJ_REF_GPU
     if ((cmd == "rhs" && argc == 11) || (cmd == "step" && argc == 13)) return cmd_gpu(argc, argv);
 #endif

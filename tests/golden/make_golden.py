@@ -82,6 +82,34 @@ def run(cmd):
     return r
 
 
+# Pointwise physics pins: state pairs covering every branch of the reference's
+# Riemann solvers and ghost states (subsonic/supersonic, both wave directions,
+# near-vacuum densities).
+PHYS_PARAMS = dict(g=1.4, mach=0.5, aoa=10.0, rho_inf=1.2, p_inf=1.0e5, p_total=1.2e5,
+                   T_total=300.0, dx=1.0, dy=0.5, p_static=0.9e5, T_wall=350.0)
+
+
+def phys_samples(n=400, seed=21):
+    r = M.uniform01(seed, n * 10).reshape(n, 10)
+    g = PHYS_PARAMS["g"]
+    out = np.empty((n, 10))
+    for k in range(n):
+        rho = 1.2 * (0.2 + 1.8 * r[k, :2])
+        if k % 37 == 0:
+            rho = rho * 1e-9
+        p = 1.0e5 * (0.2 + 1.8 * r[k, 2:4])
+        c = np.sqrt(g * p / rho)
+        mach = 3.0 * (2.0 * r[k, 4:6] - 1.0)          # up to supersonic both ways
+        ang = 2.0 * np.pi * r[k, 6:8]
+        u = mach * c * np.cos(ang)
+        v = mach * c * np.sin(ang)
+        UL = M.prim_to_cons(rho[0], u[0], v[0], p[0], g)
+        UR = M.prim_to_cons(rho[1], u[1], v[1], p[1], g)
+        th = 2.0 * np.pi * r[k, 8]
+        out[k] = np.concatenate([UL, UR, [np.cos(th), np.sin(th)]])
+    return out
+
+
 def gen_cpu(out):
     tmp = tempfile.mkdtemp()
     ops = {}
@@ -105,6 +133,17 @@ def gen_cpu(out):
             geo[f"{key}_face_{fld}"] = np.asarray(faces[fld])
         geo[f"{key}_J"], geo[f"{key}_Jinv"], geo[f"{key}_spxy"], geo[f"{key}_area"] = J, Ji, sxy, area
     np.savez_compressed(os.path.join(out, "ref_geometry.npz"), **geo)
+    smp = phys_samples()
+    fin = os.path.join(tmp, "phys_in.bin")
+    with open(fin, "wb") as f:
+        f.write(np.int64(smp.shape[0]).tobytes())
+        f.write(smp.tobytes())
+    fo = os.path.join(tmp, "phys_out.bin")
+    P_ = PHYS_PARAMS
+    run([O.REF_CPU, "phys", fin, fo] + [repr(P_[k]) for k in
+        ("g", "mach", "aoa", "rho_inf", "p_inf", "p_total", "T_total", "dx", "dy", "p_static", "T_wall")])
+    res = np.fromfile(fo, dtype=np.float64).reshape(smp.shape[0], 10, 4)
+    np.savez_compressed(os.path.join(out, "ref_physics.npz"), samples=smp, out=res)
     print("cpu goldens written to", out)
 
 

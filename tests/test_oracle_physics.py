@@ -1,0 +1,143 @@
+"""The physics-mode oracle (conservative FR, VCJH, the reference's Riemann
+solvers and ghost states).  No reference residual exists for this mode
+(parity unpinned at the residual level); its pieces are pinned pointwise to
+the reference's own header code and the assembled scheme is checked for the
+properties FR must have: freestream preservation on jittered meshes, discrete
+conservation, VCJH identities and the design order of accuracy."""
+import math
+import os
+
+import numpy as np
+import pytest
+
+from tests.golden import make_golden as G
+from zhijian_b200 import meshgen as M
+
+GOLD = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+
+
+@pytest.fixture(scope="module")
+def phys():
+    return np.load(os.path.join(GOLD, "ref_physics.npz"))
+
+
+@pytest.mark.parametrize("which", [0, 1, 2])
+def test_riemann_solvers_bitwise_vs_reference(oracle_mod, phys, which):
+    smp, ref = phys["samples"], phys["out"]
+    g = G.PHYS_PARAMS["g"]
+    got = np.array([oracle_mod.riemann_point(which, s[:4], s[4:8], s[8], s[9], g) for s in smp])
+    assert np.array_equal(got, ref[:, which])
+
+
+def _ghost_oracle(oracle_mod):
+    P_ = G.PHYS_PARAMS
+    tags = [(1, 1, 0.0), (2, 1, 0.0), (3, 2, 0.0), (4, 3, 0.0), (5, 4, 0.0), (6, 5, 0.0),
+            (7, 6, P_["p_static"])]
+    orc = oracle_mod.Oracle(G.mixed_mesh(), 3, P_["g"], P_["rho_inf"], P_["p_inf"], P_["mach"],
+                            P_["aoa"], tags=tags)
+    orc.set_physics(2, 0, False, 1000.0, 0.72, 300.0)
+    orc.set_bc_extra([(2, 0.0, 0.0, 1.0, 0.0, P_["T_wall"]),
+                      (6, P_["p_total"], P_["T_total"], P_["dx"], P_["dy"], 0.0)])
+    return orc
+
+
+@pytest.mark.parametrize("k,bct,tag", [(0, 1, 1), (1, 1, 2), (2, 2, 3), (3, 3, 4), (4, 4, 5),
+                                       (5, 5, 6), (6, 6, 7)])
+def test_ghost_states_bitwise_vs_reference(oracle_mod, phys, k, bct, tag):
+    smp, ref = phys["samples"], phys["out"]
+    orc = _ghost_oracle(oracle_mod)
+    got = np.array([orc.ghost(bct, tag, s[:4], s[8], s[9]) for s in smp])
+    assert np.array_equal(got, ref[:, 3 + k])
+
+
+def _legendre(n, x):
+    return np.polynomial.legendre.legval(x, [0] * n + [1])
+
+
+def _dlegendre(n, x):
+    return np.polynomial.legendre.legval(x, np.polynomial.legendre.legder([0] * n + [1]))
+
+
+@pytest.mark.parametrize("P", [1, 2, 3, 4, 5])
+def test_vcjh_identities(oracle_mod, P):
+    orc = oracle_mod.Oracle(M.vortex_mesh(2), P)
+    pts = orc.operators()["pts"]
+    w = np.polynomial.legendre.leggauss(P + 1)[1]
+    ref_corr = np.load(os.path.join(GOLD, "ref_operators.npz"))[f"P{P}_corr"]
+    for ft in range(4):
+        orc.set_physics(ft)
+        gL, gR = orc.vcjh()
+        # g_R rises from 0 to 1 and g_L falls from 1 to 0 on [-1, 1]
+        assert abs(np.dot(w, gR) - 1.0) < 1e-13 and abs(np.dot(w, gL) + 1.0) < 1e-13
+        if ft == 0:   # DG = the right/left Radau polynomials the reference always uses
+            assert np.array_equal(gR, ref_corr[1][:P + 1])
+            assert np.array_equal(gL, ref_corr[3][:P + 1])
+        if ft == 1:   # SD: g_R = (1+x)/2 P_p(x)  (Huynh's g_Ga)
+            d = 0.5 * _legendre(P, pts) + 0.5 * (1 + pts) * _dlegendre(P, pts)
+            assert np.allclose(gR, d, atol=1e-12)
+        if ft == 2:   # Huynh g2 = (p R_{R,p+1} + (p+1) R_{R,p}) / (2p+1)
+            RR = lambda k, x: 0.5 * (_dlegendre(k, x) + _dlegendre(k - 1, x))
+            d = (P * RR(P + 1, pts) + (P + 1) * RR(P, pts)) / (2 * P + 1)
+            assert np.allclose(gR, d, atol=1e-12)
+
+
+def _farfield_box(n, jitter, seed, P, rho=1.2, p=1.0e5, mach=0.4, aoa=25.0):
+    mesh = M.structured_quads(n, n, -1.0, 1.0, -1.0, 1.0, jitter, seed, (1, 1, 1, 1),
+                              {1: "farfield"})
+    return mesh, dict(gamma=1.4, rho_inf=rho, p_inf=p, Mach=mach, AoA=aoa)
+
+
+@pytest.mark.parametrize("riemann", [0, 1, 2])
+@pytest.mark.parametrize("P", [1, 3, 5])
+def test_freestream_preserved_on_jittered_mesh(oracle_mod, P, riemann):
+    mesh, kw = _farfield_box(6, 0.2, 4, P)
+    orc = oracle_mod.Oracle(mesh, P, **kw)
+    orc.set_physics(2, riemann)
+    c = math.sqrt(1.4 * kw["p_inf"] / kw["rho_inf"])
+    u = kw["Mach"] * c * math.cos(math.radians(kw["AoA"]))
+    v = kw["Mach"] * c * math.sin(math.radians(kw["AoA"]))
+    U = np.broadcast_to(M.prim_to_cons(kw["rho_inf"], u, v, kw["p_inf"], 1.4),
+                        (orc.n_elem, orc.nsp, 4)).copy()
+    R = orc.rhs_phys(U)
+    flux = (kw["p_inf"] + U[0, 0, 3]) * c
+    assert np.abs(R).max() <= 1e-11 * flux
+
+
+@pytest.mark.parametrize("riemann", [0, 1, 2])
+def test_mass_and_energy_conserved_in_slip_wall_box(oracle_mod, riemann):
+    P = 3
+    mesh = M.tgv_mesh(8, seed=5)
+    orc = oracle_mod.Oracle(mesh, P, 1.4, 1.0, 1.0 / (1.4 * 0.09), 0.3, 0.0)
+    orc.set_physics(2, riemann)
+    U = M.taylor_green(orc.sp_coords())
+    R = orc.rhs_phys(U)
+    J, _ = orc.geometry()
+    w1 = np.polynomial.legendre.leggauss(P + 1)[1]
+    w = np.outer(w1, w1).ravel()           # sp = j*(P+1) + i
+    tot = np.einsum("s,es,esv->v", w, J, R)
+    scale = np.einsum("s,es,esv->", w, J, np.abs(R))   # all variables: a flux-sized scale
+    assert abs(tot[0]) <= 1e-13 * scale
+    assert abs(tot[3]) <= 1e-13 * scale
+
+
+@pytest.mark.parametrize("P", [2, 3])
+def test_design_order_on_the_isentropic_vortex(oracle_mod, P):
+    """Residual error against the exact dU/dt = -u_inf dU/dx of the advected
+    (exact) isentropic vortex, in the vortex core, on two uniform meshes:
+    observed order >= P - 0.5."""
+    errs = []
+    for n in (16, 32):
+        mesh = M.structured_quads(n, n, -5.0, 5.0, -5.0, 5.0, 0.0, 0, (1, 1, 1, 1),
+                                  {1: "farfield"})
+        orc = oracle_mod.Oracle(mesh, P, 1.4, 1.0, 1.0, 0.5 / math.sqrt(1.4), 0.0)
+        orc.set_physics(2, 1)
+        xy = orc.sp_coords()
+        U = M.shu_vortex(xy, 1.4)
+        R = orc.rhs_phys(U)
+        h = 1e-5
+        dUdx = (M.shu_vortex(xy + [h, 0.0], 1.4) - M.shu_vortex(xy - [h, 0.0], 1.4)) / (2 * h)
+        exact = -0.5 * dUdx
+        core = (np.hypot(xy[..., 0], xy[..., 1]) < 2.5)
+        errs.append(np.abs(R - exact)[core].max())
+    order = math.log2(errs[0] / errs[1])
+    assert order >= P - 0.5, (errs, order)
