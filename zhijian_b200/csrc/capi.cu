@@ -104,9 +104,15 @@ zj_status validate_params(const zj_params* p, std::string& msg) {
     if (p->flux_type < 0 || p->flux_type > 3) { msg = "flux_type must be DG, SD, HU or GA"; return ZJ_ERR_ARG; }
     if (p->riemann < 0 || p->riemann > 2) { msg = "riemann must be Rusanov, Roe or HLLC"; return ZJ_ERR_ARG; }
     if (p->n_bc < 0 || p->n_bc > ZJ_MAX_BC) { msg = "n_bc out of range"; return ZJ_ERR_ARG; }
-    if (!p->compat) { msg = "physics mode (compat off) is not built yet"; return ZJ_ERR_UNSUPPORTED; }
+    if (!p->compat && p->viscous) { msg = "viscous physics mode is not built yet"; return ZJ_ERR_UNSUPPORTED; }
     if (p->precision != ZJ_FP64) { msg = "the mixed-precision form is not built yet"; return ZJ_ERR_UNSUPPORTED; }
     return ZJ_OK;
+}
+
+// One residual or RK-stage launch in the handle's mode.
+cudaError_t launch_stage(const zj_solver* s, const StageArgs& a) {
+    if (s->prm.compat) return launch_compat_stage(s->P, a, s->stream, nullptr);
+    return launch_phys_stage(s->P, s->prm.riemann, a, s->stream);
 }
 
 StageArgs base_args(const zj_solver* s) {
@@ -130,15 +136,15 @@ zj_status enqueue_step(zj_solver* s) {
     // stage 1: U(1) = U0 + dt R(U0)
     a.U = s->dU[c]; a.U0 = s->dU[c]; a.Uout = s->dU[a1]; a.Tin = s->dT[p]; a.Tout = s->dT[1 - p];
     a.stage = 1;
-    ZJ_CK(s, launch_compat_stage(s->P, a, s->stream, nullptr), "stage 1 launch");
+    ZJ_CK(s, launch_stage(s, a), "stage 1 launch");
     // stage 2: U(2) = 3/4 U0 + 1/4 U(1) + 1/4 dt R(U(1))
     a.U = s->dU[a1]; a.Uout = s->dU[b1]; a.Tin = s->dT[1 - p]; a.Tout = s->dT[p];
     a.stage = 2;
-    ZJ_CK(s, launch_compat_stage(s->P, a, s->stream, nullptr), "stage 2 launch");
+    ZJ_CK(s, launch_stage(s, a), "stage 2 launch");
     // stage 3: U = 1/3 U0 + 2/3 U(2) + 2/3 dt R(U(2))
     a.U = s->dU[b1]; a.Uout = s->dU[a1]; a.Tin = s->dT[p]; a.Tout = s->dT[1 - p];
     a.stage = 3;
-    ZJ_CK(s, launch_compat_stage(s->P, a, s->stream, nullptr), "stage 3 launch");
+    ZJ_CK(s, launch_stage(s, a), "stage 3 launch");
     s->cur = a1;
     s->tpar = 1 - p;
     return ZJ_OK;
@@ -170,7 +176,12 @@ zj_status zj_solver_create(const zj_mesh_desc* mesh, const zj_params* params, zj
     if (!build_mesh(mesh, params, s->mesh, msg)) { delete s; return fail(nullptr, ZJ_ERR_ARG, msg); }
     s->E = s->mesh.n_elem;
     if (s->E > (1LL << 31) / (4LL * s->nsp)) { delete s; return fail(nullptr, ZJ_ERR_ARG, "mesh too large"); }
-    build_operators_compat(s->P, s->ops);
+    if (!params->compat && s->mesh.order != 1) {
+        delete s;
+        return fail(nullptr, ZJ_ERR_UNSUPPORTED, "physics mode needs straight-edged (Q1) elements");
+    }
+    if (params->compat) build_operators_compat(s->P, s->ops);
+    else build_operators_vcjh(s->P, params->flux_type, s->ops);
     std::vector<double> J, Jinv, bc, nrm, area, packed;
     std::vector<EdgeRec> rec;
     if (!build_metrics(s->mesh, s->ops, J, Jinv, msg)) { delete s; return fail(nullptr, ZJ_ERR_ARG, msg); }
@@ -326,7 +337,7 @@ zj_status zj_rhs(zj_solver* s, const double* U_dev, double* R_dev) {
     StageArgs a = base_args(s);
     a.U = U_dev; a.U0 = U_dev; a.Uout = nullptr; a.Tin = s->dT[2]; a.Tout = nullptr;
     a.R = R_dev; a.partials = s->dPartR; a.stage = 0;
-    ZJ_CK(s, launch_compat_stage(s->P, a, s->stream, nullptr), "residual launch");
+    ZJ_CK(s, launch_stage(s, a), "residual launch");
     return ZJ_OK;
 }
 
@@ -436,7 +447,7 @@ zj_status zj_rhs_noalloc(zj_solver* s, const double* U_dev, double* R_dev) {
     StageArgs a = base_args(s);
     a.U = U_dev; a.U0 = U_dev; a.Uout = nullptr; a.Tin = traces; a.Tout = nullptr;
     a.R = R_dev; a.partials = partials; a.stage = 0;
-    ZJ_CK(s, launch_compat_stage(s->P, a, s->stream, nullptr), "residual launch");
+    ZJ_CK(s, launch_stage(s, a), "residual launch");
     return ZJ_OK;
 }
 

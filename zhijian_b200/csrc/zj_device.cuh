@@ -1,0 +1,115 @@
+// zj_device.cuh -- device helpers shared by the residual kernels: CTA shape
+// of an element block, vectorised global/shared accesses, the branch-free
+// trace of a flux point, block reductions.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "zj_math.h"
+
+namespace zj {
+namespace dev {
+
+template <int P>
+struct Shape {
+    static constexpr int N1 = P + 1;
+    static constexpr int NSP = N1 * N1;
+    static constexpr int NFT = 4 * N1;                 // flux points per element
+    static constexpr int TPE = NSP > NFT ? NSP : NFT;  // threads per element
+    static constexpr int EB = (256 / TPE) > 0 ? (256 / TPE) : 1;
+    static constexpr int THREADS = EB * TPE;
+    static constexpr int NOPS = N1 * N1 + 4 * N1;
+    // Shared-memory layout of per-element fields (doubles): [var][eta row][xi]
+    // with rows padded to an even length so every row starts 16-byte aligned
+    // (vector loads), and a per-element stride of 6 mod 16 so the elements
+    // that share a warp start on different banks.  Flux differences use
+    // [flux point][var] with a per-element stride of 2 mod 16.
+    static constexpr int RS = (N1 + 1) & ~1;
+    static constexpr int VS = N1 * RS;
+    static constexpr int FS = 4 * VS + (6 - (4 * VS) % 16 + 16) % 16;
+    static constexpr int DS = 4 * NFT + 2;
+};
+
+__device__ __forceinline__ void load4(const double* p, double* v) {
+    const double2 a = *reinterpret_cast<const double2*>(p);
+    const double2 b = *reinterpret_cast<const double2*>(p + 2);
+    v[0] = a.x; v[1] = a.y; v[2] = b.x; v[3] = b.y;
+}
+__device__ __forceinline__ void load4_nc(const double* p, double* v) {
+    const double2 a = __ldg(reinterpret_cast<const double2*>(p));
+    const double2 b = __ldg(reinterpret_cast<const double2*>(p + 2));
+    v[0] = a.x; v[1] = a.y; v[2] = b.x; v[3] = b.y;
+}
+__device__ __forceinline__ void store4(double* p, const double* v) {
+    *reinterpret_cast<double2*>(p) = make_double2(v[0], v[1]);
+    *reinterpret_cast<double2*>(p + 2) = make_double2(v[2], v[3]);
+}
+
+// 1/x: Newton-Raphson for positive normal x, IEEE division otherwise (zero,
+// negative or non-finite densities, which the reference also divides by).
+__device__ __forceinline__ double rcp_any(double x) {
+    return (x > 1e-300 && x < 1e300) ? zj_rcp(x) : 1.0 / x;
+}
+
+__device__ __forceinline__ void prefetch_l2(const void* p) {
+    asm volatile("prefetch.global.L2 [%0];" ::"l"(p));
+}
+
+// N values of a 16-byte aligned shared-memory row, with 16-byte loads.
+template <int N>
+__device__ __forceinline__ void load_row(const double* row, double* out) {
+#pragma unroll
+    for (int m = 0; m + 1 < N; m += 2) {
+        const double2 t = *reinterpret_cast<const double2*>(row + m);
+        out[m] = t.x;
+        out[m + 1] = t.y;
+    }
+    if (N & 1) out[N - 1] = row[N - 1];
+}
+
+// Trace of one flux point from a state held in shared memory as
+// s[var*VS + j*RS + i] (i: xi index, j: eta index).  Edge parametrisations
+// follow FROperators::initQuad (basis.cpp:540-552): edges 0,1 run with +s,
+// edges 2,3 with -s, so fp on edges 2,3 meets xi/eta index N1-1-fp.  The sum
+// runs over the index the reference's dense row has nonzero weights on,
+// ascending:  edge 0: sum_j l_j(-1) s[j][fp]     edge 1: sum_i l_i(1) s[fp][i]
+//             edge 2: sum_j l_j(1) s[j][N1-1-fp] edge 3: sum_i l_i(-1) s[N1-1-fp][i]
+// Written without branches on the edge (the four edges share a warp).
+template <int N1, int RS, int VS>
+__device__ __forceinline__ void trace_point(const double* s, const double* Lm, const double* Lp,
+                                            int edge, int fp, double* out) {
+    const int line = (edge >= 2) ? (N1 - 1 - fp) : fp;
+    const bool along_eta = (edge == 0 || edge == 2);
+    const int base = along_eta ? line : line * RS;
+    const int stride = along_eta ? RS : 1;
+    const double* W = (edge == 0 || edge == 3) ? Lm : Lp;
+    double w[N1];
+#pragma unroll
+    for (int m = 0; m < N1; ++m) w[m] = W[m];
+#pragma unroll
+    for (int v = 0; v < 4; ++v) {
+        const double* sv = s + v * VS + base;
+        double t = 0.0;
+#pragma unroll
+        for (int m = 0; m < N1; ++m) t = fma(w[m], sv[m * stride], t);
+        out[v] = t;
+    }
+}
+
+// Block-wide deterministic sum; result valid in thread 0.
+__device__ __forceinline__ double block_sum(double x, double* red) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) x += __shfl_down_sync(0xffffffffu, x, o);
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    if (lane == 0) red[w] = x;
+    __syncthreads();
+    double s = 0.0;
+    if (threadIdx.x == 0) {
+        const int nw = (blockDim.x + 31) >> 5;
+        for (int i = 0; i < nw; ++i) s += red[i];
+    }
+    return s;
+}
+
+}  // namespace dev
+}  // namespace zj

@@ -34,6 +34,8 @@ void pack_ops(const Operators1D& o, std::vector<double>& out);
 
 // Compat-mode FP64 launches (reference residual semantics).
 cudaError_t launch_compat_stage(int P, const StageArgs& a, cudaStream_t s, int* grid_out);
+// Physics-mode FP64 launches (conservative FR, VCJH, selected Riemann solver).
+cudaError_t launch_phys_stage(int P, int riemann, const StageArgs& a, cudaStream_t s);
 cudaError_t launch_traces(int P, const double* U, double* T, const double* ops,
                           long long n_elem, cudaStream_t s);
 int stage_grid(int P, long long n_elem);

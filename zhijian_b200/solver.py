@@ -16,7 +16,7 @@ from .meshgen import QuadMesh
 
 def make_params(poly_order=3, gamma=1.4, rho_inf=1.0, p_inf=1.0 / 1.4, Mach=0.5, AoA=0.0,
                 flux_type="HU", riemann="Rusanov", CFL=0.5, viscous=False, Re=1000.0,
-                Pr=0.72, compat=True, precision="fp64", bcs=(), config_text=None):
+                Pr=0.72, compat=True, precision="fp64", bcs=(), config_text=None, T_inf=300.0):
     """A zj_params with the reference defaults, then the given values.
     bcs: iterable of (tag, type name[, p_static]).  config_text is parsed
     with the reference grammar after the keyword values."""
@@ -35,16 +35,23 @@ def make_params(poly_order=3, gamma=1.4, rho_inf=1.0, p_inf=1.0 / 1.4, Mach=0.5,
     p.viscous = int(bool(viscous))
     p.Re = Re
     p.Pr = Pr
+    p.T_inf = T_inf
     p.compat = int(bool(compat))
     p.precision = L.FP64 if precision == "fp64" else L.MIXED
     p.n_bc = 0
     for b in bcs:
-        tag, name = b[0], b[1]
+        # (tag, type[, p_static]) or a dict with keys tag, type, p_static,
+        # p_total, T_total, T_wall, dir_x, dir_y
+        d = dict(b) if isinstance(b, dict) else dict(tag=b[0], type=b[1],
+                                                    p_static=b[2] if len(b) > 2 else 0.0)
         s = p.bc[p.n_bc]
-        s.tag = int(tag)
-        s.type = L.BC_TYPES[name] if isinstance(name, str) else int(name)
-        s.p_static = float(b[2]) if len(b) > 2 else 0.0
-        s.dir_x, s.dir_y = 1.0, 0.0
+        s.tag = int(d["tag"])
+        s.type = L.BC_TYPES[d["type"]] if isinstance(d["type"], str) else int(d["type"])
+        s.p_static = float(d.get("p_static", 0.0))
+        s.p_total = float(d.get("p_total", 0.0))
+        s.T_total = float(d.get("T_total", 0.0))
+        s.T_wall = float(d.get("T_wall", 0.0))
+        s.dir_x, s.dir_y = float(d.get("dir_x", 1.0)), float(d.get("dir_y", 0.0))
         p.n_bc += 1
     if config_text is not None:
         L.check(lib.zj_params_parse_string(config_text.encode(), C.byref(p)))
