@@ -1047,6 +1047,27 @@ void orc_get_vcjh(const orc_ctx* c, double* gL, double* gR) {
     for (int j = 0; j < c->n1; ++j) { gL[j] = c->gLp[j]; gR[j] = c->gRp[j]; }
 }
 
+/* Viscous flux of computeViscousFluxSPKernel (kernels.cu:742-786): velocity
+ * and temperature gradients from the conservative gradients, mu = T^0.7/Re,
+ * k = mu gamma/((gamma-1) Pr), Stokes hypothesis. */
+void orc_viscous_flux(const double* s, const double* dx, const double* dy, double g, double Re,
+                      double Pr, double* Fv, double* Gv) {
+    double rho = s[0], u = s[1] / rho, v = s[2] / rho;
+    double dudx = (dx[1] - u * dx[0]) / rho, dudy = (dy[1] - u * dy[0]) / rho;
+    double dvdx = (dx[2] - v * dx[0]) / rho, dvdy = (dy[2] - v * dy[0]) / rho;
+    double p = pressure_raw(s, g), T = p / rho;
+    double dpdx = (g - 1.0) * (dx[3] - 0.5 * dx[0] * (u * u + v * v) - rho * (u * dudx + v * dvdx));
+    double dpdy = (g - 1.0) * (dy[3] - 0.5 * dy[0] * (u * u + v * v) - rho * (u * dudy + v * dvdy));
+    double dTdx = (dpdx - T * dx[0]) / rho, dTdy = (dpdy - T * dy[0]) / rho;
+    double mu = pow(T, 0.7) / Re;
+    double k = mu * g / ((g - 1.0) * Pr);
+    double div = dudx + dvdy, lam = -2.0 / 3.0 * mu;
+    double txx = 2.0 * mu * dudx + lam * div, tyy = 2.0 * mu * dvdy + lam * div;
+    double txy = mu * (dudy + dvdx);
+    Fv[0] = 0.0; Fv[1] = txx; Fv[2] = txy; Fv[3] = u * txx + v * txy + k * dTdx;
+    Gv[0] = 0.0; Gv[1] = txy; Gv[2] = tyy; Gv[3] = u * txy + v * tyy + k * dTdy;
+}
+
 void orc_rhs_phys(orc_ctx* c, const double* U, double* R) {
     const int nsp = c->nsp, n1 = c->n1, nfp = c->nfp;
     const int64_t ne = c->n_elem, nf = c->n_faces;
@@ -1056,11 +1077,87 @@ void orc_rhs_phys(orc_ctx* c, const double* U, double* R) {
     size_t fpn = (size_t)ne * 4 * nfp * 4;
     double* Ft = c->Fx; double* Gt = c->Fy;          /* transformed fluxes at sp */
     double* FnD = (double*)malloc(sizeof(double) * fpn);
-    /* transformed fluxes F~ = J (xi_x F + xi_y G), G~ = J (eta_x F + eta_y G) */
+    /* traces of the state (dense interp) */
+#pragma omp parallel for num_threads(nt) schedule(static)
+    for (int64_t e = 0; e < ne; ++e)
+        for (int t = 0; t < 4 * nfp; ++t) {
+            const double* w = c->interp + t * nsp;
+            for (int v = 0; v < 4; ++v) {
+                double su = 0.0;
+                for (int sp = 0; sp < nsp; ++sp) su += w[sp] * U[(e * nsp + sp) * 4 + v];
+                c->Ufp[((e * 4) * nfp + t) * 4 + v] = su;
+            }
+        }
+    /* Navier-Stokes: corrected gradient with the common solution
+     * U_c = (U_L + U_R)/2 at every face point (ghost state on boundaries),
+     * Q = grad U at the solution points, and its traces. */
+    double *Q = NULL, *Qfp = NULL;
+    if (c->viscous) {
+        double* dU = (double*)calloc(fpn, sizeof(double));
+        Q = (double*)malloc(sizeof(double) * (size_t)ne * nsp * 8);
+        Qfp = (double*)malloc(sizeof(double) * fpn * 2);
+#pragma omp parallel for num_threads(nt) schedule(static)
+        for (int64_t f = 0; f < nf; ++f) {
+            int le = c->fle[f], ll = c->fll[f], re = c->fre[f], rl = c->frl[f];
+            double nx = c->fn[2 * f], ny = c->fn[2 * f + 1];
+            for (int fp = 0; fp < nfp; ++fp) {
+                int64_t lo = (((int64_t)le * 4 + ll) * nfp + fp) * 4;
+                const double* UL = c->Ufp + lo;
+                double UR[4];
+                int64_t ro = -1;
+                if (re >= 0) {
+                    ro = (((int64_t)re * 4 + rl) * nfp + (nfp - 1 - fp)) * 4;
+                    for (int v = 0; v < 4; ++v) UR[v] = c->Ufp[ro + v];
+                } else {
+                    orc_ghost_point(c, c->fbct[f], c->ftag[f], UL, nx, ny, UR);
+                }
+                for (int v = 0; v < 4; ++v) {
+                    double uc = 0.5 * (UL[v] + UR[v]);
+                    dU[lo + v] = uc - UL[v];
+                    if (ro >= 0) dU[ro + v] = uc - UR[v];
+                }
+            }
+        }
+#pragma omp parallel for num_threads(nt) schedule(static)
+        for (int64_t e = 0; e < ne; ++e)
+            for (int sp = 0; sp < nsp; ++sp) {
+                int i = sp % n1, j = sp / n1;
+                const double* D = dU + e * 4 * nfp * 4;
+                const double* Ji = c->Jinv + (e * nsp + sp) * 4;
+                for (int v = 0; v < 4; ++v) {
+                    double dxi = 0.0, deta = 0.0;
+                    for (int k = 0; k < nsp; ++k) {
+                        dxi += c->dxi[sp * nsp + k] * U[(e * nsp + k) * 4 + v];
+                        deta += c->deta[sp * nsp + k] * U[(e * nsp + k) * 4 + v];
+                    }
+                    dxi += c->gRp[i] * D[(1 * nfp + j) * 4 + v] + c->gLp[i] * D[(3 * nfp + (nfp - 1 - j)) * 4 + v];
+                    deta += c->gLp[j] * D[(0 * nfp + i) * 4 + v] + c->gRp[j] * D[(2 * nfp + (nfp - 1 - i)) * 4 + v];
+                    Q[(e * nsp + sp) * 8 + v] = Ji[0] * dxi + Ji[2] * deta;
+                    Q[(e * nsp + sp) * 8 + 4 + v] = Ji[1] * dxi + Ji[3] * deta;
+                }
+            }
+#pragma omp parallel for num_threads(nt) schedule(static)
+        for (int64_t e = 0; e < ne; ++e)
+            for (int t = 0; t < 4 * nfp; ++t) {
+                const double* w = c->interp + t * nsp;
+                for (int v = 0; v < 8; ++v) {
+                    double sq = 0.0;
+                    for (int sp = 0; sp < nsp; ++sp) sq += w[sp] * Q[(e * nsp + sp) * 8 + v];
+                    Qfp[((e * 4) * nfp + t) * 8 + v] = sq;
+                }
+            }
+        free(dU);
+    }
+    /* transformed total fluxes F~ = J (xi_x (F - Fv) + xi_y (G - Gv)), G~ likewise */
 #pragma omp parallel for num_threads(nt) schedule(static)
     for (int64_t idx = 0; idx < ne * nsp; ++idx) {
         double F[4], G[4];
         flux_xy(U + idx * 4, g, F, G);
+        if (c->viscous) {
+            double Fv[4], Gv[4];
+            orc_viscous_flux(U + idx * 4, Q + idx * 8, Q + idx * 8 + 4, g, c->Re, c->Pr, Fv, Gv);
+            for (int v = 0; v < 4; ++v) { F[v] -= Fv[v]; G[v] -= Gv[v]; }
+        }
         const double* Ji = c->Jinv + idx * 4;
         double J = c->J[idx];
         for (int v = 0; v < 4; ++v) {
@@ -1068,22 +1165,19 @@ void orc_rhs_phys(orc_ctx* c, const double* U, double* R) {
             Gt[idx * 4 + v] = J * (Ji[2] * F[v] + Ji[3] * G[v]);
         }
     }
-    /* traces of U and outward reference-normal transformed flux, dense interp */
+    /* outward reference-normal extrapolated transformed flux, dense interp */
 #pragma omp parallel for num_threads(nt) schedule(static)
     for (int64_t e = 0; e < ne; ++e)
         for (int t = 0; t < 4 * nfp; ++t) {
-            int edge = t / nfp, fp = t % nfp;
-            const double* w = c->interp + (edge * nfp + fp) * nsp;
+            int edge = t / nfp;
+            const double* w = c->interp + t * nsp;
             for (int v = 0; v < 4; ++v) {
-                double su = 0.0, sf = 0.0, sg = 0.0;
+                double sf = 0.0, sg = 0.0;
                 for (int sp = 0; sp < nsp; ++sp) {
-                    su += w[sp] * U[(e * nsp + sp) * 4 + v];
                     sf += w[sp] * Ft[(e * nsp + sp) * 4 + v];
                     sg += w[sp] * Gt[(e * nsp + sp) * 4 + v];
                 }
-                int64_t o = ((e * 4 + edge) * nfp + fp) * 4 + v;
-                c->Ufp[o] = su;
-                FnD[o] = (edge == 0) ? -sg : (edge == 1) ? sf : (edge == 2) ? sg : -sf;
+                FnD[((e * 4) * nfp + t) * 4 + v] = (edge == 0) ? -sg : (edge == 1) ? sf : (edge == 2) ? sg : -sf;
             }
         }
     memset(c->Fdiff, 0, sizeof(double) * fpn);
@@ -1104,6 +1198,21 @@ void orc_rhs_phys(orc_ctx* c, const double* U, double* R) {
                 orc_ghost_point(c, c->fbct[f], c->ftag[f], UL, nx, ny, UR);
             }
             orc_riemann_point(c->riemann, UL, UR, nx, ny, g, Fc);
+            if (c->viscous) {
+                /* BR2Scheme::commonFlux (navierstokes.hpp:177-204): average state
+                 * and gradients; boundaries copy the interior gradient
+                 * (BoundaryCondition::ghostGradient) */
+                const double* QL = Qfp + (lo / 4) * 8;
+                const double* QR = (ro >= 0) ? Qfp + (ro / 4) * 8 : QL;
+                double Ua[4], dxa[4], dya[4], Fv[4], Gv[4];
+                for (int v = 0; v < 4; ++v) {
+                    Ua[v] = 0.5 * (UL[v] + UR[v]);
+                    dxa[v] = 0.5 * (QL[v] + QR[v]);
+                    dya[v] = 0.5 * (QL[4 + v] + QR[4 + v]);
+                }
+                orc_viscous_flux(Ua, dxa, dya, g, c->Re, c->Pr, Fv, Gv);
+                for (int v = 0; v < 4; ++v) Fc[v] -= Fv[v] * nx + Gv[v] * ny;
+            }
             for (int v = 0; v < 4; ++v) c->Fdiff[lo + v] = s * Fc[v] - FnD[lo + v];
             if (ro >= 0)
                 for (int v = 0; v < 4; ++v) c->Fdiff[ro + v] = s * (-Fc[v]) - FnD[ro + v];
@@ -1126,6 +1235,8 @@ void orc_rhs_phys(orc_ctx* c, const double* U, double* R) {
             }
         }
     free(FnD);
+    free(Q);
+    free(Qfp);
 }
 
 void orc_step_phys(orc_ctx* c, double* U, double dt, int nsteps, double* R_last) {

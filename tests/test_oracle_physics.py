@@ -141,3 +141,105 @@ def test_design_order_on_the_isentropic_vortex(oracle_mod, P):
         errs.append(np.abs(R - exact)[core].max())
     order = math.log2(errs[0] / errs[1])
     assert order >= P - 0.5, (errs, order)
+
+
+# ---------------------------------------------------------------- Navier-Stokes --
+
+def _mms_prim(x, y):
+    rho = 1.0 + 0.1 * np.sin(2.0 * x + y)
+    u = 0.3 + 0.1 * np.cos(3.0 * y)
+    v = 0.2 * np.sin(2.0 * x)
+    p = (1.0 + 0.1 * np.cos(x - 2.0 * y)) / 1.4
+    return rho, u, v, p
+
+
+def _mms_U(x, y):
+    rho, u, v, p = _mms_prim(x, y)
+    # conserved variables; complex inputs stay complex (complex-step derivatives)
+    return np.stack([rho, rho * u, rho * v, p / 0.4 + 0.5 * rho * (u * u + v * v)], axis=-1)
+
+
+def _grad_U(x, y):
+    """Exact gradients by complex step."""
+    h = 1e-30
+    dx = np.imag(_mms_U(x + 1j * h, y + 0j)) / h
+    dy = np.imag(_mms_U(x + 0j, y + 1j * h)) / h
+    return dx, dy
+
+
+def _total_flux(oracle_mod, x, y, Re, Pr):
+    import ctypes as C
+    U = _mms_U(x, y)
+    dx, dy = _grad_U(x, y)
+    F = np.empty(U.shape)
+    G = np.empty(U.shape)
+    lib = oracle_mod.lib()
+    lib.orc_viscous_flux.argtypes = [C.POINTER(C.c_double)] * 3 + [C.c_double] * 3 + \
+        [C.POINTER(C.c_double)] * 2
+    d = oracle_mod._d
+    flat = U.reshape(-1, 4)
+    for k in range(flat.shape[0]):
+        s = np.ascontiguousarray(flat[k])
+        a = np.ascontiguousarray(dx.reshape(-1, 4)[k])
+        b = np.ascontiguousarray(dy.reshape(-1, 4)[k])
+        fv, gv = np.empty(4), np.empty(4)
+        lib.orc_viscous_flux(d(s), d(a), d(b), 1.4, Re, Pr, d(fv), d(gv))
+        rho, u, v = s[0], s[1] / s[0], s[2] / s[0]
+        pr = 0.4 * (s[3] - 0.5 * rho * (u * u + v * v))
+        Fi = np.array([s[1], s[1] * u + pr, s[1] * v, (s[3] + pr) * u])
+        Gi = np.array([s[2], s[2] * u, s[2] * v + pr, (s[3] + pr) * v])
+        F.reshape(-1, 4)[k] = Fi - fv
+        G.reshape(-1, 4)[k] = Gi - gv
+    return F, G
+
+
+def _exact_ns_rhs(oracle_mod, xy, Re, Pr, h=1e-3):
+    x, y = xy[..., 0], xy[..., 1]
+    c = [(-2, 1.0 / 12.0), (-1, -8.0 / 12.0), (1, 8.0 / 12.0), (2, -1.0 / 12.0)]
+    div = 0.0
+    for k, w in c:
+        F, _ = _total_flux(oracle_mod, x + k * h, y, Re, Pr)
+        _, G = _total_flux(oracle_mod, x, y + k * h, Re, Pr)
+        div = div + w * (F + G) / h
+    return -div
+
+
+@pytest.mark.parametrize("P", [2, 3])
+def test_navier_stokes_design_order(oracle_mod, P):
+    Re, Pr = 20.0, 0.72
+    errs = []
+    for n in (6, 12):
+        mesh = M.structured_quads(n, n, 0.0, 1.0, 0.0, 1.0, 0.0, 0, (1, 1, 1, 1), {1: "farfield"})
+        orc = oracle_mod.Oracle(mesh, P, 1.4, 1.0, 1.0 / 1.4, 0.3, 0.0)
+        orc.set_physics(2, 1, True, Re, Pr, 300.0)
+        xy = orc.sp_coords()
+        R = orc.rhs_phys(_mms_U(xy[..., 0], xy[..., 1]))
+        ex = _exact_ns_rhs(oracle_mod, xy, Re, Pr)
+        cx, cy = xy[..., 0].mean(1), xy[..., 1].mean(1)
+        inner = (cx > 0.3) & (cx < 0.7) & (cy > 0.3) & (cy < 0.7)
+        errs.append(np.abs(R - ex)[inner].max())
+    # the central (BR1-type) viscous flux of navierstokes.hpp:177-204 makes the
+    # pointwise residual error O(h^(P-1)) for second derivatives
+    order = math.log2(errs[0] / errs[1])
+    assert order >= P - 1.3, (errs, order)
+
+
+def test_navier_stokes_freestream_and_mass(oracle_mod):
+    mesh, kw = _farfield_box(6, 0.2, 4, 3)
+    orc = oracle_mod.Oracle(mesh, 3, **kw)
+    orc.set_physics(2, 1, True, 50.0, 0.72, 300.0)
+    c = math.sqrt(1.4 * kw["p_inf"] / kw["rho_inf"])
+    U = np.broadcast_to(M.prim_to_cons(kw["rho_inf"], kw["Mach"] * c * math.cos(math.radians(25.0)),
+                                       kw["Mach"] * c * math.sin(math.radians(25.0)), kw["p_inf"], 1.4),
+                        (orc.n_elem, orc.nsp, 4)).copy()
+    assert np.abs(orc.rhs_phys(U)).max() <= 1e-11 * (kw["p_inf"] + U[0, 0, 3]) * c
+    box = M.tgv_mesh(8, seed=5)
+    orc = oracle_mod.Oracle(box, 3, 1.4, 1.0, 1.0 / (1.4 * 0.09), 0.3, 0.0)
+    orc.set_physics(2, 1, True, 100.0, 0.72, 300.0)
+    R = orc.rhs_phys(M.taylor_green(orc.sp_coords()))
+    J, _ = orc.geometry()
+    w1 = np.polynomial.legendre.leggauss(4)[1]
+    w = np.outer(w1, w1).ravel()
+    tot = np.einsum("s,es,esv->v", w, J, R)
+    scale = np.einsum("s,es,esv->", w, J, np.abs(R))
+    assert abs(tot[0]) <= 1e-13 * scale
