@@ -121,3 +121,70 @@ def test_physics_mode_rejects_curved_elements(zjlib):
     with pytest.raises(L.ZJError) as e:
         FRSolver(q2, make_params(compat=False))
     assert e.value.code == L.ERR_UNSUPPORTED
+
+
+# ------------------------------------------------------------ Navier-Stokes --
+
+def make_ns_pair(oracle_mod, mesh, bcs, P, flux, riem, Re=50.0, rho=1.2, p=1.0e5, mach=0.4,
+                 aoa=10.0):
+    prm = make_params(poly_order=P, rho_inf=rho, p_inf=p, Mach=mach, AoA=aoa, flux_type=flux,
+                      riemann=riem, compat=False, viscous=True, Re=Re, Pr=0.72, bcs=bcs,
+                      T_inf=8.5e4)
+    s = FRSolver(mesh, prm)
+    tags = [(b["tag"], L.BC_TYPES[b["type"]], b.get("p_static", 0.0)) for b in bcs]
+    orc = oracle_mod.Oracle(mesh, P, 1.4, rho, p, mach, aoa, tags=tags)
+    orc.set_physics(FLUX.index(flux), RIEMANN.index(riem), True, Re, 0.72, 8.5e4)
+    orc.set_bc_extra([(b["tag"], b.get("p_total", 0.0), b.get("T_total", 0.0), b.get("dir_x", 1.0),
+                       b.get("dir_y", 0.0), b.get("T_wall", 0.0)) for b in bcs])
+    return s, orc
+
+
+@pytest.mark.parametrize("P", [1, 2, 3, 4, 5])
+@pytest.mark.parametrize("riem", RIEMANN)
+@pytest.mark.parametrize("bcs", [BCS_A, BCS_B], ids=["A", "B"])
+def test_ns_rhs_matches_physics_oracle(zjlib, oracle_mod, P, riem, bcs):
+    mesh = case_mesh(bcs)
+    flux = FLUX[(P + 2 * RIEMANN.index(riem)) % 4]
+    s, orc = make_ns_pair(oracle_mod, mesh, bcs, P, flux, riem)
+    U = M.random_state(mesh.n_elem, (P + 1) ** 2, 51 + P, 1.4, 1.2, 1.0e5, 0.1)
+    R = s.rhs(U)
+    Ro = orc.rhs_phys(U)
+    scale = T.euler_flux_scale(U, orc.geometry()[1])
+    assert T.rel_err(R, Ro, scale) <= TOL
+
+
+def test_ns_steps_match_physics_oracle(zjlib, oracle_mod):
+    mesh = case_mesh(BCS_A)
+    s, orc = make_ns_pair(oracle_mod, mesh, BCS_A, 3, "HU", "Roe", Re=20.0)
+    U = M.random_state(mesh.n_elem, 16, 79, 1.4, 1.2, 1.0e5, 0.05)
+    s.copyToDevice(U)
+    s.advance(2e-8, 3)
+    Uo, Ro = orc.step_phys(U, 2e-8, 3)
+    assert T.rel_err(s.copyToHost(), Uo, T.euler_flux_scale(Uo)) <= TOL
+    no = float(np.sqrt(np.sum(Ro * Ro)))
+    assert abs(s.computeResidual() - no) <= 1e-11 * no
+
+
+def test_ns_full_size_tgv(zjlib, oracle_mod):
+    """The Taylor-Green configuration of the benchmark (256x256 jittered, P3,
+    Roe, Re 5000, Pr 0.72): residual against the oracle at full size."""
+    import os
+    mesh = M.tgv_mesh(256, seed=1)
+    prm = make_params(poly_order=3, rho_inf=1.0, p_inf=1.0 / (1.4 * 0.09), Mach=0.3, riemann="Roe",
+                      compat=False, viscous=True, Re=5000.0, Pr=0.72, bcs=[(1, "slipwall")])
+    s = FRSolver(mesh, prm)
+    orc = oracle_mod.Oracle(mesh, 3, 1.4, 1.0, 1.0 / (1.4 * 0.09), 0.3, 0.0,
+                            threads=os.cpu_count() or 1)
+    orc.set_physics(2, 1, True, 5000.0, 0.72)
+    U = M.taylor_green(s.solution_point_coords())
+    R = s.rhs(U)
+    Ro = orc.rhs_phys(U)
+    assert T.rel_err(R, Ro, T.euler_flux_scale(U, orc.geometry()[1])) <= TOL
+    # the allocation-free entry point covers the viscous path too
+    import ctypes as C
+    import torch
+    Ud = torch.from_numpy(U).cuda()
+    Rd = torch.empty_like(Ud)
+    torch.cuda.synchronize()
+    code = zjlib.zj_rhs_noalloc(s.h, C.c_void_p(Ud.data_ptr()), C.c_void_p(Rd.data_ptr()))
+    assert code == L.ERR_ARG   # 65 536 P3 elements need 3 trace buffers: above the static limit

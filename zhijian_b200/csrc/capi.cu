@@ -32,6 +32,7 @@ struct zj_solver {
     size_t state_n = 0, trace_n = 0;
     double* dU[3] = {nullptr, nullptr, nullptr};
     double* dT[3] = {nullptr, nullptr, nullptr};
+    double* dTQ = nullptr;      // gradient traces (Navier-Stokes)
     double* dUs = nullptr;      // scratch state (host-buffer residual)
     double* dRs = nullptr;      // scratch residual
     double* dJinv = nullptr;
@@ -86,6 +87,8 @@ cudaError_t dalloc(T** p, size_t n) {
 void free_all(zj_solver* s) {
     for (auto& p : s->dU) { if (p) cudaFree(p); p = nullptr; }
     for (auto& p : s->dT) { if (p) cudaFree(p); p = nullptr; }
+    if (s->dTQ) cudaFree(s->dTQ);
+    s->dTQ = nullptr;
     double** ds[] = {&s->dUs, &s->dRs, &s->dJinv, &s->dJ, &s->dOps, &s->dBC, &s->dH,
                      &s->dScal, &s->dPart, &s->dPartR, &s->dScratch};
     for (auto pp : ds) { if (*pp) cudaFree(*pp); *pp = nullptr; }
@@ -104,15 +107,21 @@ zj_status validate_params(const zj_params* p, std::string& msg) {
     if (p->flux_type < 0 || p->flux_type > 3) { msg = "flux_type must be DG, SD, HU or GA"; return ZJ_ERR_ARG; }
     if (p->riemann < 0 || p->riemann > 2) { msg = "riemann must be Rusanov, Roe or HLLC"; return ZJ_ERR_ARG; }
     if (p->n_bc < 0 || p->n_bc > ZJ_MAX_BC) { msg = "n_bc out of range"; return ZJ_ERR_ARG; }
-    if (!p->compat && p->viscous) { msg = "viscous physics mode is not built yet"; return ZJ_ERR_UNSUPPORTED; }
+    if (!p->compat && p->viscous && !(p->Re > 0.0 && p->Pr > 0.0)) { msg = "Re and Pr must be > 0"; return ZJ_ERR_ARG; }
     if (p->precision != ZJ_FP64) { msg = "the mixed-precision form is not built yet"; return ZJ_ERR_UNSUPPORTED; }
     return ZJ_OK;
 }
 
-// One residual or RK-stage launch in the handle's mode.
+bool is_ns(const zj_solver* s) { return !s->prm.compat && s->prm.viscous; }
+
+// One residual or RK-stage evaluation in the handle's mode: one launch, or
+// the gradient launch then the stage launch for Navier-Stokes.
 cudaError_t launch_stage(const zj_solver* s, const StageArgs& a) {
     if (s->prm.compat) return launch_compat_stage(s->P, a, s->stream, nullptr);
-    return launch_phys_stage(s->P, s->prm.riemann, a, s->stream);
+    if (!is_ns(s)) return launch_phys_stage(s->P, s->prm.riemann, a, s->stream);
+    cudaError_t e = launch_ns_grad(s->P, a, s->stream);
+    if (e != cudaSuccess) return e;
+    return launch_ns_stage(s->P, s->prm.riemann, a, s->stream);
 }
 
 StageArgs base_args(const zj_solver* s) {
@@ -126,6 +135,10 @@ StageArgs base_args(const zj_solver* s) {
     a.dt = s->dScal;
     a.n_elem = s->E;
     a.gamma = s->prm.gamma;
+    a.TQ = s->dTQ;
+    a.TQout = s->dTQ;
+    a.Re = s->prm.Re;
+    a.Pr = s->prm.Pr;
     return a;
 }
 
@@ -200,6 +213,7 @@ zj_status zj_solver_create(const zj_mesh_desc* mesh, const zj_params* params, zj
     if (e == cudaSuccess) e = dalloc(&(ptr), (n));
     for (int i = 0; i < 3; ++i) { ZJ_ALLOC(s->dU[i], s->state_n); }
     for (int i = 0; i < 3; ++i) { ZJ_ALLOC(s->dT[i], s->trace_n); }
+    if (is_ns(s)) { ZJ_ALLOC(s->dTQ, 2 * s->trace_n); }
     ZJ_ALLOC(s->dUs, s->state_n);
     ZJ_ALLOC(s->dRs, s->state_n);
     ZJ_ALLOC(s->dJinv, Jinv.size());
@@ -430,7 +444,7 @@ zj_status zj_rhs_noalloc(zj_solver* s, const double* U_dev, double* R_dev) {
     if (!s || !U_dev || !R_dev) return ZJ_ERR_ARG;
     if ((reinterpret_cast<uintptr_t>(U_dev) | reinterpret_cast<uintptr_t>(R_dev)) & 15u)
         return fail(s, ZJ_ERR_ARG, "U_dev and R_dev must be 16-byte aligned");
-    const size_t trace_bytes = s->trace_n * sizeof(double);
+    const size_t trace_bytes = (is_ns(s) ? 3 : 1) * s->trace_n * sizeof(double);
     const size_t part_bytes = (size_t)s->grid * sizeof(double);
     if (trace_bytes + part_bytes > ZJ_NOALLOC_SCRATCH_BYTES)
         return fail(s, ZJ_ERR_ARG,
@@ -442,11 +456,13 @@ zj_status zj_rhs_noalloc(zj_solver* s, const double* U_dev, double* R_dev) {
     // Every scratch value is written before it is read (all traces by the
     // trace launch, one partial per CTA), so nothing needs clearing.
     double* traces = scratch;
-    double* partials = scratch + s->trace_n;
+    double* grad_traces = scratch + s->trace_n;          // Navier-Stokes only
+    double* partials = scratch + (is_ns(s) ? 3 : 1) * s->trace_n;
     ZJ_CK(s, launch_traces(s->P, U_dev, traces, s->dOps, s->E, s->stream), "trace launch");
     StageArgs a = base_args(s);
     a.U = U_dev; a.U0 = U_dev; a.Uout = nullptr; a.Tin = traces; a.Tout = nullptr;
     a.R = R_dev; a.partials = partials; a.stage = 0;
+    if (is_ns(s)) { a.TQ = grad_traces; a.TQout = grad_traces; }
     ZJ_CK(s, launch_stage(s, a), "residual launch");
     return ZJ_OK;
 }

@@ -26,6 +26,10 @@ struct StageArgs {
     long long n_elem;
     double gamma;
     int stage;              // 0: residual only; 1..3: SSP-RK3 stage
+    // Navier-Stokes
+    const double* TQ;       // gradient traces of U, [E][4 edges][n1][8] = (dU/dx, dU/dy)
+    double* TQout;          // gradient traces written by the gradient launch
+    double Re, Pr;
 };
 
 // Packed operator block: D1[n1*n1], Lm[n1], Lp[n1], gL[n1], gR[n1].
@@ -36,6 +40,9 @@ void pack_ops(const Operators1D& o, std::vector<double>& out);
 cudaError_t launch_compat_stage(int P, const StageArgs& a, cudaStream_t s, int* grid_out);
 // Physics-mode FP64 launches (conservative FR, VCJH, selected Riemann solver).
 cudaError_t launch_phys_stage(int P, int riemann, const StageArgs& a, cudaStream_t s);
+// Navier-Stokes: gradient traces of a stage state, then the stage itself.
+cudaError_t launch_ns_grad(int P, const StageArgs& a, cudaStream_t s);
+cudaError_t launch_ns_stage(int P, int riemann, const StageArgs& a, cudaStream_t s);
 cudaError_t launch_traces(int P, const double* U, double* T, const double* ops,
                           long long n_elem, cudaStream_t s);
 int stage_grid(int P, long long n_elem);
