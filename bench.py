@@ -2,16 +2,20 @@
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
-Workload: the 256x256 jittered (seed 1, +-0.15h) Q1 Taylor-Green mesh on
-[0,pi]^2 with slip walls, P3 (65 536 elements, 1 048 576 DOF per variable),
-TGV initial state at M=0.3.  One bench step = one SSP-RK3 time step = three
-residual evaluations over the whole mesh; DOF-RHS/s = E * n_sp * 3 * K / t.
+Workload: the Taylor-Green configuration -- 256x256 jittered (seed 1,
++-0.15h) Q1 quads on [0,pi]^2 with slip walls, P3 (65 536 elements, 1 048 576
+DOF per variable), u = sin x cos y, v = -cos x sin y, M = 0.3, compressible
+Navier-Stokes with Re = 5000, Pr = 0.72, Roe flux, HU correction, FP64.  One
+bench step = one SSP-RK3 time step = three residual evaluations over the whole
+mesh; DOF-RHS/s = E * n_sp * 3 * K / t.  The same mesh and state in the
+reference's residual semantics (compat: Rusanov, inviscid, clamps) is timed
+as a second line of the JSON ("compat").
 
 ours:      the CUDA path, timed with CUDA events on the solver's stream, max
            over ranks; N > 1 runs one independent replica per GPU (the path
            has no exchange on one GPU; weak scaling).
-reference: the oracle (the CPU restatement of the reference's residual, the
-           reference having no CPU path) with every host thread, rank 0 only.
+reference: the oracle (the CPU restatement of the residual; the reference has
+           no CPU path) on the same workload with every host thread, rank 0.
 """
 from __future__ import annotations
 
@@ -38,8 +42,18 @@ P = 3
 DT = 2.0e-4
 
 
-def workload_name():
-    return f"TGV {NX}x{NX} jittered Q1 quads on [0,pi]^2, slip walls, P{P}, SSP-RK3"
+MODES = {
+    "ns": dict(compat=False, viscous=True, riemann="Roe", flux_type="HU", Re=5000.0, Pr=0.72),
+    "compat": dict(compat=True, viscous=False, riemann="Rusanov", flux_type="HU"),
+}
+
+
+def workload_name(mode="ns"):
+    if mode == "ns":
+        return (f"TGV {NX}x{NX} jittered Q1 quads on [0,pi]^2, slip walls, P{P}, Navier-Stokes "
+                f"Re 5000 Pr 0.72, Roe, HU, SSP-RK3")
+    return (f"TGV {NX}x{NX} jittered Q1 quads on [0,pi]^2, slip walls, P{P}, reference residual "
+            f"semantics (Rusanov, inviscid, clamps), SSP-RK3")
 
 
 def load_peaks():
@@ -132,28 +146,43 @@ def build_case():
     return mesh
 
 
-def make_solver(mesh):
+def make_solver(mesh, mode="ns"):
     from zhijian_b200.solver import FRSolver, make_params
     prm = make_params(poly_order=P, gamma=GAMMA, rho_inf=1.0, p_inf=1.0 / (GAMMA * MACH * MACH),
-                      Mach=MACH, flux_type="HU", riemann="Rusanov", viscous=False,
-                      bcs=[(1, "slipwall")])
+                      Mach=MACH, bcs=[(1, "slipwall")], **MODES[mode])
     return FRSolver(mesh, prm)
 
 
-def cpu_baseline(mesh, seconds=10.0):
-    """The oracle (compat FP64) on the host cores over a bounded sample: SSP-RK3
-    steps on a 64x64-element block of the same mesh density."""
+def make_oracle(mesh, mode, threads):
     from oracle import oracle as O
+    orc = O.Oracle(mesh, P, GAMMA, 1.0, 1.0 / (GAMMA * MACH * MACH), MACH, 0.0, threads=threads)
+    m = MODES[mode]
+    step = orc.step
+    if not m["compat"]:
+        orc.set_physics(2, 1, m["viscous"], m.get("Re", 1000.0), m.get("Pr", 0.72))
+        step = orc.step_phys
+    return orc, step
+
+
+def sample_block():
+    """A 64x64-element block of the benchmark mesh's density (the CPU sample)."""
+    from zhijian_b200 import meshgen as M
+    return M.structured_quads(64, 64, 0.0, math.pi / 4, 0.0, math.pi / 4, 0.15, 1, (1, 1, 1, 1),
+                              {1: "slipwall"})
+
+
+def cpu_baseline(mesh, seconds=10.0, mode="ns"):
+    """The oracle (FP64, same mode) on the host cores over a bounded sample:
+    SSP-RK3 steps on a 64x64-element block of the same mesh density."""
     from zhijian_b200 import meshgen as M
     threads = os.cpu_count() or 1
-    sub = M.structured_quads(64, 64, 0.0, math.pi / 4, 0.0, math.pi / 4, 0.15, 1, (1, 1, 1, 1),
-                             {1: "slipwall"})
-    orc = O.Oracle(sub, P, GAMMA, 1.0, 1.0 / (GAMMA * MACH * MACH), MACH, 0.0, threads=threads)
+    sub = sample_block()
+    orc, step = make_oracle(sub, mode, threads)
     U = M.taylor_green(orc.sp_coords())
-    orc.step(U, DT, 1)  # warm-up
+    step(U, DT, 1)  # warm-up
     n, t0 = 0, time.perf_counter()
     while True:
-        U, _ = orc.step(U, DT, 1)
+        U, _ = step(U, DT, 1)
         n += 1
         el = time.perf_counter() - t0
         if el >= seconds or n >= 1000:
@@ -161,7 +190,7 @@ def cpu_baseline(mesh, seconds=10.0):
     dof = sub.n_elem * (P + 1) ** 2
     return {"value": dof * 3 * n / el, "unit": UNIT, "cores": threads, "kind": "port",
             "sample": f"{n} SSP-RK3 steps of a 64x64 jittered P{P} TGV block "
-                      f"({sub.n_elem} elements), {el:.1f} s"}
+                      f"({sub.n_elem} elements, {mode}), {el:.1f} s"}
 
 
 def run_reference(args):
@@ -169,18 +198,16 @@ def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return None
-    from oracle import oracle as O
     from zhijian_b200 import meshgen as M
     threads = os.cpu_count() or 1
-    sub = M.structured_quads(64, 64, 0.0, math.pi / 4, 0.0, math.pi / 4, 0.15, 1, (1, 1, 1, 1),
-                             {1: "slipwall"})
-    orc = O.Oracle(sub, P, GAMMA, 1.0, 1.0 / (GAMMA * MACH * MACH), MACH, 0.0, threads=threads)
+    sub = sample_block()
+    orc, step = make_oracle(sub, "ns", threads)
     U = M.taylor_green(orc.sp_coords())
     for _ in range(args.warmup):
-        U, _ = orc.step(U, DT, 1)
+        U, _ = step(U, DT, 1)
     t0 = time.perf_counter()
     for _ in range(args.steps):
-        U, _ = orc.step(U, DT, 1)
+        U, _ = step(U, DT, 1)
     el = time.perf_counter() - t0
     dof = sub.n_elem * (P + 1) ** 2
     v = dof * 3 * args.steps / el
@@ -189,11 +216,15 @@ def run_reference(args):
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
             "impl": "reference",
             "config": {"workload": workload_name() + " (CPU sample: 64x64 block per step)",
-                       "mode": "compat", "precision": "fp64"},
+                       "mode": "ns", "precision": "fp64"},
             "cpu_baseline": {"value": v, "unit": UNIT, "cores": threads, "kind": "port",
                              "sample": f"each step: one SSP-RK3 step of a 64x64 jittered block "
                                        f"({sub.n_elem} elements, P{P})"},
             "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+
+
+KERNELS = {"ns": "k_ns_grad<3> + k_ns_stage<3,Roe> (one residual)", "compat": "k_compat_stage<3>"}
+LAUNCHES_PER_RHS = {"ns": 2, "compat": 1}
 
 
 def run_ours(args):
@@ -223,40 +254,42 @@ def run_ours(args):
 
     from zhijian_b200 import meshgen as M
     mesh = build_case()
-    s = make_solver(mesh)
     stream = torch.cuda.Stream(dev)        # a real stream: events and kernels share it
-    s.set_stream(stream.cuda_stream)
-    U0 = M.taylor_green(s.solution_point_coords())
-    s.copyToDevice(U0)
-    dof = s.n_elem * s.n_sp
-    sampler = ClockSampler(local)   # sampled from warm-up through the timed region
+    peak, peak_kind = load_peaks()
+    sampler = ClockSampler(local)   # sampled from warm-up through the timed regions
     sampler.start()
     time.sleep(0.2)
-    s.advance(DT, args.warmup)
-    barrier_sync()
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    barrier_sync()
-    e0.record(stream)
-    s.advance(DT, args.steps, sync=False)
-    e1.record(stream)
-    barrier_sync()
-    ms = e0.elapsed_time(e1)
-    clocks = sampler.stop()
-    s.check_state()
-    ms = max_over_ranks(ms)
-    value = world * dof * 3 * args.steps / (ms * 1e-3)
-    launches = 3 * args.steps
 
-    # roofline of the dominant kernel (the fused stage kernel: every launch)
-    per_launch_s = ms * 1e-3 / launches
-    bytes_launch = algorithmic_bytes_per_element(P) * s.n_elem
-    peak, peak_kind = load_peaks()
-    achieved = bytes_launch / per_launch_s / 1e9
-    traffic = traffic_from_profile(f"k_compat_stage<3>|tgv{NX}")
-    roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                "frac": achieved / peak, "traffic": traffic, "peak_kind": peak_kind,
-                "kernel": "k_compat_stage<3>",
-                "algorithmic_bytes_per_launch": bytes_launch}
+    def timed(mode):
+        s = make_solver(mesh, mode)
+        s.set_stream(stream.cuda_stream)
+        U0 = M.taylor_green(s.solution_point_coords())
+        s.copyToDevice(U0)
+        s.advance(DT, args.warmup)
+        barrier_sync()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        barrier_sync()
+        e0.record(stream)
+        s.advance(DT, args.steps, sync=False)
+        e1.record(stream)
+        barrier_sync()
+        ms = max_over_ranks(e0.elapsed_time(e1))
+        s.check_state()
+        dof = s.n_elem * s.n_sp
+        per_rhs = ms * 1e-3 / (3 * args.steps)
+        nbytes = algorithmic_bytes_per_element(P, viscous=(mode == "ns")) * s.n_elem
+        achieved = nbytes / per_rhs / 1e9
+        roof = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                "frac": achieved / peak, "traffic": traffic_from_profile(f"{mode}|tgv{NX}"),
+                "peak_kind": peak_kind, "kernel": KERNELS[mode],
+                "algorithmic_bytes_per_launch": nbytes,
+                "launches_per_residual": LAUNCHES_PER_RHS[mode]}
+        return s, U0, dof, ms, roof
+
+    s, U0, dof, ms, roofline = timed("ns")
+    value = world * dof * 3 * args.steps / (ms * 1e-3)
+    launches = 3 * args.steps * LAUNCHES_PER_RHS["ns"]
+    clocks = sampler.stop()
 
     # end to end through the C-ABI with host buffers: per step the state goes
     # H2D from pinned memory, one SSP-RK3 step, the new state comes back D2H
@@ -278,6 +311,13 @@ def run_ours(args):
     e2e = {"value": world * dof * 3 * n_e2e / (ems * 1e-3), "unit": UNIT,
            "h2d_bytes_per_step": int(U0.nbytes), "d2h_bytes_per_step": int(U0.nbytes),
            "steps": n_e2e}
+    s.close()
+
+    sc, _, dofc, msc, roofc = timed("compat")
+    sc.close()
+    compat = {"workload": workload_name("compat"), "value": world * dofc * 3 * args.steps / (msc * 1e-3),
+              "ms_per_step": msc / args.steps, "roofline": roofc,
+              "gpu_launches": 3 * args.steps}
 
     out = None
     if rank == 0:
@@ -285,15 +325,15 @@ def run_ours(args):
                "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
                "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
                "dtype": "f64", "data": "synthetic",
-               "config": {"workload": workload_name(), "elements": s.n_elem,
-                          "dof_per_var": dof, "rhs_per_step": 3, "mode": "compat",
+               "config": {"workload": workload_name("ns"), "elements": mesh.n_elem,
+                          "dof_per_var": dof, "rhs_per_step": 3, "mode": "ns",
                           "precision": "fp64", "dt": DT,
                           "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
-                          "l2": "no flush: each stage streams ~200 MB > 126 MB L2"},
-               "roofline": roofline, "e2e": e2e, "gpu_launches": launches, "clocks": clocks}
+                          "l2": "no flush: each stage streams > 200 MB > 126 MB L2"},
+               "roofline": roofline, "e2e": e2e, "gpu_launches": launches, "clocks": clocks,
+               "compat": compat}
         if world == 1 and not args.no_cpu_baseline:
-            out["cpu_baseline"] = cpu_baseline(mesh, args.cpu_seconds)
-    s.close()
+            out["cpu_baseline"] = cpu_baseline(mesh, args.cpu_seconds, "ns")
     if world > 1:
         dist.destroy_process_group()
     return out

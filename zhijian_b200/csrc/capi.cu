@@ -124,6 +124,17 @@ cudaError_t launch_stage(const zj_solver* s, const StageArgs& a) {
     return launch_ns_stage(s->P, s->prm.riemann, a, s->stream);
 }
 
+StageArgs base_args(const zj_solver* s);
+
+// Traces of U into T in the handle's mode (physics mode adds the ghost rows).
+cudaError_t launch_trace_any(const zj_solver* s, const double* U, double* T) {
+    if (s->prm.compat) return launch_traces(s->P, U, T, s->dOps, s->E, s->stream);
+    StageArgs a = base_args(s);
+    a.U = U;
+    a.Tout = T;
+    return launch_phys_traces(s->P, a, s->stream);
+}
+
 StageArgs base_args(const zj_solver* s) {
     StageArgs a{};
     a.Jinv = s->dJinv;
@@ -205,7 +216,8 @@ zj_status zj_solver_create(const zj_mesh_desc* mesh, const zj_params* params, zj
     pack_ops(s->ops, packed);
 
     s->state_n = (size_t)s->E * s->nsp * 4;
-    s->trace_n = (size_t)s->E * 4 * s->n1 * 4;
+    // element traces, then one ghost row per boundary slot (physics mode)
+    s->trace_n = ((size_t)s->E * 4 + (size_t)s->mesh.n_bnd_faces) * s->n1 * 4;
     s->grid = stage_grid(s->P, s->E);
     s->scratch_n = 148 * 8;
     cudaError_t e = cudaSuccess;
@@ -324,7 +336,7 @@ zj_status zj_step(zj_solver* s, double dt, int nsteps) {
         s->last_dt = dt;
     }
     if (!s->traces_valid) {
-        ZJ_CK(s, launch_traces(s->P, s->dU[s->cur], s->dT[s->tpar], s->dOps, s->E, s->stream), "trace launch");
+        ZJ_CK(s, launch_trace_any(s, s->dU[s->cur], s->dT[s->tpar]), "trace launch");
         s->traces_valid = true;
     }
     for (int k = 0; k < nsteps; ++k) {
@@ -347,7 +359,7 @@ zj_status zj_rhs(zj_solver* s, const double* U_dev, double* R_dev) {
     if (!s || !U_dev || !R_dev) return ZJ_ERR_ARG;
     if ((reinterpret_cast<uintptr_t>(U_dev) | reinterpret_cast<uintptr_t>(R_dev)) & 15u)
         return fail(s, ZJ_ERR_ARG, "U_dev and R_dev must be 16-byte aligned");
-    ZJ_CK(s, launch_traces(s->P, U_dev, s->dT[2], s->dOps, s->E, s->stream), "trace launch");
+    ZJ_CK(s, launch_trace_any(s, U_dev, s->dT[2]), "trace launch");
     StageArgs a = base_args(s);
     a.U = U_dev; a.U0 = U_dev; a.Uout = nullptr; a.Tin = s->dT[2]; a.Tout = nullptr;
     a.R = R_dev; a.partials = s->dPartR; a.stage = 0;
@@ -458,7 +470,7 @@ zj_status zj_rhs_noalloc(zj_solver* s, const double* U_dev, double* R_dev) {
     double* traces = scratch;
     double* grad_traces = scratch + s->trace_n;          // Navier-Stokes only
     double* partials = scratch + (is_ns(s) ? 3 : 1) * s->trace_n;
-    ZJ_CK(s, launch_traces(s->P, U_dev, traces, s->dOps, s->E, s->stream), "trace launch");
+    ZJ_CK(s, launch_trace_any(s, U_dev, traces), "trace launch");
     StageArgs a = base_args(s);
     a.U = U_dev; a.U0 = U_dev; a.Uout = nullptr; a.Tin = traces; a.Tout = nullptr;
     a.R = R_dev; a.partials = partials; a.stage = 0;

@@ -31,7 +31,10 @@ using namespace dev;
 using namespace phys;
 
 #ifndef ZJ_NS_MIN_BLOCKS
-#define ZJ_NS_MIN_BLOCKS 2
+#define ZJ_NS_MIN_BLOCKS 2        // stage kernel
+#endif
+#ifndef ZJ_NSG_MIN_BLOCKS
+#define ZJ_NSG_MIN_BLOCKS 4       // gradient kernel
 #endif
 
 // Corrected gradient at solution point (i, j) of one element: su is the
@@ -87,15 +90,17 @@ __device__ __forceinline__ void load_face_point(const StageArgs& a, long long e,
     f.nx = n01.x; f.ny = n01.y; f.len = n23.x;
     load4_nc(a.Tin + (e * NFT + edge * N1 + fp) * 4, f.qo);
     f.qn[0] = f.qo[0]; f.qn[1] = f.qo[1]; f.qn[2] = f.qo[2]; f.qn[3] = f.qo[3];
-    if (!(f.r.flags & (kEdgeOrphan | kEdgeBoundary)))
-        load4_nc(a.Tin + (((long long)f.r.nbr * 4 + f.r.nbr_edge) * N1 + (N1 - 1 - fp)) * 4, f.qn);
-    else if (f.r.flags & kEdgeBoundary)
-        ghost_phys(f.qo, f.nx, f.ny, edge_bc_type(f.r.flags), a.bc + (long long)f.r.nbr_edge * 8,
-                   a.gamma, f.qn);
+    if (!(f.r.flags & kEdgeOrphan)) {
+        // interior: the neighbour's coinciding point; boundary: the ghost row
+        // written with the trace (phys_fp64.cu)
+        const long long row = (f.r.flags & kEdgeBoundary) ? a.n_elem * 4 + f.r.nbr_edge
+                                                          : (long long)f.r.nbr * 4 + f.r.nbr_edge;
+        load4_nc(a.Tin + (row * N1 + (N1 - 1 - fp)) * 4, f.qn);
+    }
 }
 
 template <int P>
-__global__ void __launch_bounds__(Shape<P>::THREADS, ZJ_NS_MIN_BLOCKS)
+__global__ void __launch_bounds__(Shape<P>::THREADS, ZJ_NSG_MIN_BLOCKS)
 k_ns_grad(const StageArgs a) {
     using S = Shape<P>;
     constexpr int N1 = S::N1, NSP = S::NSP, NFT = S::NFT, TPE = S::TPE, EB = S::EB;
@@ -329,6 +334,11 @@ k_ns_stage(const StageArgs a) {
         double t[4];
         trace_point<N1, RS, VS>(sU + el * FS, sOps + N1 * N1, sOps + N1 * N1 + N1, edge, fp, t);
         store4(a.Tout + (e * NFT + k) * 4, t);
+        if (f.r.flags & kEdgeBoundary) {
+            double q[4];
+            ghost_phys(t, f.nx, f.ny, edge_bc_type(f.r.flags), a.bc + (long long)f.r.nbr_edge * 8, g, q);
+            store4(a.Tout + ((a.n_elem * 4 + f.r.nbr_edge) * N1 + (N1 - 1 - fp)) * 4, q);
+        }
     }
 }
 

@@ -34,6 +34,24 @@ using namespace phys;
 
 // -------------------------------------------------------------- kernels --
 
+// Boundary ghost states live in extra rows of every trace buffer, after the
+// E*4 element edges: row E*4 + slot of boundary slot `slot`, stored at the
+// mirrored point n1-1-fp, so a boundary edge loads its ghost exactly like an
+// interior edge loads its neighbour (index (row*n1 + n1-1-fp)).  They are
+// written where the trace itself is produced, which keeps the ghost-state
+// arithmetic (pow, branches per boundary class) out of the face phases.
+__device__ __forceinline__ long long neighbour_row(const EdgeRec& r, long long n_elem) {
+    return (r.flags & kEdgeBoundary) ? n_elem * 4 + r.nbr_edge : (long long)r.nbr * 4 + r.nbr_edge;
+}
+
+template <int N1>
+__device__ __forceinline__ void store_ghost(const StageArgs& a, const EdgeRec& r, double nx, double ny,
+                                            int fp, const double* t) {
+    double q[4];
+    ghost_phys(t, nx, ny, edge_bc_type(r.flags), a.bc + (long long)r.nbr_edge * 8, a.gamma, q);
+    store4(a.Tout + ((a.n_elem * 4 + r.nbr_edge) * N1 + (N1 - 1 - fp)) * 4, q);
+}
+
 template <int P, int RIEM>
 __global__ void __launch_bounds__(Shape<P>::THREADS, ZJ_PHYS_MIN_BLOCKS)
 k_phys_stage(const StageArgs a) {
@@ -92,8 +110,8 @@ k_phys_stage(const StageArgs a) {
     }
     // The neighbour's point that coincides with this one: both elements run
     // their shared edge counter-clockwise.
-    if (is_fp && !(r.flags & (kEdgeOrphan | kEdgeBoundary)))
-        load4_nc(a.Tin + (((long long)r.nbr * 4 + r.nbr_edge) * N1 + (N1 - 1 - fp)) * 4, qn);
+    if (is_fp && !(r.flags & kEdgeOrphan))
+        load4_nc(a.Tin + (neighbour_row(r, a.n_elem) * N1 + (N1 - 1 - fp)) * 4, qn);
     __syncthreads();   // sOps, sF, sG ready
 
     // ---- B: interface terms.  The common flux is evaluated from the left
@@ -102,8 +120,6 @@ k_phys_stage(const StageArgs a) {
         double Fd[4] = {0.0, 0.0, 0.0, 0.0};
         if (!(r.flags & kEdgeOrphan)) {
             const double nx = nr.x, ny = nr.y, s = 0.5 * nr.z;
-            if (r.flags & kEdgeBoundary)
-                ghost_phys(qo, nx, ny, edge_bc_type(r.flags), a.bc + (long long)r.nbr_edge * 8, g, qn);
             const bool right = (r.flags & kEdgeRight) != 0;
             double UL[4], UR[4], Fc[4];
 #pragma unroll
@@ -194,6 +210,43 @@ k_phys_stage(const StageArgs a) {
         double t[4];
         trace_point<N1, RS, VS>(sU + el * FS, sOps + N1 * N1, sOps + N1 * N1 + N1, edge, fp, t);
         store4(a.Tout + (e * NFT + k) * 4, t);
+        if (r.flags & kEdgeBoundary) store_ghost<N1>(a, r, nr.x, nr.y, fp, t);
+    }
+}
+
+// Traces (and boundary ghost rows) of a state that did not come out of a
+// stage launch.  a.U: state, a.Tout: trace buffer.
+template <int P>
+__global__ void __launch_bounds__(Shape<P>::THREADS)
+k_phys_traces(const StageArgs a) {
+    using S = Shape<P>;
+    constexpr int N1 = S::N1, NSP = S::NSP, NFT = S::NFT, TPE = S::TPE, EB = S::EB;
+    constexpr int RS = S::RS, VS = S::VS, FS = S::FS;
+    __shared__ double sOps[S::NOPS];
+    __shared__ double sU[EB * FS];
+    const int tid = threadIdx.x;
+    for (int t = tid; t < S::NOPS; t += blockDim.x) sOps[t] = a.ops[t];
+    const int el = tid / TPE, k = tid - el * TPE;
+    const long long e = (long long)blockIdx.x * EB + el;
+    const bool valid = (el < EB) && (e < a.n_elem);
+    if (valid && k < NSP) {
+        double u[4];
+        load4_nc(a.U + (e * NSP + k) * 4, u);
+        double* su = sU + el * FS + (k / N1) * RS + (k % N1);
+#pragma unroll
+        for (int v = 0; v < 4; ++v) su[v * VS] = u[v];
+    }
+    __syncthreads();
+    if (valid && k < NFT) {
+        const int edge = k / N1, fp = k - edge * N1;
+        double t[4];
+        trace_point<N1, RS, VS>(sU + el * FS, sOps + N1 * N1, sOps + N1 * N1 + N1, edge, fp, t);
+        store4(a.Tout + (e * NFT + k) * 4, t);
+        const EdgeRec r = a.edges[e * 4 + edge];
+        if (r.flags & kEdgeBoundary) {
+            const double2 n01 = __ldg(reinterpret_cast<const double2*>(a.enrm + e * 4 + edge));
+            store_ghost<N1>(a, r, n01.x, n01.y, fp, t);
+        }
     }
 }
 
@@ -222,7 +275,27 @@ cudaError_t launch_p(int riemann, const StageArgs& a, cudaStream_t s) {
     }
 }
 
+template <int P>
+cudaError_t traces_t(const StageArgs& a, cudaStream_t s) {
+    using S = Shape<P>;
+    const long long grid = (a.n_elem + S::EB - 1) / S::EB;
+    if (grid <= 0) return cudaSuccess;
+    k_phys_traces<P><<<(unsigned)grid, S::THREADS, 0, s>>>(a);
+    return cudaGetLastError();
+}
+
 }  // namespace
+
+cudaError_t launch_phys_traces(int P, const StageArgs& a, cudaStream_t s) {
+    switch (P) {
+        case 1: return traces_t<1>(a, s);
+        case 2: return traces_t<2>(a, s);
+        case 3: return traces_t<3>(a, s);
+        case 4: return traces_t<4>(a, s);
+        case 5: return traces_t<5>(a, s);
+        default: return cudaErrorInvalidValue;
+    }
+}
 
 cudaError_t launch_phys_stage(int P, int riemann, const StageArgs& a, cudaStream_t s) {
     switch (P) {

@@ -12,7 +12,8 @@ struct StageArgs {
     const double* U;        // stage input state, AoS [E][n_sp][4]
     const double* U0;       // RK base state (stages 2, 3)
     double* Uout;           // stage output state
-    const double* Tin;      // traces of U, [E][4 edges][n1][4]
+    const double* Tin;      // traces of U, [E][4 edges][n1][4], then the physics-mode
+                            // boundary ghost rows [n_bnd][n1][4] (stored mirrored)
     double* Tout;           // traces of Uout
     double* R;              // residual output (stage 0 only)
     const double* Jinv;     // [E][n_sp][4] = (xi_x, xi_y, eta_x, eta_y)
@@ -40,6 +41,8 @@ void pack_ops(const Operators1D& o, std::vector<double>& out);
 cudaError_t launch_compat_stage(int P, const StageArgs& a, cudaStream_t s, int* grid_out);
 // Physics-mode FP64 launches (conservative FR, VCJH, selected Riemann solver).
 cudaError_t launch_phys_stage(int P, int riemann, const StageArgs& a, cudaStream_t s);
+// Physics-mode traces of a.U into a.Tout, boundary ghost rows included.
+cudaError_t launch_phys_traces(int P, const StageArgs& a, cudaStream_t s);
 // Navier-Stokes: gradient traces of a stage state, then the stage itself.
 cudaError_t launch_ns_grad(int P, const StageArgs& a, cudaStream_t s);
 cudaError_t launch_ns_stage(int P, int riemann, const StageArgs& a, cudaStream_t s);
