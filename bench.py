@@ -44,6 +44,8 @@ DT = 2.0e-4
 
 MODES = {
     "ns": dict(compat=False, viscous=True, riemann="Roe", flux_type="HU", Re=5000.0, Pr=0.72),
+    "ns32": dict(compat=False, viscous=True, riemann="Roe", flux_type="HU", Re=5000.0, Pr=0.72,
+                 precision="mixed"),
     "compat": dict(compat=True, viscous=False, riemann="Rusanov", flux_type="HU"),
 }
 
@@ -75,6 +77,13 @@ def algorithmic_bytes_per_element(p, w_s=8, w_g=8, w_t=8, viscous=False):
     if viscous:
         b += w_t * 64 * nf
     return b
+
+
+def mode_bytes_per_element(mode, p=P):
+    """Algorithmic bytes per element and residual of a bench mode: FP64
+    everywhere, or (mixed) FP64 state with FP32 metrics and traces."""
+    w = 4 if MODES[mode].get("precision") == "mixed" else 8
+    return algorithmic_bytes_per_element(p, 8, w, w, viscous=MODES[mode].get("viscous", False))
 
 
 def traffic_from_profile(kernel_key):
@@ -223,8 +232,10 @@ def run_reference(args):
             "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
 
 
-KERNELS = {"ns": "k_ns_grad<3> + k_ns_stage<3,Roe> (one residual)", "compat": "k_compat_stage<3>"}
-LAUNCHES_PER_RHS = {"ns": 2, "compat": 1}
+KERNELS = {"ns": "k_ns_grad<3> + k_ns_stage<3,Roe> (one residual)",
+           "ns32": "k_ns_grad<3,float> + k_ns_stage<3,Roe,float> (one residual)",
+           "compat": "k_compat_stage<3>"}
+LAUNCHES_PER_RHS = {"ns": 2, "ns32": 2, "compat": 1}
 
 
 def run_ours(args):
@@ -277,7 +288,7 @@ def run_ours(args):
         s.check_state()
         dof = s.n_elem * s.n_sp
         per_rhs = ms * 1e-3 / (3 * args.steps)
-        nbytes = algorithmic_bytes_per_element(P, viscous=(mode == "ns")) * s.n_elem
+        nbytes = mode_bytes_per_element(mode) * s.n_elem
         achieved = nbytes / per_rhs / 1e9
         roof = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                 "frac": achieved / peak, "traffic": traffic_from_profile(f"{mode}|tgv{NX}"),

@@ -163,3 +163,13 @@ def test_no_device_reports_cuda_error(zjlib):
     with pytest.raises(L.ZJError) as e:
         _create(M.vortex_mesh(2), make_params())
     assert e.value.code == L.ERR_CUDA
+
+
+def test_mixed_precision_needs_physics_mode(zjlib):
+    """precision = mixed is the physics-mode form; compat mode (the
+    reference's FP64 residual) refuses it before touching a device."""
+    from zhijian_b200 import meshgen as M
+    from zhijian_b200.solver import FRSolver, make_params
+    with pytest.raises(L.ZJError) as e:
+        FRSolver(M.vortex_mesh(4), make_params(compat=True, precision="mixed"))
+    assert e.value.code == L.ERR_UNSUPPORTED

@@ -16,7 +16,9 @@ CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libzj_fr.so")
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 
-SOURCES = ["host_setup.cpp", "compat_fp64.cu", "phys_fp64.cu", "ns_fp64.cu", "capi.cu"]
+SOURCES = ["host_setup.cpp", "compat_fp64.cu", "phys_fp64.cu", "phys_fp32.cu", "ns_fp64.cu",
+           "ns_fp32.cu", "capi.cu"]
+OBJDIR = os.path.join(HERE, "_build")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 
@@ -30,23 +32,38 @@ def _stale() -> bool:
 
 
 def build(force: bool = False, verbose: bool = False, ptxas_v: bool = False) -> str:
-    """Compile the library if any source is newer than it; returns its path."""
+    """Compile the library if any source is newer than it; returns its path.
+    Each translation unit compiles in its own nvcc process (in parallel),
+    then one nvcc links the shared library."""
     if not force and not _stale():
         return LIB
-    cmd = [NVCC, "-shared", "-O3", "-std=c++17", "-lineinfo", *ARCH,
-           "-Xcompiler", "-fPIC,-O2,-ffp-contract=off",
-           "-I", os.path.join(ROOT, "include"), "-I", CSRC,
-           "-o", LIB + ".tmp"]
+    os.makedirs(OBJDIR, exist_ok=True)
+    flags = ["-O3", "-std=c++17", "-lineinfo", *ARCH, "-Xcompiler", "-fPIC,-O2,-ffp-contract=off",
+             "-I", os.path.join(ROOT, "include"), "-I", CSRC]
     if ptxas_v:
-        cmd += ["-Xptxas", "-v"]
-    cmd += [os.path.join(CSRC, s) for s in SOURCES]
-    if verbose:
-        print(" ".join(cmd), flush=True)
+        flags += ["-Xptxas", "-v"]
+    procs, objs = [], []
+    for src in SOURCES:
+        obj = os.path.join(OBJDIR, os.path.splitext(src)[0] + ".o")
+        cmd = [NVCC, "-c", *flags, "-o", obj, os.path.join(CSRC, src)]
+        if verbose:
+            print(" ".join(cmd), flush=True)
+        procs.append((src, subprocess.Popen(cmd, stdout=subprocess.PIPE, stderr=subprocess.STDOUT,
+                                            text=True)))
+        objs.append(obj)
+    errors = []
+    for src, pr in procs:
+        out, _ = pr.communicate()
+        if pr.returncode != 0:
+            errors.append(f"{src}:\n{out}")
+        elif verbose or ptxas_v:
+            sys.stdout.write(out)
+    if errors:
+        raise RuntimeError("nvcc failed:\n" + "\n".join(errors))
+    cmd = [NVCC, "-shared", *ARCH, "-o", LIB + ".tmp", *objs]
     r = subprocess.run(cmd, capture_output=True, text=True)
     if r.returncode != 0:
-        raise RuntimeError("nvcc failed:\n" + r.stdout + r.stderr)
-    if verbose or ptxas_v:
-        sys.stdout.write(r.stdout + r.stderr)
+        raise RuntimeError("nvcc link failed:\n" + r.stdout + r.stderr)
     os.replace(LIB + ".tmp", LIB)
     build_driver()
     return LIB

@@ -3,10 +3,13 @@
 // A zj_solver owns every device buffer, allocated once in zj_solver_create:
 //   state   3 x [E][n_sp][4] f64   rotating stage buffers (no stage writes a
 //                                  buffer it reads, so no aliasing)
-//   traces  3 x [E][4][n1][4] f64  ping-pong pair for the stepper + one for
-//                                  zj_rhs
+//   traces  3 x [E][4][n1][4]      ping-pong pair for the stepper + one for
+//                                  zj_rhs (+ boundary ghost rows)
 //   metrics [E][n_sp][4] Jinv, [E][n_sp] J, per-element edge records, bc
 //   scratch state + residual for the host-buffer entry points, reductions
+// Traces, gradient traces, metrics, normals, operators and bc data exist in
+// the arithmetic type of the handle: FP64, or FP32 for the mixed-precision
+// form (whose state and reductions stay FP64).
 // An SSP-RK3 step is three fused stage launches; the first step after a state
 // upload is preceded by one trace launch.
 #include <cuda_runtime.h>
@@ -48,6 +51,15 @@ struct zj_solver {
     int* dFlag = nullptr;
     EdgeRec* dEdges = nullptr;
     double4* dNrm = nullptr;
+    // mixed-precision form: FP32 traces, gradient traces and geometry
+    bool mixed = false;
+    float* fT[3] = {nullptr, nullptr, nullptr};
+    float* fTQ = nullptr;
+    float* fJinv = nullptr;
+    float* fJ = nullptr;
+    float* fOps = nullptr;
+    float* fBC = nullptr;
+    float4* fNrm = nullptr;
     int grid = 0;
     int cur = 0, tpar = 0;
     bool traces_valid = false;
@@ -92,6 +104,11 @@ void free_all(zj_solver* s) {
     double** ds[] = {&s->dUs, &s->dRs, &s->dJinv, &s->dJ, &s->dOps, &s->dBC, &s->dH,
                      &s->dScal, &s->dPart, &s->dPartR, &s->dScratch};
     for (auto pp : ds) { if (*pp) cudaFree(*pp); *pp = nullptr; }
+    for (auto& p : s->fT) { if (p) cudaFree(p); p = nullptr; }
+    float** fs[] = {&s->fTQ, &s->fJinv, &s->fJ, &s->fOps, &s->fBC};
+    for (auto pp : fs) { if (*pp) cudaFree(*pp); *pp = nullptr; }
+    if (s->fNrm) cudaFree(s->fNrm);
+    s->fNrm = nullptr;
     if (s->dFlag) cudaFree(s->dFlag);
     if (s->dEdges) cudaFree(s->dEdges);
     if (s->dNrm) cudaFree(s->dNrm);
@@ -108,70 +125,126 @@ zj_status validate_params(const zj_params* p, std::string& msg) {
     if (p->riemann < 0 || p->riemann > 2) { msg = "riemann must be Rusanov, Roe or HLLC"; return ZJ_ERR_ARG; }
     if (p->n_bc < 0 || p->n_bc > ZJ_MAX_BC) { msg = "n_bc out of range"; return ZJ_ERR_ARG; }
     if (!p->compat && p->viscous && !(p->Re > 0.0 && p->Pr > 0.0)) { msg = "Re and Pr must be > 0"; return ZJ_ERR_ARG; }
-    if (p->precision != ZJ_FP64) { msg = "the mixed-precision form is not built yet"; return ZJ_ERR_UNSUPPORTED; }
+    if (p->precision != ZJ_FP64 && p->precision != ZJ_MIXED) { msg = "precision must be fp64 or mixed"; return ZJ_ERR_ARG; }
+    if (p->precision == ZJ_MIXED && p->compat) {
+        msg = "the mixed-precision form needs physics mode (compat off): compat mode is the reference's FP64 residual";
+        return ZJ_ERR_UNSUPPORTED;
+    }
     return ZJ_OK;
 }
 
 bool is_ns(const zj_solver* s) { return !s->prm.compat && s->prm.viscous; }
 
+// Buffers of the handle's arithmetic type.
+template <typename T> T* tbuf(const zj_solver* s, int i);
+template <> double* tbuf<double>(const zj_solver* s, int i) { return s->dT[i]; }
+template <> float* tbuf<float>(const zj_solver* s, int i) { return s->fT[i]; }
+
+template <typename T> StageArgsT<T> base_args(const zj_solver* s);
+template <> StageArgsT<double> base_args<double>(const zj_solver* s) {
+    StageArgsT<double> a{};
+    a.Jinv = s->dJinv; a.J = s->dJ; a.enrm = s->dNrm; a.bc = s->dBC; a.ops = s->dOps;
+    a.TQ = s->dTQ; a.TQout = s->dTQ;
+    return a;
+}
+template <> StageArgsT<float> base_args<float>(const zj_solver* s) {
+    StageArgsT<float> a{};
+    a.Jinv = s->fJinv; a.J = s->fJ; a.enrm = s->fNrm; a.bc = s->fBC; a.ops = s->fOps;
+    a.TQ = s->fTQ; a.TQout = s->fTQ;
+    return a;
+}
+
+template <typename T>
+StageArgsT<T> stage_args(const zj_solver* s) {
+    StageArgsT<T> a = base_args<T>(s);
+    a.edges = s->dEdges;
+    a.dt = s->dScal;
+    a.n_elem = s->E;
+    a.gamma = s->prm.gamma;
+    a.Re = s->prm.Re;
+    a.Pr = s->prm.Pr;
+    return a;
+}
+
 // One residual or RK-stage evaluation in the handle's mode: one launch, or
 // the gradient launch then the stage launch for Navier-Stokes.
-cudaError_t launch_stage(const zj_solver* s, const StageArgs& a) {
-    if (s->prm.compat) return launch_compat_stage(s->P, a, s->stream, nullptr);
+template <typename T>
+cudaError_t launch_stage(const zj_solver* s, const StageArgsT<T>& a) {
+    if constexpr (sizeof(T) == 8) {
+        if (s->prm.compat) return launch_compat_stage(s->P, a, s->stream, nullptr);
+    }
     if (!is_ns(s)) return launch_phys_stage(s->P, s->prm.riemann, a, s->stream);
     cudaError_t e = launch_ns_grad(s->P, a, s->stream);
     if (e != cudaSuccess) return e;
     return launch_ns_stage(s->P, s->prm.riemann, a, s->stream);
 }
 
-StageArgs base_args(const zj_solver* s);
-
-// Traces of U into T in the handle's mode (physics mode adds the ghost rows).
-cudaError_t launch_trace_any(const zj_solver* s, const double* U, double* T) {
-    if (s->prm.compat) return launch_traces(s->P, U, T, s->dOps, s->E, s->stream);
-    StageArgs a = base_args(s);
+// Traces of U into Tb in the handle's mode (physics mode adds the ghost rows).
+template <typename T>
+cudaError_t launch_trace_any(const zj_solver* s, const double* U, T* Tb) {
+    if constexpr (sizeof(T) == 8) {
+        if (s->prm.compat) return launch_traces(s->P, U, Tb, s->dOps, s->E, s->stream);
+    }
+    StageArgsT<T> a = stage_args<T>(s);
     a.U = U;
-    a.Tout = T;
+    a.Tout = Tb;
     return launch_phys_traces(s->P, a, s->stream);
 }
 
-StageArgs base_args(const zj_solver* s) {
-    StageArgs a{};
-    a.Jinv = s->dJinv;
-    a.J = s->dJ;
-    a.edges = s->dEdges;
-    a.enrm = s->dNrm;
-    a.bc = s->dBC;
-    a.ops = s->dOps;
-    a.dt = s->dScal;
-    a.n_elem = s->E;
-    a.gamma = s->prm.gamma;
-    a.TQ = s->dTQ;
-    a.TQout = s->dTQ;
-    a.Re = s->prm.Re;
-    a.Pr = s->prm.Pr;
-    return a;
-}
-
+template <typename T>
 zj_status enqueue_step(zj_solver* s) {
     const int c = s->cur, a1 = (c + 1) % 3, b1 = (c + 2) % 3, p = s->tpar;
-    StageArgs a = base_args(s);
+    StageArgsT<T> a = stage_args<T>(s);
     a.partials = s->dPart;
     // stage 1: U(1) = U0 + dt R(U0)
-    a.U = s->dU[c]; a.U0 = s->dU[c]; a.Uout = s->dU[a1]; a.Tin = s->dT[p]; a.Tout = s->dT[1 - p];
+    a.U = s->dU[c]; a.U0 = s->dU[c]; a.Uout = s->dU[a1]; a.Tin = tbuf<T>(s, p); a.Tout = tbuf<T>(s, 1 - p);
     a.stage = 1;
     ZJ_CK(s, launch_stage(s, a), "stage 1 launch");
     // stage 2: U(2) = 3/4 U0 + 1/4 U(1) + 1/4 dt R(U(1))
-    a.U = s->dU[a1]; a.Uout = s->dU[b1]; a.Tin = s->dT[1 - p]; a.Tout = s->dT[p];
+    a.U = s->dU[a1]; a.Uout = s->dU[b1]; a.Tin = tbuf<T>(s, 1 - p); a.Tout = tbuf<T>(s, p);
     a.stage = 2;
     ZJ_CK(s, launch_stage(s, a), "stage 2 launch");
     // stage 3: U = 1/3 U0 + 2/3 U(2) + 2/3 dt R(U(2))
-    a.U = s->dU[b1]; a.Uout = s->dU[a1]; a.Tin = s->dT[p]; a.Tout = s->dT[1 - p];
+    a.U = s->dU[b1]; a.Uout = s->dU[a1]; a.Tin = tbuf<T>(s, p); a.Tout = tbuf<T>(s, 1 - p);
     a.stage = 3;
     ZJ_CK(s, launch_stage(s, a), "stage 3 launch");
     s->cur = a1;
     s->tpar = 1 - p;
     return ZJ_OK;
+}
+
+template <typename T>
+zj_status step_impl(zj_solver* s, int nsteps, double dt) {
+    if (!s->traces_valid) {
+        ZJ_CK(s, launch_trace_any(s, s->dU[s->cur], tbuf<T>(s, s->tpar)), "trace launch");
+        s->traces_valid = true;
+    }
+    for (int k = 0; k < nsteps; ++k) {
+        zj_status st = enqueue_step<T>(s);
+        if (st != ZJ_OK) return st;
+        s->time += dt;
+        s->iter += 1;
+    }
+    return ZJ_OK;
+}
+
+// Residual of U_dev into R_dev with the given trace / gradient-trace /
+// partial-sum scratch.
+template <typename T>
+zj_status rhs_impl(zj_solver* s, const double* U_dev, double* R_dev, T* traces, T* grad_traces,
+                   double* partials) {
+    ZJ_CK(s, launch_trace_any(s, U_dev, traces), "trace launch");
+    StageArgsT<T> a = stage_args<T>(s);
+    a.U = U_dev; a.U0 = U_dev; a.Uout = nullptr; a.Tin = traces; a.Tout = nullptr;
+    a.R = R_dev; a.partials = partials; a.stage = 0;
+    if (grad_traces) { a.TQ = grad_traces; a.TQout = grad_traces; }
+    ZJ_CK(s, launch_stage(s, a), "residual launch");
+    return ZJ_OK;
+}
+
+template <typename T>
+std::vector<T> narrow(const std::vector<double>& v) {
+    return std::vector<T>(v.begin(), v.end());
 }
 
 }  // namespace
@@ -224,8 +297,19 @@ zj_status zj_solver_create(const zj_mesh_desc* mesh, const zj_params* params, zj
 #define ZJ_ALLOC(ptr, n)                                                     \
     if (e == cudaSuccess) e = dalloc(&(ptr), (n));
     for (int i = 0; i < 3; ++i) { ZJ_ALLOC(s->dU[i], s->state_n); }
-    for (int i = 0; i < 3; ++i) { ZJ_ALLOC(s->dT[i], s->trace_n); }
-    if (is_ns(s)) { ZJ_ALLOC(s->dTQ, 2 * s->trace_n); }
+    s->mixed = params->precision == ZJ_MIXED;
+    if (!s->mixed) {
+        for (int i = 0; i < 3; ++i) { ZJ_ALLOC(s->dT[i], s->trace_n); }
+        if (is_ns(s)) { ZJ_ALLOC(s->dTQ, 2 * s->trace_n); }
+    } else {
+        for (int i = 0; i < 3; ++i) { ZJ_ALLOC(s->fT[i], s->trace_n); }
+        if (is_ns(s)) { ZJ_ALLOC(s->fTQ, 2 * s->trace_n); }
+        ZJ_ALLOC(s->fJinv, Jinv.size());
+        ZJ_ALLOC(s->fJ, J.size());
+        ZJ_ALLOC(s->fOps, packed.size());
+        ZJ_ALLOC(s->fBC, bc.size());
+        ZJ_ALLOC(s->fNrm, rec.size());
+    }
     ZJ_ALLOC(s->dUs, s->state_n);
     ZJ_ALLOC(s->dRs, s->state_n);
     ZJ_ALLOC(s->dJinv, Jinv.size());
@@ -249,6 +333,18 @@ zj_status zj_solver_create(const zj_mesh_desc* mesh, const zj_params* params, zj
     if (e == cudaSuccess) e = cudaMemcpy(s->dH, area.data(), area.size() * 8, cudaMemcpyHostToDevice);
     if (e == cudaSuccess) e = cudaMemcpy(s->dEdges, rec.data(), rec.size() * sizeof(EdgeRec), cudaMemcpyHostToDevice);
     if (e == cudaSuccess) e = cudaMemcpy(s->dNrm, nrm.data(), nrm.size() * 8, cudaMemcpyHostToDevice);
+    if (s->mixed) {
+        // The geometry is computed once in FP64 on the host and rounded to
+        // FP32 for the mixed-precision kernels.
+        const std::vector<float> fJinv = narrow<float>(Jinv), fJ = narrow<float>(J),
+                                 fOps = narrow<float>(packed), fBC = narrow<float>(bc),
+                                 fNrm = narrow<float>(nrm);
+        if (e == cudaSuccess) e = cudaMemcpy(s->fJinv, fJinv.data(), fJinv.size() * 4, cudaMemcpyHostToDevice);
+        if (e == cudaSuccess) e = cudaMemcpy(s->fJ, fJ.data(), fJ.size() * 4, cudaMemcpyHostToDevice);
+        if (e == cudaSuccess) e = cudaMemcpy(s->fOps, fOps.data(), fOps.size() * 4, cudaMemcpyHostToDevice);
+        if (e == cudaSuccess) e = cudaMemcpy(s->fBC, fBC.data(), fBC.size() * 4, cudaMemcpyHostToDevice);
+        if (e == cudaSuccess) e = cudaMemcpy(s->fNrm, fNrm.data(), fNrm.size() * 4, cudaMemcpyHostToDevice);
+    }
     if (e == cudaSuccess) e = cudaMemset(s->dU[0], 0, s->state_n * 8);
     if (e == cudaSuccess) e = cudaMemset(s->dScal, 0, 8 * 8);
     if (e == cudaSuccess) e = cudaDeviceSynchronize();
@@ -335,16 +431,8 @@ zj_status zj_step(zj_solver* s, double dt, int nsteps) {
         ZJ_CK(s, cudaMemcpyAsync(s->dScal, &dt, sizeof(double), cudaMemcpyHostToDevice, s->stream), "dt upload");
         s->last_dt = dt;
     }
-    if (!s->traces_valid) {
-        ZJ_CK(s, launch_trace_any(s, s->dU[s->cur], s->dT[s->tpar]), "trace launch");
-        s->traces_valid = true;
-    }
-    for (int k = 0; k < nsteps; ++k) {
-        zj_status st = enqueue_step(s);
-        if (st != ZJ_OK) return st;
-        s->time += dt;
-        s->iter += 1;
-    }
+    zj_status st = s->mixed ? step_impl<float>(s, nsteps, dt) : step_impl<double>(s, nsteps, dt);
+    if (st != ZJ_OK) return st;
     s->has_norm = true;
     return ZJ_OK;
 }
@@ -359,12 +447,8 @@ zj_status zj_rhs(zj_solver* s, const double* U_dev, double* R_dev) {
     if (!s || !U_dev || !R_dev) return ZJ_ERR_ARG;
     if ((reinterpret_cast<uintptr_t>(U_dev) | reinterpret_cast<uintptr_t>(R_dev)) & 15u)
         return fail(s, ZJ_ERR_ARG, "U_dev and R_dev must be 16-byte aligned");
-    ZJ_CK(s, launch_trace_any(s, U_dev, s->dT[2]), "trace launch");
-    StageArgs a = base_args(s);
-    a.U = U_dev; a.U0 = U_dev; a.Uout = nullptr; a.Tin = s->dT[2]; a.Tout = nullptr;
-    a.R = R_dev; a.partials = s->dPartR; a.stage = 0;
-    ZJ_CK(s, launch_stage(s, a), "residual launch");
-    return ZJ_OK;
+    if (s->mixed) return rhs_impl<float>(s, U_dev, R_dev, s->fT[2], nullptr, s->dPartR);
+    return rhs_impl<double>(s, U_dev, R_dev, s->dT[2], nullptr, s->dPartR);
 }
 
 zj_status zj_rhs_host(zj_solver* s, const double* U, double* R) {
@@ -456,7 +540,8 @@ zj_status zj_rhs_noalloc(zj_solver* s, const double* U_dev, double* R_dev) {
     if (!s || !U_dev || !R_dev) return ZJ_ERR_ARG;
     if ((reinterpret_cast<uintptr_t>(U_dev) | reinterpret_cast<uintptr_t>(R_dev)) & 15u)
         return fail(s, ZJ_ERR_ARG, "U_dev and R_dev must be 16-byte aligned");
-    const size_t trace_bytes = (is_ns(s) ? 3 : 1) * s->trace_n * sizeof(double);
+    const size_t tsz = s->mixed ? sizeof(float) : sizeof(double);
+    const size_t trace_bytes = (is_ns(s) ? 3 : 1) * s->trace_n * tsz;
     const size_t part_bytes = (size_t)s->grid * sizeof(double);
     if (trace_bytes + part_bytes > ZJ_NOALLOC_SCRATCH_BYTES)
         return fail(s, ZJ_ERR_ARG,
@@ -466,17 +551,16 @@ zj_status zj_rhs_noalloc(zj_solver* s, const double* U_dev, double* R_dev) {
     double* scratch = nullptr;
     ZJ_CK(s, noalloc_scratch(&scratch), "static scratch address");
     // Every scratch value is written before it is read (all traces by the
-    // trace launch, one partial per CTA), so nothing needs clearing.
+    // trace launch, one partial per CTA), so nothing needs clearing.  The
+    // trace block is a multiple of 16 bytes, so the partials stay aligned.
+    char* base = reinterpret_cast<char*>(scratch);
+    double* partials = reinterpret_cast<double*>(base + trace_bytes);
+    if (s->mixed) {
+        float* traces = reinterpret_cast<float*>(base);
+        return rhs_impl<float>(s, U_dev, R_dev, traces, is_ns(s) ? traces + s->trace_n : nullptr, partials);
+    }
     double* traces = scratch;
-    double* grad_traces = scratch + s->trace_n;          // Navier-Stokes only
-    double* partials = scratch + (is_ns(s) ? 3 : 1) * s->trace_n;
-    ZJ_CK(s, launch_trace_any(s, U_dev, traces), "trace launch");
-    StageArgs a = base_args(s);
-    a.U = U_dev; a.U0 = U_dev; a.Uout = nullptr; a.Tin = traces; a.Tout = nullptr;
-    a.R = R_dev; a.partials = partials; a.stage = 0;
-    if (is_ns(s)) { a.TQ = grad_traces; a.TQout = grad_traces; }
-    ZJ_CK(s, launch_stage(s, a), "residual launch");
-    return ZJ_OK;
+    return rhs_impl<double>(s, U_dev, R_dev, traces, is_ns(s) ? traces + s->trace_n : nullptr, partials);
 }
 
 zj_status zj_solver_create_from_gmsh(const char* msh_path, const zj_params* params, zj_solver** out) {

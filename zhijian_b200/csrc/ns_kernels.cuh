@@ -1,0 +1,461 @@
+// ns_kernels.cuh -- Navier-Stokes residual and SSP-RK3 stages (physics mode,
+// viscous on), templated on the arithmetic type T: double in ns_fp64.cu (the
+// reference-parity path), float in ns_fp32.cu (the mixed-precision form; the
+// state, the RK accumulation and the norm partials stay FP64).  Two launches
+// per residual:
+//
+//  k_ns_grad   corrected gradient Q = grad U at the solution points and its
+//              traces at the flux points (written for the neighbours);
+//  k_ns_stage  recomputes Q at the solution points, total flux F - F_v, the
+//              common flux = Riemann(U_L, U_R) - F_v(avg U, avg Q).n, FR
+//              correction, stage update and traces of the new state.
+//
+// Gradient: U^C = U^D + (U_c - U^D) g at the edges with the common solution
+// U_c = (U_L + U_R)/2 (the ghost state on boundaries), the same VCJH
+// correction functions as the flux, chain rule with the pointwise metrics:
+//   dU/dxi  = D_xi U  + g_R'(xi) dU_1 + g_L'(xi) dU_3
+//   dU/deta = D_eta U + g_L'(eta) dU_0 + g_R'(eta) dU_2,   dU_e = U_c - U_own
+//   Q_x = xi_x dU/dxi + eta_x dU/deta,  Q_y = xi_y dU/dxi + eta_y dU/deta.
+// Viscous flux: the reference's computeViscousFluxSPKernel law
+// (kernels.cu:742-786); common viscous flux: average state and average
+// gradients (BR2Scheme::commonFlux, navierstokes.hpp:177-204); boundaries
+// copy the interior gradient (BoundaryCondition::ghostGradient).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "zj_device.cuh"
+#include "zj_kernels.h"
+#include "zj_math.h"
+#include "zj_physics.cuh"
+#include "phys_kernels.cuh"
+
+#ifndef ZJ_NS_MIN_BLOCKS
+#define ZJ_NS_MIN_BLOCKS 2        // FP64 stage kernel
+#endif
+#ifndef ZJ_NSG_MIN_BLOCKS
+#define ZJ_NSG_MIN_BLOCKS 4       // FP64 gradient kernel
+#endif
+#ifndef ZJ_NS32_MIN_BLOCKS
+#define ZJ_NS32_MIN_BLOCKS 4      // mixed-precision stage kernel (64 registers)
+#endif
+#ifndef ZJ_NSG32_MIN_BLOCKS
+#define ZJ_NSG32_MIN_BLOCKS 6     // mixed-precision gradient kernel (40 registers)
+#endif
+
+namespace zj {
+namespace {
+
+using namespace dev;
+using namespace phys;
+
+template <typename T> struct NSMinBlocks;
+template <> struct NSMinBlocks<double> {
+    static constexpr int stage = ZJ_NS_MIN_BLOCKS, grad = ZJ_NSG_MIN_BLOCKS;
+};
+template <> struct NSMinBlocks<float> {
+    static constexpr int stage = ZJ_NS32_MIN_BLOCKS, grad = ZJ_NSG32_MIN_BLOCKS;
+};
+
+// Corrected gradient at solution point (i, j) of one element: su is the
+// element's state in the [var][row][col] shared layout, du its face jumps
+// U_c - U_own in the [flux point][var] layout.
+template <int N1, int RS, int VS, typename T>
+__device__ __forceinline__ void corrected_gradient(const T* su, const T* du, const T* ops, int i,
+                                                   int j, const T* ji, T* Qx, T* Qy) {
+    const T* gL = ops + N1 * N1 + 2 * N1;
+    const T* gR = gL + N1;
+    T Di[N1], Dj[N1];
+#pragma unroll
+    for (int m = 0; m < N1; ++m) { Di[m] = ops[i * N1 + m]; Dj[m] = ops[j * N1 + m]; }
+    T d1[4], d3[4], d0[4], d2[4];
+    load4(du + (1 * N1 + j) * 4, d1);
+    load4(du + (3 * N1 + (N1 - 1 - j)) * 4, d3);
+    load4(du + (0 * N1 + i) * 4, d0);
+    load4(du + (2 * N1 + (N1 - 1 - i)) * 4, d2);
+    const T gRi = gR[i], gLi = gL[i], gRj = gR[j], gLj = gL[j];
+#pragma unroll
+    for (int v = 0; v < 4; ++v) {
+        T row[N1];
+        load_row<N1>(su + v * VS + j * RS, row);
+        T dxi = T(0), deta = T(0);
+#pragma unroll
+        for (int m = 0; m < N1; ++m) {
+            dxi = fma_any(Di[m], row[m], dxi);
+            deta = fma_any(Dj[m], su[v * VS + m * RS + i], deta);
+        }
+        dxi += gRi * d1[v] + gLi * d3[v];
+        deta += gLj * d0[v] + gRj * d2[v];
+        Qx[v] = ji[0] * dxi + ji[2] * deta;
+        Qy[v] = ji[1] * dxi + ji[3] * deta;
+    }
+}
+
+// Loads of a flux-point thread: edge record, normal, own trace, the
+// neighbour's coinciding trace point or the ghost state.
+template <typename T>
+struct FacePoint {
+    EdgeRec r;
+    T nx, ny, len;
+    T qo[4], qn[4];
+};
+
+template <int N1, typename T>
+__device__ __forceinline__ void load_face_point(const StageArgsT<T>& a, long long e, int edge, int fp,
+                                                FacePoint<T>& f) {
+    constexpr int NFT = 4 * N1;
+    f.r = a.edges[e * 4 + edge];
+    T n[3];
+    load_normal(a.enrm + e * 4 + edge, n);
+    f.nx = n[0]; f.ny = n[1]; f.len = n[2];
+    load4_nc(a.Tin + (e * NFT + edge * N1 + fp) * 4, f.qo);
+    f.qn[0] = f.qo[0]; f.qn[1] = f.qo[1]; f.qn[2] = f.qo[2]; f.qn[3] = f.qo[3];
+    if (!(f.r.flags & kEdgeOrphan)) {
+        // interior: the neighbour's coinciding point; boundary: the ghost row
+        // written with the trace
+        load4_nc(a.Tin + (neighbour_row(f.r, a.n_elem) * N1 + (N1 - 1 - fp)) * 4, f.qn);
+    }
+}
+
+template <int P, typename T>
+__global__ void __launch_bounds__(Shape<P>::THREADS, NSMinBlocks<T>::grad)
+k_ns_grad(const StageArgsT<T> a) {
+    using S = Shape<P>;
+    constexpr int N1 = S::N1, NSP = S::NSP, NFT = S::NFT, TPE = S::TPE, EB = S::EB;
+    constexpr int RS = S::RS, VS = S::VS, FS = Tiles<P, T>::FS, DS = Tiles<P, T>::DS;
+    constexpr int QS = Tiles<P, T>::QS;
+    __shared__ T sOps[S::NOPS];
+    __shared__ __align__(16) T sU[EB * FS];
+    __shared__ __align__(16) T sDU[EB * DS];
+    __shared__ __align__(16) T sQ[EB * QS];
+
+    const int tid = threadIdx.x;
+    for (int t = tid; t < S::NOPS; t += blockDim.x) sOps[t] = a.ops[t];
+    const int el = tid / TPE, k = tid - el * TPE;
+    const long long e = (long long)blockIdx.x * EB + el;
+    const bool valid = (el < EB) && (e < a.n_elem);
+    const bool is_sp = valid && k < NSP, is_fp = valid && k < NFT;
+    const int edge = k / N1, fp = k - edge * N1;
+    const int i = k % N1, j = k / N1;
+
+    constexpr bool kRef = UsesRef<T>::value;
+    T ji[4];
+    if (is_sp) {
+        const long long idx = e * NSP + k;
+        T u[4];
+        if constexpr (kRef) {
+            // D (U - U_e): the reference drops out of the derivative exactly
+            double ud[4];
+            T ue[4];
+            load4(a.U + idx * 4, ud);
+            load_state(a.U + e * NSP * 4, ue);
+            state_minus_ref(ud, ue, u);
+        } else {
+            load_state(a.U + idx * 4, u);
+        }
+        load4_nc(a.Jinv + idx * 4, ji);
+        T* su = sU + el * FS + j * RS + i;
+#pragma unroll
+        for (int v = 0; v < 4; ++v) su[v * VS] = u[v];
+    }
+    if (is_fp) {
+        FacePoint<T> f;
+        load_face_point<N1>(a, e, edge, fp, f);
+        T d[4];
+#pragma unroll
+        for (int v = 0; v < 4; ++v) d[v] = (f.r.flags & kEdgeOrphan) ? T(0) : T(0.5) * (f.qn[v] - f.qo[v]);
+        store4(sDU + el * DS + k * 4, d);
+    }
+    __syncthreads();
+    if (is_sp) {
+        T Qx[4], Qy[4];
+        corrected_gradient<N1, RS, VS>(sU + el * FS, sDU + el * DS, sOps, i, j, ji, Qx, Qy);
+        T* sq = sQ + el * QS + j * RS + i;
+#pragma unroll
+        for (int v = 0; v < 4; ++v) { sq[v * VS] = Qx[v]; sq[(4 + v) * VS] = Qy[v]; }
+    }
+    __syncthreads();
+    if (is_fp) {
+        T t[8];
+        trace_point<N1, RS, VS>(sQ + el * QS, sOps + N1 * N1, sOps + N1 * N1 + N1, edge, fp, t);
+        trace_point<N1, RS, VS>(sQ + el * QS + 4 * VS, sOps + N1 * N1, sOps + N1 * N1 + N1, edge,
+                                fp, t + 4);
+        T* o = a.TQout + (e * NFT + k) * 8;
+        store4(o, t);
+        store4(o + 4, t + 4);
+    }
+}
+
+template <int P, int RIEM, typename T>
+__global__ void __launch_bounds__(Shape<P>::THREADS, NSMinBlocks<T>::stage)
+k_ns_stage(const StageArgsT<T> a) {
+    using S = Shape<P>;
+    constexpr int N1 = S::N1, NSP = S::NSP, NFT = S::NFT, TPE = S::TPE, EB = S::EB;
+    constexpr int RS = S::RS, VS = S::VS, FS = Tiles<P, T>::FS, DS = Tiles<P, T>::DS;
+    __shared__ T sOps[S::NOPS];
+    __shared__ __align__(16) T sF[EB * FS];
+    __shared__ __align__(16) T sG[EB * FS];
+    __shared__ __align__(16) T sD[EB * DS];   // face jumps of U, then flux differences
+    __shared__ __align__(16) T sU[EB * FS];   // stage state, then the new state
+    __shared__ double sRed[32];
+
+    const int tid = threadIdx.x;
+    for (int t = tid; t < S::NOPS; t += blockDim.x) sOps[t] = a.ops[t];
+    const int el = tid / TPE, k = tid - el * TPE;
+    const long long e = (long long)blockIdx.x * EB + el;
+    const bool valid = (el < EB) && (e < a.n_elem);
+    const bool is_sp = valid && k < NSP, is_fp = valid && k < NFT;
+    const T g = T(a.gamma), Re = T(a.Re), Pr = T(a.Pr);
+    const int edge = k / N1, fp = k - edge * N1;
+    const int i = k % N1, j = k / N1;
+
+    // ---- A1: loads, face jumps, stage state into shared memory
+    FacePoint<T> f;
+    T Qo[8], Qn[8];
+    if (is_fp) {
+        load_face_point<N1>(a, e, edge, fp, f);
+        const T* qt = a.TQ + (e * NFT + k) * 8;
+        load4_nc(qt, Qo);
+        load4_nc(qt + 4, Qo + 4);
+#pragma unroll
+        for (int v = 0; v < 8; ++v) Qn[v] = Qo[v];
+        if (!(f.r.flags & (kEdgeOrphan | kEdgeBoundary))) {
+            const T* qn = a.TQ + (((long long)f.r.nbr * 4 + f.r.nbr_edge) * N1 + (N1 - 1 - fp)) * 8;
+            load4_nc(qn, Qn);
+            load4_nc(qn + 4, Qn + 4);
+        }
+        T d[4];
+#pragma unroll
+        for (int v = 0; v < 4; ++v) d[v] = (f.r.flags & kEdgeOrphan) ? T(0) : T(0.5) * (f.qn[v] - f.qo[v]);
+        store4(sD + el * DS + k * 4, d);
+    }
+    constexpr bool kRef = UsesRef<T>::value;
+    T ue[4] = {T(0), T(0), T(0), T(0)};   // reference state (mixed form)
+    if (kRef && valid) load_state(a.U + e * NSP * 4, ue);
+    T u[4], ji[4], Jd = T(1);
+    if (is_sp) {
+        const long long idx = e * NSP + k;
+        double ud[4];
+        load4(a.U + idx * 4, ud);
+#pragma unroll
+        for (int v = 0; v < 4; ++v) u[v] = T(ud[v]);
+        load4_nc(a.Jinv + idx * 4, ji);
+        Jd = __ldg(a.J + idx);
+        if ((k & 3) == 0 && a.stage >= 2) prefetch_l2(a.U0 + idx * 4);
+        T* su = sU + el * FS + j * RS + i;
+        T w[4];
+        if constexpr (kRef) state_minus_ref(ud, ue, w);
+        else {
+#pragma unroll
+            for (int v = 0; v < 4; ++v) w[v] = u[v];
+        }
+#pragma unroll
+        for (int v = 0; v < 4; ++v) su[v * VS] = w[v];
+    }
+    __syncthreads();
+
+    // ---- A2: gradient, total transformed fluxes
+    if (is_sp) {
+        T Qx[4], Qy[4], Fv[4], Gv[4];
+        corrected_gradient<N1, RS, VS>(sU + el * FS, sD + el * DS, sOps, i, j, ji, Qx, Qy);
+        viscous_flux(u, Qx, Qy, g, Re, Pr, Fv, Gv);
+        T F[4], G[4];
+        euler_flux(u, g, F, G);
+        if constexpr (kRef) {
+            T Fe[4], Ge[4];
+            euler_flux(ue, g, Fe, Ge);
+#pragma unroll
+            for (int v = 0; v < 4; ++v) { F[v] -= Fe[v]; G[v] -= Ge[v]; }
+        }
+#pragma unroll
+        for (int v = 0; v < 4; ++v) { F[v] -= Fv[v]; G[v] -= Gv[v]; }
+        T* fo = sF + el * FS + j * RS + i;
+        T* ho = sG + el * FS + j * RS + i;
+#pragma unroll
+        for (int v = 0; v < 4; ++v) {
+            fo[v * VS] = Jd * (ji[0] * F[v] + ji[1] * G[v]);
+            ho[v * VS] = Jd * (ji[2] * F[v] + ji[3] * G[v]);
+        }
+    }
+    __syncthreads();   // face jumps and the stage state in shared memory are dead now
+
+    // ---- B: interface terms, evaluated from the left element's side
+    if (is_fp) {
+        T Fd[4] = {T(0), T(0), T(0), T(0)};
+        if (!(f.r.flags & kEdgeOrphan)) {
+            const bool right = (f.r.flags & kEdgeRight) != 0;
+            T UL[4], UR[4], Fc[4];
+#pragma unroll
+            for (int v = 0; v < 4; ++v) { UL[v] = right ? f.qn[v] : f.qo[v]; UR[v] = right ? f.qo[v] : f.qn[v]; }
+            riemann<RIEM>(UL, UR, f.nx, f.ny, g, Fc);
+            if constexpr (kRef) {
+                T Fe[4];
+                ref_flux_n(ue, g, f.nx, f.ny, Fe);
+#pragma unroll
+                for (int v = 0; v < 4; ++v) Fc[v] -= Fe[v];
+            }
+            T Ua[4], dxa[4], dya[4], Fv[4], Gv[4];
+#pragma unroll
+            for (int v = 0; v < 4; ++v) {
+                Ua[v] = T(0.5) * (UL[v] + UR[v]);
+                dxa[v] = T(0.5) * (Qo[v] + Qn[v]);
+                dya[v] = T(0.5) * (Qo[4 + v] + Qn[4 + v]);
+            }
+            viscous_flux(Ua, dxa, dya, g, Re, Pr, Fv, Gv);
+            const T ss = right ? T(-0.5) * f.len : T(0.5) * f.len;
+            const bool along_eta = (edge == 0 || edge == 2);
+            T Fn[4];
+            trace_point<N1, RS, VS>((along_eta ? sG : sF) + el * FS, sOps + N1 * N1,
+                                    sOps + N1 * N1 + N1, edge, fp, Fn);
+            const T sgn = (edge == 0 || edge == 3) ? T(-1) : T(1);
+#pragma unroll
+            for (int v = 0; v < 4; ++v)
+                Fd[v] = ss * (Fc[v] - (Fv[v] * f.nx + Gv[v] * f.ny)) - sgn * Fn[v];
+        }
+        store4(sD + el * DS + k * 4, Fd);
+    }
+    __syncthreads();
+
+    // ---- C: divergence, VCJH correction, 1/J, stage update
+    double rsq = 0.0;
+    if (is_sp) {
+        const long long idx = e * NSP + k;
+        double u0[4];
+        if (a.stage >= 2) load4(a.U0 + idx * 4, u0);
+        T Di[N1], Dj[N1];
+#pragma unroll
+        for (int m = 0; m < N1; ++m) { Di[m] = sOps[i * N1 + m]; Dj[m] = sOps[j * N1 + m]; }
+        const T* gL = sOps + N1 * N1 + 2 * N1;
+        const T* gR = gL + N1;
+        const T gRi = gR[i], gLi = gL[i], gRj = gR[j], gLj = gL[j];
+        const T* fo = sF + el * FS;
+        const T* ho = sG + el * FS;
+        const T* d = sD + el * DS;
+        T c1[4], c3[4], c2[4], c0[4];
+        load4(d + (1 * N1 + j) * 4, c1);
+        load4(d + (3 * N1 + (N1 - 1 - j)) * 4, c3);
+        load4(d + (2 * N1 + (N1 - 1 - i)) * 4, c2);
+        load4(d + (0 * N1 + i) * 4, c0);
+        const T iJ = rcp_any(Jd);
+        T res[4];
+#pragma unroll
+        for (int v = 0; v < 4; ++v) {
+            T fr[N1];
+            load_row<N1>(fo + v * VS + j * RS, fr);
+            T div = T(0);
+#pragma unroll
+            for (int m = 0; m < N1; ++m) div = fma_any(Di[m], fr[m], div);
+#pragma unroll
+            for (int m = 0; m < N1; ++m) div = fma_any(Dj[m], ho[v * VS + m * RS + i], div);
+            const T corr = gRi * c1[v] - gLi * c3[v] + gRj * c2[v] - gLj * c0[v];
+            res[v] = -(div + corr) * iJ;
+        }
+        if (a.stage == 0) {
+            double rd[4];
+#pragma unroll
+            for (int v = 0; v < 4; ++v) { rd[v] = double(res[v]); rsq += rd[v] * rd[v]; }
+            store4(a.R + idx * 4, rd);
+        } else {
+            double us[4];
+            if constexpr (sizeof(T) == 8) {
+#pragma unroll
+                for (int v = 0; v < 4; ++v) us[v] = double(u[v]);
+            } else {
+                load4(a.U + idx * 4, us);
+            }
+            double uo[4];
+            rk_update(a.stage, *a.dt, us, u0, res, uo);
+            store4(a.Uout + idx * 4, uo);
+            T* su = sU + el * FS + j * RS + i;
+            T un[4];
+            if constexpr (kRef) state_minus_ref(uo, ue, un);
+            else {
+#pragma unroll
+                for (int v = 0; v < 4; ++v) un[v] = T(uo[v]);
+            }
+#pragma unroll
+            for (int v = 0; v < 4; ++v) su[v * VS] = un[v];
+            if (a.stage == 3) {
+#pragma unroll
+                for (int v = 0; v < 4; ++v) rsq += double(res[v]) * double(res[v]);
+            }
+        }
+    }
+    if (a.stage == 0 || a.stage == 3) {
+        const double bs = block_sum(rsq, sRed);
+        if (tid == 0) a.partials[blockIdx.x] = bs;
+    }
+    if (a.stage == 0) return;
+    __syncthreads();
+
+    // ---- D: traces of the new state
+    if (is_fp) {
+        T t[4];
+        trace_point<N1, RS, VS>(sU + el * FS, sOps + N1 * N1, sOps + N1 * N1 + N1, edge, fp, t);
+        if constexpr (kRef) {
+#pragma unroll
+            for (int v = 0; v < 4; ++v) t[v] += ue[v];
+        }
+        store4(a.Tout + (e * NFT + k) * 4, t);
+        if (f.r.flags & kEdgeBoundary) store_ghost<N1>(a, f.r, f.nx, f.ny, fp, t);
+    }
+}
+
+template <int P, typename T>
+cudaError_t ns_grad_t(const StageArgsT<T>& a, cudaStream_t s) {
+    using S = Shape<P>;
+    const long long grid = (a.n_elem + S::EB - 1) / S::EB;
+    if (grid <= 0) return cudaSuccess;
+    static bool set = false;
+    if (!set) { prefer_shared(k_ns_grad<P, T>); set = true; }
+    k_ns_grad<P, T><<<(unsigned)grid, S::THREADS, 0, s>>>(a);
+    return cudaGetLastError();
+}
+
+template <int P, int RIEM, typename T>
+cudaError_t ns_stage_t(const StageArgsT<T>& a, cudaStream_t s) {
+    using S = Shape<P>;
+    const long long grid = (a.n_elem + S::EB - 1) / S::EB;
+    if (grid <= 0) return cudaSuccess;
+    static bool set = false;
+    if (!set) { prefer_shared(k_ns_stage<P, RIEM, T>); set = true; }
+    k_ns_stage<P, RIEM, T><<<(unsigned)grid, S::THREADS, 0, s>>>(a);
+    return cudaGetLastError();
+}
+
+template <int P, typename T>
+cudaError_t ns_stage_p(int riemann, const StageArgsT<T>& a, cudaStream_t s) {
+    switch (riemann) {
+        case ZJ_RIEMANN_RUSANOV: return ns_stage_t<P, ZJ_RIEMANN_RUSANOV>(a, s);
+        case ZJ_RIEMANN_ROE: return ns_stage_t<P, ZJ_RIEMANN_ROE>(a, s);
+        case ZJ_RIEMANN_HLLC: return ns_stage_t<P, ZJ_RIEMANN_HLLC>(a, s);
+        default: return cudaErrorInvalidValue;
+    }
+}
+
+template <typename T>
+cudaError_t ns_grad_dispatch(int P, const StageArgsT<T>& a, cudaStream_t s) {
+    switch (P) {
+        case 1: return ns_grad_t<1>(a, s);
+        case 2: return ns_grad_t<2>(a, s);
+        case 3: return ns_grad_t<3>(a, s);
+        case 4: return ns_grad_t<4>(a, s);
+        case 5: return ns_grad_t<5>(a, s);
+        default: return cudaErrorInvalidValue;
+    }
+}
+
+template <typename T>
+cudaError_t ns_stage_dispatch(int P, int riemann, const StageArgsT<T>& a, cudaStream_t s) {
+    switch (P) {
+        case 1: return ns_stage_p<1>(riemann, a, s);
+        case 2: return ns_stage_p<2>(riemann, a, s);
+        case 3: return ns_stage_p<3>(riemann, a, s);
+        case 4: return ns_stage_p<4>(riemann, a, s);
+        case 5: return ns_stage_p<5>(riemann, a, s);
+        default: return cudaErrorInvalidValue;
+    }
+}
+
+}  // namespace
+}  // namespace zj

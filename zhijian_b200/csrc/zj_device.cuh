@@ -45,17 +45,77 @@ __device__ __forceinline__ void store4(double* p, const double* v) {
     *reinterpret_cast<double2*>(p + 2) = make_double2(v[2], v[3]);
 }
 
+// FP32 twins (the mixed-precision kernels' traces, metrics and tiles).
+__device__ __forceinline__ void load4(const float* p, float* v) {
+    const float4 a = *reinterpret_cast<const float4*>(p);
+    v[0] = a.x; v[1] = a.y; v[2] = a.z; v[3] = a.w;
+}
+__device__ __forceinline__ void load4_nc(const float* p, float* v) {
+    const float4 a = __ldg(reinterpret_cast<const float4*>(p));
+    v[0] = a.x; v[1] = a.y; v[2] = a.z; v[3] = a.w;
+}
+__device__ __forceinline__ void store4(float* p, const float* v) {
+    *reinterpret_cast<float4*>(p) = make_float4(v[0], v[1], v[2], v[3]);
+}
+
+// (nx, ny, len) of an edge-normal record.
+__device__ __forceinline__ void load_normal(const double4* p, double* n) {
+    const double2 a = __ldg(reinterpret_cast<const double2*>(p));
+    const double2 b = __ldg(reinterpret_cast<const double2*>(p) + 1);
+    n[0] = a.x; n[1] = a.y; n[2] = b.x;
+}
+__device__ __forceinline__ void load_normal(const float4* p, float* n) {
+    const float4 a = __ldg(p);
+    n[0] = a.x; n[1] = a.y; n[2] = a.z;
+}
+
 // 1/x: Newton-Raphson for positive normal x, IEEE division otherwise (zero,
 // negative or non-finite densities, which the reference also divides by).
 __device__ __forceinline__ double rcp_any(double x) {
     return (x > 1e-300 && x < 1e300) ? zj_rcp(x) : 1.0 / x;
 }
 
+// FP32 (the mixed-precision form): the hardware's approximate reciprocal and
+// square root (rcp.approx / sqrt.approx, within 1-2 ulp of float), whose
+// error sits at the FP32 rounding level the form already carries.
+__device__ __forceinline__ float rcp_any(float x) {
+    float y;
+    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
+__device__ __forceinline__ double sqrt_any(double a) { return zj_sqrt(a); }
+__device__ __forceinline__ float sqrt_any(float a) {
+    float y;
+    asm("sqrt.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(a));
+    return y;
+}
+// a / b: IEEE division in FP64, a * (1/b) in FP32.
+__device__ __forceinline__ double div_any(double a, double b) { return a / b; }
+__device__ __forceinline__ float div_any(float a, float b) { return a * rcp_any(b); }
+__device__ __forceinline__ double pow_any(double a, double b) { return pow(a, b); }
+__device__ __forceinline__ float pow_any(float a, float b) { return __powf(a, b); }
+__device__ __forceinline__ double fma_any(double a, double b, double c) { return __fma_rn(a, b, c); }
+__device__ __forceinline__ float fma_any(float a, float b, float c) { return __fmaf_rn(a, b, c); }
+__device__ __forceinline__ double max_any(double a, double b) { return fmax(a, b); }
+__device__ __forceinline__ float max_any(float a, float b) { return fmaxf(a, b); }
+__device__ __forceinline__ double abs_any(double a) { return fabs(a); }
+__device__ __forceinline__ float abs_any(float a) { return fabsf(a); }
+
 __device__ __forceinline__ void prefetch_l2(const void* p) {
     asm volatile("prefetch.global.L2 [%0];" ::"l"(p));
 }
 
 // N values of a 16-byte aligned shared-memory row, with 16-byte loads.
+template <int N>
+__device__ __forceinline__ void load_row(const float* row, float* out) {
+#pragma unroll
+    for (int m = 0; m + 1 < N; m += 2) {
+        const float2 t = *reinterpret_cast<const float2*>(row + m);
+        out[m] = t.x;
+        out[m + 1] = t.y;
+    }
+    if (N & 1) out[N - 1] = row[N - 1];
+}
 template <int N>
 __device__ __forceinline__ void load_row(const double* row, double* out) {
 #pragma unroll
@@ -75,23 +135,23 @@ __device__ __forceinline__ void load_row(const double* row, double* out) {
 // ascending:  edge 0: sum_j l_j(-1) s[j][fp]     edge 1: sum_i l_i(1) s[fp][i]
 //             edge 2: sum_j l_j(1) s[j][N1-1-fp] edge 3: sum_i l_i(-1) s[N1-1-fp][i]
 // Written without branches on the edge (the four edges share a warp).
-template <int N1, int RS, int VS>
-__device__ __forceinline__ void trace_point(const double* s, const double* Lm, const double* Lp,
-                                            int edge, int fp, double* out) {
+template <int N1, int RS, int VS, typename T>
+__device__ __forceinline__ void trace_point(const T* s, const T* Lm, const T* Lp,
+                                            int edge, int fp, T* out) {
     const int line = (edge >= 2) ? (N1 - 1 - fp) : fp;
     const bool along_eta = (edge == 0 || edge == 2);
     const int base = along_eta ? line : line * RS;
     const int stride = along_eta ? RS : 1;
-    const double* W = (edge == 0 || edge == 3) ? Lm : Lp;
-    double w[N1];
+    const T* W = (edge == 0 || edge == 3) ? Lm : Lp;
+    T w[N1];
 #pragma unroll
     for (int m = 0; m < N1; ++m) w[m] = W[m];
 #pragma unroll
     for (int v = 0; v < 4; ++v) {
-        const double* sv = s + v * VS + base;
-        double t = 0.0;
+        const T* sv = s + v * VS + base;
+        T t = T(0);
 #pragma unroll
-        for (int m = 0; m < N1; ++m) t = fma(w[m], sv[m * stride], t);
+        for (int m = 0; m < N1; ++m) t = fma_any(w[m], sv[m * stride], t);
         out[v] = t;
     }
 }

@@ -7,31 +7,41 @@
 
 namespace zj {
 
-// Arguments of one fused residual / RK-stage launch.  Device pointers.
-struct StageArgs {
+// Arguments of one fused residual / RK-stage launch.  Device pointers.  T is
+// the arithmetic type of the kernels (double: FP64 path; float: the
+// mixed-precision form); the conserved state, the residual output, dt and the
+// norm partials are FP64 in both.
+template <typename T> struct Vec4Of;
+template <> struct Vec4Of<double> { using type = double4; };
+template <> struct Vec4Of<float> { using type = float4; };
+
+template <typename T>
+struct StageArgsT {
     const double* U;        // stage input state, AoS [E][n_sp][4]
     const double* U0;       // RK base state (stages 2, 3)
     double* Uout;           // stage output state
-    const double* Tin;      // traces of U, [E][4 edges][n1][4], then the physics-mode
+    const T* Tin;           // traces of U, [E][4 edges][n1][4], then the physics-mode
                             // boundary ghost rows [n_bnd][n1][4] (stored mirrored)
-    double* Tout;           // traces of Uout
+    T* Tout;                // traces of Uout
     double* R;              // residual output (stage 0 only)
-    const double* Jinv;     // [E][n_sp][4] = (xi_x, xi_y, eta_x, eta_y)
-    const double* J;        // [E][n_sp]
+    const T* Jinv;          // [E][n_sp][4] = (xi_x, xi_y, eta_x, eta_y)
+    const T* J;             // [E][n_sp]
     const EdgeRec* edges;   // [E][4]
-    const double4* enrm;    // [E][4] = (face nx, face ny, edge length, 0)
-    const double* bc;       // [slots][8]
-    const double* ops;      // packed 1D operators, see OpsLayout
+    const typename Vec4Of<T>::type* enrm;  // [E][4] = (face nx, face ny, edge length, 0)
+    const T* bc;            // [slots][8]
+    const T* ops;           // packed 1D operators, see OpsLayout
     const double* dt;       // device scalar: step size
     double* partials;       // [grid] per-CTA sum of R^2 (stage 3 and stage 0)
     long long n_elem;
     double gamma;
     int stage;              // 0: residual only; 1..3: SSP-RK3 stage
     // Navier-Stokes
-    const double* TQ;       // gradient traces of U, [E][4 edges][n1][8] = (dU/dx, dU/dy)
-    double* TQout;          // gradient traces written by the gradient launch
+    const T* TQ;            // gradient traces of U, [E][4 edges][n1][8] = (dU/dx, dU/dy)
+    T* TQout;               // gradient traces written by the gradient launch
     double Re, Pr;
 };
+using StageArgs = StageArgsT<double>;
+using StageArgs32 = StageArgsT<float>;
 
 // Packed operator block: D1[n1*n1], Lm[n1], Lp[n1], gL[n1], gR[n1].
 inline int ops_size(int n1) { return n1 * n1 + 4 * n1; }
@@ -39,13 +49,18 @@ void pack_ops(const Operators1D& o, std::vector<double>& out);
 
 // Compat-mode FP64 launches (reference residual semantics).
 cudaError_t launch_compat_stage(int P, const StageArgs& a, cudaStream_t s, int* grid_out);
-// Physics-mode FP64 launches (conservative FR, VCJH, selected Riemann solver).
+// Physics-mode launches (conservative FR, VCJH, selected Riemann solver),
+// FP64 and mixed precision.
 cudaError_t launch_phys_stage(int P, int riemann, const StageArgs& a, cudaStream_t s);
+cudaError_t launch_phys_stage(int P, int riemann, const StageArgs32& a, cudaStream_t s);
 // Physics-mode traces of a.U into a.Tout, boundary ghost rows included.
 cudaError_t launch_phys_traces(int P, const StageArgs& a, cudaStream_t s);
+cudaError_t launch_phys_traces(int P, const StageArgs32& a, cudaStream_t s);
 // Navier-Stokes: gradient traces of a stage state, then the stage itself.
 cudaError_t launch_ns_grad(int P, const StageArgs& a, cudaStream_t s);
+cudaError_t launch_ns_grad(int P, const StageArgs32& a, cudaStream_t s);
 cudaError_t launch_ns_stage(int P, int riemann, const StageArgs& a, cudaStream_t s);
+cudaError_t launch_ns_stage(int P, int riemann, const StageArgs32& a, cudaStream_t s);
 cudaError_t launch_traces(int P, const double* U, double* T, const double* ops,
                           long long n_elem, cudaStream_t s);
 int stage_grid(int P, long long n_elem);

@@ -1,6 +1,8 @@
 // zj_physics.cuh -- device physics of the physics-mode residual kernels:
 // ideal-gas relations, the reference's Riemann solvers and ghost states, and
-// the viscous flux.
+// the viscous flux.  Templated on the arithmetic type T: double for the FP64
+// path, float for the mixed-precision form.  Both instantiations run the same
+// operations in the same order; the FP64 one is the reference-parity path.
 #pragma once
 
 #include <cuda_runtime.h>
@@ -17,28 +19,30 @@ using namespace dev;
 // ------------------------------------------------------------ physics --
 
 // IdealGas::pressure (euler.hpp:16-23)
-__device__ __forceinline__ double pressure(const double* U, double g) {
-    const double ir = rcp_any(U[0]);
-    const double u = U[1] * ir, v = U[2] * ir, E = U[3] * ir;
-    return (g - 1.0) * U[0] * (E - 0.5 * (u * u + v * v));
+template <typename T>
+__device__ __forceinline__ T pressure(const T* U, T g) {
+    const T ir = rcp_any(U[0]);
+    const T u = U[1] * ir, v = U[2] * ir, E = U[3] * ir;
+    return (g - T(1)) * U[0] * (E - T(0.5) * (u * u + v * v));
 }
 
 // IdealGas::soundSpeed (euler.hpp:34-41)
-__device__ __forceinline__ double sound_speed(double p_raw, double rho_raw, double g) {
-    const double p = fmax(p_raw, 1e-10), rho = fmax(rho_raw, 1e-10);
-    return zj_sqrt(g * p * rcp_any(rho));
+template <typename T>
+__device__ __forceinline__ T sound_speed(T p_raw, T rho_raw, T g) {
+    const T p = max_any(p_raw, T(1e-10)), rho = max_any(rho_raw, T(1e-10));
+    return sqrt_any(g * p * rcp_any(rho));
 }
 
 // IdealGas::fluxNormal (euler.hpp:133-147): floored density and pressure,
 // total enthalpy from the unfloored pressure.
-__device__ __forceinline__ void flux_normal(const double* U, double praw, double nx, double ny,
-                                            double* Fn) {
-    const double rho = fmax(U[0], 1e-10);
-    const double ir = rcp_any(rho);
-    const double u = U[1] * ir, v = U[2] * ir;
-    const double p = fmax(praw, 1e-10);
-    const double H = U[3] + praw;
-    const double vn = u * nx + v * ny;
+template <typename T>
+__device__ __forceinline__ void flux_normal(const T* U, T praw, T nx, T ny, T* Fn) {
+    const T rho = max_any(U[0], T(1e-10));
+    const T ir = rcp_any(rho);
+    const T u = U[1] * ir, v = U[2] * ir;
+    const T p = max_any(praw, T(1e-10));
+    const T H = U[3] + praw;
+    const T vn = u * nx + v * ny;
     Fn[0] = rho * vn;
     Fn[1] = rho * u * vn + p * nx;
     Fn[2] = rho * v * vn + p * ny;
@@ -46,170 +50,171 @@ __device__ __forceinline__ void flux_normal(const double* U, double praw, double
 }
 
 // RiemannSolvers::rusanov (euler.hpp:184-200): s = |u| + c of each side.
-__device__ __forceinline__ void riemann_rusanov(const double* UL, const double* UR, double nx,
-                                                double ny, double g, double* F) {
-    const double pL = pressure(UL, g), pR = pressure(UR, g);
-    double FL[4], FR[4];
+template <typename T>
+__device__ __forceinline__ void riemann_rusanov(const T* UL, const T* UR, T nx, T ny, T g, T* F) {
+    const T pL = pressure(UL, g), pR = pressure(UR, g);
+    T FL[4], FR[4];
     flux_normal(UL, pL, nx, ny, FL);
     flux_normal(UR, pR, nx, ny, FR);
-    const double irL = rcp_any(UL[0]), irR = rcp_any(UR[0]);
-    const double uL = UL[1] * irL, vL = UL[2] * irL, uR = UR[1] * irR, vR = UR[2] * irR;
-    const double sL = zj_sqrt(uL * uL + vL * vL) + sound_speed(pL, UL[0], g);
-    const double sR = zj_sqrt(uR * uR + vR * vR) + sound_speed(pR, UR[0], g);
-    const double smax = fmax(sL, sR);
+    const T irL = rcp_any(UL[0]), irR = rcp_any(UR[0]);
+    const T uL = UL[1] * irL, vL = UL[2] * irL, uR = UR[1] * irR, vR = UR[2] * irR;
+    const T sL = sqrt_any(uL * uL + vL * vL) + sound_speed(pL, UL[0], g);
+    const T sR = sqrt_any(uR * uR + vR * vR) + sound_speed(pR, UR[0], g);
+    const T smax = max_any(sL, sR);
 #pragma unroll
-    for (int i = 0; i < 4; ++i) F[i] = 0.5 * (FL[i] + FR[i]) - 0.5 * smax * (UR[i] - UL[i]);
+    for (int i = 0; i < 4; ++i) F[i] = T(0.5) * (FL[i] + FR[i]) - T(0.5) * smax * (UR[i] - UL[i]);
 }
 
 // RiemannSolvers::roe with Harten's entropy fix (euler.hpp:204-294).
-__device__ __forceinline__ void riemann_roe(const double* UL, const double* UR, double nx,
-                                            double ny, double g, double* F) {
-    const double rhoL = fmax(UL[0], 1e-10), rhoR = fmax(UR[0], 1e-10);
-    const double irL = rcp_any(rhoL), irR = rcp_any(rhoR);
-    const double uL = UL[1] * irL, vL = UL[2] * irL, uR = UR[1] * irR, vR = UR[2] * irR;
-    const double pL = pressure(UL, g), pR = pressure(UR, g);
-    const double HL = (UL[3] + pL) * irL, HR = (UR[3] + pR) * irR;
-    const double sL = zj_sqrt(rhoL), sR = zj_sqrt(rhoR);
-    const double iden = rcp_any(fmax(sL + sR, 1e-10));
-    const double rhoRoe = sL * sR;
-    const double uRoe = (sL * uL + sR * uR) * iden, vRoe = (sL * vL + sR * vR) * iden;
-    const double HRoe = (sL * HL + sR * HR) * iden;
-    const double vnRoe = uRoe * nx + vRoe * ny, qsq = uRoe * uRoe + vRoe * vRoe;
-    const double c = zj_sqrt(fmax((g - 1.0) * (HRoe - 0.5 * qsq), 1e-10));
-    double l1 = fabs(vnRoe - c);
-    const double l2 = fabs(vnRoe);
-    double l4 = fabs(vnRoe + c);
-    const double eps = 0.1 * c;
-    if (l1 < eps) l1 = (l1 * l1 + eps * eps) * rcp_any(2.0 * eps);
-    if (l4 < eps) l4 = (l4 * l4 + eps * eps) * rcp_any(2.0 * eps);
-    const double drho = rhoR - rhoL, du = uR - uL, dv = vR - vL;
-    const double dp = pR - pL;
-    const double dvn = du * nx + dv * ny;
-    const double ics = rcp_any(fmax(c * c, 1e-10));
-    const double a1 = (dp - rhoRoe * c * dvn) * (0.5 * ics);
-    const double a2 = drho - dp * ics;
-    const double a3 = rhoRoe * (dv * nx - du * ny);
-    const double a4 = (dp + rhoRoe * c * dvn) * (0.5 * ics);
-    double FL[4], FR[4];
+template <typename T>
+__device__ __forceinline__ void riemann_roe(const T* UL, const T* UR, T nx, T ny, T g, T* F) {
+    const T rhoL = max_any(UL[0], T(1e-10)), rhoR = max_any(UR[0], T(1e-10));
+    const T irL = rcp_any(rhoL), irR = rcp_any(rhoR);
+    const T uL = UL[1] * irL, vL = UL[2] * irL, uR = UR[1] * irR, vR = UR[2] * irR;
+    const T pL = pressure(UL, g), pR = pressure(UR, g);
+    const T HL = (UL[3] + pL) * irL, HR = (UR[3] + pR) * irR;
+    const T sL = sqrt_any(rhoL), sR = sqrt_any(rhoR);
+    const T iden = rcp_any(max_any(sL + sR, T(1e-10)));
+    const T rhoRoe = sL * sR;
+    const T uRoe = (sL * uL + sR * uR) * iden, vRoe = (sL * vL + sR * vR) * iden;
+    const T HRoe = (sL * HL + sR * HR) * iden;
+    const T vnRoe = uRoe * nx + vRoe * ny, qsq = uRoe * uRoe + vRoe * vRoe;
+    const T c = sqrt_any(max_any((g - T(1)) * (HRoe - T(0.5) * qsq), T(1e-10)));
+    T l1 = abs_any(vnRoe - c);
+    const T l2 = abs_any(vnRoe);
+    T l4 = abs_any(vnRoe + c);
+    const T eps = T(0.1) * c;
+    if (l1 < eps) l1 = (l1 * l1 + eps * eps) * rcp_any(T(2) * eps);
+    if (l4 < eps) l4 = (l4 * l4 + eps * eps) * rcp_any(T(2) * eps);
+    const T drho = rhoR - rhoL, du = uR - uL, dv = vR - vL;
+    const T dp = pR - pL;
+    const T dvn = du * nx + dv * ny;
+    const T ics = rcp_any(max_any(c * c, T(1e-10)));
+    const T a1 = (dp - rhoRoe * c * dvn) * (T(0.5) * ics);
+    const T a2 = drho - dp * ics;
+    const T a3 = rhoRoe * (dv * nx - du * ny);
+    const T a4 = (dp + rhoRoe * c * dvn) * (T(0.5) * ics);
+    T FL[4], FR[4];
     flux_normal(UL, pL, nx, ny, FL);
     flux_normal(UR, pR, nx, ny, FR);
-    const double tx = -ny, ty = nx;
-    const double w1 = l1 * a1, w2 = l2 * a2, w3 = l2 * a3, w4 = l4 * a4;
-    const double dF0 = w1 + w2 + w4;
-    const double dF1 = w1 * (uRoe - c * nx) + w2 * uRoe + w3 * tx + w4 * (uRoe + c * nx);
-    const double dF2 = w1 * (vRoe - c * ny) + w2 * vRoe + w3 * ty + w4 * (vRoe + c * ny);
-    const double dF3 = w1 * (HRoe - c * vnRoe) + w2 * 0.5 * qsq + w3 * (uRoe * tx + vRoe * ty) +
-                       w4 * (HRoe + c * vnRoe);
-    F[0] = 0.5 * (FL[0] + FR[0]) - 0.5 * dF0;
-    F[1] = 0.5 * (FL[1] + FR[1]) - 0.5 * dF1;
-    F[2] = 0.5 * (FL[2] + FR[2]) - 0.5 * dF2;
-    F[3] = 0.5 * (FL[3] + FR[3]) - 0.5 * dF3;
+    const T tx = -ny, ty = nx;
+    const T w1 = l1 * a1, w2 = l2 * a2, w3 = l2 * a3, w4 = l4 * a4;
+    const T dF0 = w1 + w2 + w4;
+    const T dF1 = w1 * (uRoe - c * nx) + w2 * uRoe + w3 * tx + w4 * (uRoe + c * nx);
+    const T dF2 = w1 * (vRoe - c * ny) + w2 * vRoe + w3 * ty + w4 * (vRoe + c * ny);
+    const T dF3 = w1 * (HRoe - c * vnRoe) + w2 * T(0.5) * qsq + w3 * (uRoe * tx + vRoe * ty) +
+                  w4 * (HRoe + c * vnRoe);
+    F[0] = T(0.5) * (FL[0] + FR[0]) - T(0.5) * dF0;
+    F[1] = T(0.5) * (FL[1] + FR[1]) - T(0.5) * dF1;
+    F[2] = T(0.5) * (FL[2] + FR[2]) - T(0.5) * dF2;
+    F[3] = T(0.5) * (FL[3] + FR[3]) - T(0.5) * dF3;
 }
 
-__device__ __forceinline__ double away_from_zero(double d) {
-    return (fabs(d) < 1e-10) ? ((d >= 0) ? 1e-10 : -1e-10) : d;
+template <typename T>
+__device__ __forceinline__ T away_from_zero(T d) {
+    return (abs_any(d) < T(1e-10)) ? ((d >= T(0)) ? T(1e-10) : T(-1e-10)) : d;
 }
 
 // RiemannSolvers::hllc (euler.hpp:298-375).
-__device__ __forceinline__ void riemann_hllc(const double* UL, const double* UR, double nx,
-                                             double ny, double g, double* F) {
-    const double rhoL = fmax(UL[0], 1e-10), rhoR = fmax(UR[0], 1e-10);
-    const double irL = rcp_any(rhoL), irR = rcp_any(rhoR);
-    const double uL = UL[1] * irL, vL = UL[2] * irL, uR = UR[1] * irR, vR = UR[2] * irR;
-    const double pLr = pressure(UL, g), pRr = pressure(UR, g);
-    const double pL = fmax(pLr, 1e-10), pR = fmax(pRr, 1e-10);
-    const double cL = sound_speed(pLr, UL[0], g), cR = sound_speed(pRr, UR[0], g);
-    const double vnL = uL * nx + vL * ny, vnR = uR * nx + vR * ny;
-    double ps = 0.5 * (pL + pR) - 0.5 * (vnR - vnL) * 0.5 * (rhoL + rhoR) * 0.5 * (cL + cR);
-    ps = fmax(ps, 1e-10);
-    const double k = (g + 1.0) / (2.0 * g);
-    const double qL = (ps <= pL) ? 1.0 : zj_sqrt(1.0 + k * (ps * rcp_any(pL) - 1.0));
-    const double qR = (ps <= pR) ? 1.0 : zj_sqrt(1.0 + k * (ps * rcp_any(pR) - 1.0));
-    const double SL = vnL - cL * qL, SR = vnR + cR * qR;
-    const double dSM = away_from_zero(rhoL * (SL - vnL) - rhoR * (SR - vnR));
-    const double SM = (pR - pL + rhoL * vnL * (SL - vnL) - rhoR * vnR * (SR - vnR)) / dSM;
+template <typename T>
+__device__ __forceinline__ void riemann_hllc(const T* UL, const T* UR, T nx, T ny, T g, T* F) {
+    const T rhoL = max_any(UL[0], T(1e-10)), rhoR = max_any(UR[0], T(1e-10));
+    const T irL = rcp_any(rhoL), irR = rcp_any(rhoR);
+    const T uL = UL[1] * irL, vL = UL[2] * irL, uR = UR[1] * irR, vR = UR[2] * irR;
+    const T pLr = pressure(UL, g), pRr = pressure(UR, g);
+    const T pL = max_any(pLr, T(1e-10)), pR = max_any(pRr, T(1e-10));
+    const T cL = sound_speed(pLr, UL[0], g), cR = sound_speed(pRr, UR[0], g);
+    const T vnL = uL * nx + vL * ny, vnR = uR * nx + vR * ny;
+    T ps = T(0.5) * (pL + pR) - T(0.5) * (vnR - vnL) * T(0.5) * (rhoL + rhoR) * T(0.5) * (cL + cR);
+    ps = max_any(ps, T(1e-10));
+    const T k = div_any(g + T(1), T(2) * g);
+    const T qL = (ps <= pL) ? T(1) : sqrt_any(T(1) + k * (ps * rcp_any(pL) - T(1)));
+    const T qR = (ps <= pR) ? T(1) : sqrt_any(T(1) + k * (ps * rcp_any(pR) - T(1)));
+    const T SL = vnL - cL * qL, SR = vnR + cR * qR;
+    const T dSM = away_from_zero(rhoL * (SL - vnL) - rhoR * (SR - vnR));
+    const T SM = div_any(pR - pL + rhoL * vnL * (SL - vnL) - rhoR * vnR * (SR - vnR), dSM);
     // One star-state evaluation for either side of the contact (no divergent
     // call sites): the side is selected, then the same arithmetic runs.
-    const bool left = (SM >= 0.0);
-    const double* Uk = left ? UL : UR;
-    const double rk = left ? rhoL : rhoR, uk = left ? uL : uR, vk = left ? vL : vR;
-    const double vnk = left ? vnL : vnR, pk = left ? pL : pR, Sk = left ? SL : SR;
-    const double pkr = left ? pLr : pRr;
-    const double dK = away_from_zero(Sk - SM);
-    const double dvn = away_from_zero(Sk - vnk);
-    const double fac = rk * dvn / dK;
-    double Us[4];
+    const bool left = (SM >= T(0));
+    const T* Uk = left ? UL : UR;
+    const T rk = left ? rhoL : rhoR, uk = left ? uL : uR, vk = left ? vL : vR;
+    const T vnk = left ? vnL : vnR, pk = left ? pL : pR, Sk = left ? SL : SR;
+    const T pkr = left ? pLr : pRr;
+    const T dK = away_from_zero(Sk - SM);
+    const T dvn = away_from_zero(Sk - vnk);
+    const T fac = div_any(rk * dvn, dK);
+    T Us[4];
     Us[0] = fac;
     Us[1] = fac * (uk + (SM - vnk) * nx);
     Us[2] = fac * (vk + (SM - vnk) * ny);
-    Us[3] = fac * (Uk[3] / rk + (SM - vnk) * (SM + pk / (rk * dvn)));
-    double Fk[4];
+    Us[3] = fac * (div_any(Uk[3], rk) + (SM - vnk) * (SM + div_any(pk, rk * dvn)));
+    T Fk[4];
     flux_normal(Uk, pkr, nx, ny, Fk);
 #pragma unroll
     for (int i = 0; i < 4; ++i) F[i] = Fk[i] + Sk * (Us[i] - Uk[i]);
-    if (SL >= 0.0) flux_normal(UL, pLr, nx, ny, F);
-    else if (SR <= 0.0) flux_normal(UR, pRr, nx, ny, F);
+    if (SL >= T(0)) flux_normal(UL, pLr, nx, ny, F);
+    else if (SR <= T(0)) flux_normal(UR, pRr, nx, ny, F);
 }
 
-template <int RIEM>
-__device__ __forceinline__ void riemann(const double* UL, const double* UR, double nx, double ny,
-                                        double g, double* F) {
+template <int RIEM, typename T>
+__device__ __forceinline__ void riemann(const T* UL, const T* UR, T nx, T ny, T g, T* F) {
     if (RIEM == ZJ_RIEMANN_ROE) riemann_roe(UL, UR, nx, ny, g, F);
     else if (RIEM == ZJ_RIEMANN_HLLC) riemann_hllc(UL, UR, nx, ny, g, F);
     else riemann_rusanov(UL, UR, nx, ny, g, F);
 }
 
-__device__ __forceinline__ void prim2cons(double rho, double u, double v, double p, double g,
-                                          double* U) {
+template <typename T>
+__device__ __forceinline__ void prim2cons(T rho, T u, T v, T p, T g, T* U) {
     U[0] = rho; U[1] = rho * u; U[2] = rho * v;
-    U[3] = p / (g - 1.0) + 0.5 * rho * (u * u + v * v);
+    U[3] = div_any(p, g - T(1)) + T(0.5) * rho * (u * u + v * v);
 }
 
 // BoundaryCondition::ghostState of every class (boundary_condition.hpp:42-311)
 // with the parameters createBCFromSpec gives them (boundary_condition.cpp:32-64),
 // packed per boundary slot: far-field (rho, u, v, p) at infinity; outflow
 // p_static; inflow p_total, T_total, flow direction; wall T_wall (0: adiabatic).
-__device__ __forceinline__ void ghost_phys(const double* Ui, double nx, double ny, int bct,
-                           const double* __restrict__ bcd, double g, double* Ug) {
-    const double rho = Ui[0];
-    const double u = Ui[1] / rho, v = Ui[2] / rho;
-    const double p = pressure(Ui, g);
+template <typename T>
+__device__ __forceinline__ void ghost_phys(const T* Ui, T nx, T ny, int bct,
+                                           const T* __restrict__ bcd, T g, T* Ug) {
+    const T rho = Ui[0];
+    const T u = div_any(Ui[1], rho), v = div_any(Ui[2], rho);
+    const T p = pressure(Ui, g);
     switch (bct) {
         case ZJ_BC_WALL: {
-            const double Tw = bcd[0];
-            prim2cons(rho, -u, -v, (Tw > 0) ? rho * Tw : p, g, Ug);
+            const T Tw = bcd[0];
+            prim2cons(rho, -u, -v, (Tw > T(0)) ? rho * Tw : p, g, Ug);
             break;
         }
         case ZJ_BC_SLIPWALL: case ZJ_BC_SYMMETRY: {
-            const double vn = u * nx + v * ny;
-            prim2cons(rho, u - 2.0 * vn * nx, v - 2.0 * vn * ny, p, g, Ug);
+            const T vn = u * nx + v * ny;
+            prim2cons(rho, u - T(2) * vn * nx, v - T(2) * vn * ny, p, g, Ug);
             break;
         }
         case ZJ_BC_FARFIELD: {
-            const double r_inf = bcd[0], u_inf = bcd[1], v_inf = bcd[2], p_inf = bcd[3];
-            double Uinf[4];
+            const T r_inf = bcd[0], u_inf = bcd[1], v_inf = bcd[2], p_inf = bcd[3];
+            T Uinf[4];
             prim2cons(r_inf, u_inf, v_inf, p_inf, g, Uinf);
-            const double c_inf = sound_speed(pressure(Uinf, g), Uinf[0], g);
-            const double c_i = sound_speed(p, rho, g);
-            const double vn_i = u * nx + v * ny, vn_inf = u_inf * nx + v_inf * ny;
-            const double Rp = vn_i + 2.0 * c_i / (g - 1.0), Rm = vn_inf - 2.0 * c_inf / (g - 1.0);
-            const double vn_b = 0.5 * (Rp + Rm), c_b = 0.25 * (g - 1.0) * (Rp - Rm);
-            const bool out = (vn_b >= 0);
-            const double vt = out ? (u * (-ny) + v * nx) : (u_inf * (-ny) + v_inf * nx);
-            const double s = out ? p / pow(rho, g) : p_inf / pow(r_inf, g);
-            const double rb = pow(c_b * c_b / (g * s), 1.0 / (g - 1.0));
-            const double pb = rb * c_b * c_b / g;
+            const T c_inf = sound_speed(pressure(Uinf, g), Uinf[0], g);
+            const T c_i = sound_speed(p, rho, g);
+            const T vn_i = u * nx + v * ny, vn_inf = u_inf * nx + v_inf * ny;
+            const T Rp = vn_i + div_any(T(2) * c_i, g - T(1)), Rm = vn_inf - div_any(T(2) * c_inf, g - T(1));
+            const T vn_b = T(0.5) * (Rp + Rm), c_b = T(0.25) * (g - T(1)) * (Rp - Rm);
+            const bool out = (vn_b >= T(0));
+            const T vt = out ? (u * (-ny) + v * nx) : (u_inf * (-ny) + v_inf * nx);
+            const T s = out ? div_any(p, pow_any(rho, g)) : div_any(p_inf, pow_any(r_inf, g));
+            const T rb = pow_any(div_any(c_b * c_b, g * s), div_any(T(1), g - T(1)));
+            const T pb = div_any(rb * c_b * c_b, g);
             prim2cons(rb, vn_b * nx - vt * ny, vn_b * ny + vt * nx, pb, g, Ug);
             break;
         }
         case ZJ_BC_INFLOW: {
-            const double pt = bcd[0], Tt = bcd[1], dx = bcd[2], dy = bcd[3];
-            double M2 = 2.0 / (g - 1.0) * (pow(p / pt, -(g - 1.0) / g) - 1.0);
-            M2 = fmax(M2, 0.0);
-            const double Mn = sqrt(M2);
-            const double T = Tt / (1.0 + 0.5 * (g - 1.0) * M2);
-            const double rb = p / T;
-            const double vel = Mn * sqrt(g * p / rb);
+            const T pt = bcd[0], Tt = bcd[1], dx = bcd[2], dy = bcd[3];
+            T M2 = div_any(T(2), g - T(1)) * (pow_any(div_any(p, pt), div_any(-(g - T(1)), g)) - T(1));
+            M2 = max_any(M2, T(0));
+            const T Mn = sqrt(M2);
+            const T Tb = div_any(Tt, T(1) + T(0.5) * (g - T(1)) * M2);
+            const T rb = div_any(p, Tb);
+            const T vel = Mn * sqrt(div_any(g * p, rb));
             prim2cons(rb, vel * dx, vel * dy, p, g, Ug);
             break;
         }
@@ -225,25 +230,25 @@ __device__ __forceinline__ void ghost_phys(const double* Ui, double nx, double n
 // (kernels.cu:742-786): velocity and temperature gradients from the
 // conservative gradients dx = dU/dx, dy = dU/dy; mu = T^0.7/Re,
 // k = mu gamma / ((gamma-1) Pr); Stokes hypothesis.
-__device__ __forceinline__ void viscous_flux(const double* s, const double* dx, const double* dy,
-                                             double g, double Re, double Pr, double* Fv,
-                                             double* Gv) {
-    const double ir = rcp_any(s[0]);
-    const double u = s[1] * ir, v = s[2] * ir;
-    const double dudx = (dx[1] - u * dx[0]) * ir, dudy = (dy[1] - u * dy[0]) * ir;
-    const double dvdx = (dx[2] - v * dx[0]) * ir, dvdy = (dy[2] - v * dy[0]) * ir;
-    const double p = (g - 1.0) * s[0] * (s[3] * ir - 0.5 * (u * u + v * v));
-    const double T = p * ir;
-    const double dpdx = (g - 1.0) * (dx[3] - 0.5 * dx[0] * (u * u + v * v) - s[0] * (u * dudx + v * dvdx));
-    const double dpdy = (g - 1.0) * (dy[3] - 0.5 * dy[0] * (u * u + v * v) - s[0] * (u * dudy + v * dvdy));
-    const double dTdx = (dpdx - T * dx[0]) * ir, dTdy = (dpdy - T * dy[0]) * ir;
-    const double mu = pow(T, 0.7) / Re;
-    const double k = mu * g / ((g - 1.0) * Pr);
-    const double div = dudx + dvdy, lam = -2.0 / 3.0 * mu;
-    const double txx = 2.0 * mu * dudx + lam * div, tyy = 2.0 * mu * dvdy + lam * div;
-    const double txy = mu * (dudy + dvdx);
-    Fv[0] = 0.0; Fv[1] = txx; Fv[2] = txy; Fv[3] = u * txx + v * txy + k * dTdx;
-    Gv[0] = 0.0; Gv[1] = txy; Gv[2] = tyy; Gv[3] = u * txy + v * tyy + k * dTdy;
+template <typename T>
+__device__ __forceinline__ void viscous_flux(const T* s, const T* dx, const T* dy, T g, T Re,
+                                             T Pr, T* Fv, T* Gv) {
+    const T ir = rcp_any(s[0]);
+    const T u = s[1] * ir, v = s[2] * ir;
+    const T dudx = (dx[1] - u * dx[0]) * ir, dudy = (dy[1] - u * dy[0]) * ir;
+    const T dvdx = (dx[2] - v * dx[0]) * ir, dvdy = (dy[2] - v * dy[0]) * ir;
+    const T p = (g - T(1)) * s[0] * (s[3] * ir - T(0.5) * (u * u + v * v));
+    const T Tm = p * ir;
+    const T dpdx = (g - T(1)) * (dx[3] - T(0.5) * dx[0] * (u * u + v * v) - s[0] * (u * dudx + v * dvdx));
+    const T dpdy = (g - T(1)) * (dy[3] - T(0.5) * dy[0] * (u * u + v * v) - s[0] * (u * dudy + v * dvdy));
+    const T dTdx = (dpdx - Tm * dx[0]) * ir, dTdy = (dpdy - Tm * dy[0]) * ir;
+    const T mu = div_any(pow_any(Tm, T(0.7)), Re);
+    const T k = div_any(mu * g, (g - T(1)) * Pr);
+    const T div = dudx + dvdy, lam = T(-2.0 / 3.0) * mu;
+    const T txx = T(2) * mu * dudx + lam * div, tyy = T(2) * mu * dvdy + lam * div;
+    const T txy = mu * (dudy + dvdx);
+    Fv[0] = T(0); Fv[1] = txx; Fv[2] = txy; Fv[3] = u * txx + v * txy + k * dTdx;
+    Gv[0] = T(0); Gv[1] = txy; Gv[2] = tyy; Gv[3] = u * txy + v * tyy + k * dTdy;
 }
 
 }  // namespace phys
