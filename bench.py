@@ -5,17 +5,25 @@
 Workload: the Taylor-Green configuration -- 256x256 jittered (seed 1,
 +-0.15h) Q1 quads on [0,pi]^2 with slip walls, P3 (65 536 elements, 1 048 576
 DOF per variable), u = sin x cos y, v = -cos x sin y, M = 0.3, compressible
-Navier-Stokes with Re = 5000, Pr = 0.72, Roe flux, HU correction, FP64.  One
-bench step = one SSP-RK3 time step = three residual evaluations over the whole
-mesh; DOF-RHS/s = E * n_sp * 3 * K / t.  The same mesh and state in the
-reference's residual semantics (compat: Rusanov, inviscid, clamps) is timed
-as a second line of the JSON ("compat").
+Navier-Stokes with Re = 5000, Pr = 0.72, Roe flux, HU correction.  One bench
+step = one SSP-RK3 time step = three residual evaluations over the whole
+mesh; DOF-RHS/s = E * n_sp * 3 * K / t.
+
+The headline `value` is the precision form (FP32 volume, face, gradient and
+operator work; FP64 state, RK accumulation and reductions); the same case in
+FP64 is the `fp64` object with `speedup_vs_fp64`; `precision_errors` gives
+the L2 / Linf error of rho, rho u, rho v, rho E after 1000 steps at CFL 0.5
+against the FP64 path (which matches the FP64 oracle to 1e-12 per residual)
+with the FP64 conditioning floor beside it.  The same mesh and state in the
+reference's residual semantics (compat: Rusanov, inviscid, clamps, FP64) is
+the `compat` object.
 
 ours:      the CUDA path, timed with CUDA events on the solver's stream, max
            over ranks; N > 1 runs one independent replica per GPU (the path
            has no exchange on one GPU; weak scaling).
 reference: the oracle (the CPU restatement of the residual; the reference has
-           no CPU path) on the same workload with every host thread, rank 0.
+           no CPU path) on the same workload, FP64, with every host thread,
+           rank 0.
 """
 from __future__ import annotations
 
@@ -232,7 +240,7 @@ def run_reference(args):
             "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
 
 
-KERNELS = {"ns": "k_ns_grad<3> + k_ns_stage<3,Roe> (one residual)",
+KERNELS = {"ns": "k_ns_grad<3,double> + k_ns_stage<3,Roe,double> (one residual)",
            "ns32": "k_ns_grad<3,float> + k_ns_stage<3,Roe,float> (one residual)",
            "compat": "k_compat_stage<3>"}
 LAUNCHES_PER_RHS = {"ns": 2, "ns32": 2, "compat": 1}
@@ -294,13 +302,14 @@ def run_ours(args):
                 "frac": achieved / peak, "traffic": traffic_from_profile(f"{mode}|tgv{NX}"),
                 "peak_kind": peak_kind, "kernel": KERNELS[mode],
                 "algorithmic_bytes_per_launch": nbytes,
+                "algorithmic_bytes_per_element": mode_bytes_per_element(mode),
                 "launches_per_residual": LAUNCHES_PER_RHS[mode]}
         return s, U0, dof, ms, roof
 
-    s, U0, dof, ms, roofline = timed("ns")
+    head = "ns32"
+    s, U0, dof, ms, roofline = timed(head)
     value = world * dof * 3 * args.steps / (ms * 1e-3)
-    launches = 3 * args.steps * LAUNCHES_PER_RHS["ns"]
-    clocks = sampler.stop()
+    launches = 3 * args.steps * LAUNCHES_PER_RHS[head]
 
     # end to end through the C-ABI with host buffers: per step the state goes
     # H2D from pinned memory, one SSP-RK3 step, the new state comes back D2H
@@ -324,30 +333,69 @@ def run_ours(args):
            "steps": n_e2e}
     s.close()
 
+    s64, _, _, ms64, roof64 = timed("ns")
+    s64.close()
+    fp64 = {"workload": workload_name("ns") + ", FP64", "value": world * dof * 3 * args.steps / (ms64 * 1e-3),
+            "ms_per_step": ms64 / args.steps, "roofline": roof64,
+            "gpu_launches": 3 * args.steps * LAUNCHES_PER_RHS["ns"]}
+    clocks = sampler.stop()
+
     sc, _, dofc, msc, roofc = timed("compat")
     sc.close()
     compat = {"workload": workload_name("compat"), "value": world * dofc * 3 * args.steps / (msc * 1e-3),
               "ms_per_step": msc / args.steps, "roofline": roofc,
               "gpu_launches": 3 * args.steps}
 
+    precision = precision_errors(mesh, stream) if not args.no_error_run else None
+
     out = None
     if rank == 0:
         out = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
                "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
                "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-               "dtype": "f64", "data": "synthetic",
-               "config": {"workload": workload_name("ns"), "elements": mesh.n_elem,
-                          "dof_per_var": dof, "rhs_per_step": 3, "mode": "ns",
-                          "precision": "fp64", "dt": DT,
+               "dtype": "f32", "data": "synthetic",
+               "config": {"workload": workload_name("ns") + ", precision form", "elements": mesh.n_elem,
+                          "dof_per_var": dof, "rhs_per_step": 3, "mode": head,
+                          "precision": "mixed: FP32 volume/face/gradient/operator work; FP64 state, "
+                                       "SSP-RK3 accumulation, norm reductions, metrics built in FP64",
+                          "dt": DT,
                           "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
                           "l2": "no flush: each stage streams > 200 MB > 126 MB L2"},
                "roofline": roofline, "e2e": e2e, "gpu_launches": launches, "clocks": clocks,
-               "compat": compat}
+               "fp64": fp64, "speedup_vs_fp64": value / fp64["value"],
+               "precision_errors": precision, "compat": compat}
         if world == 1 and not args.no_cpu_baseline:
             out["cpu_baseline"] = cpu_baseline(mesh, args.cpu_seconds, "ns")
     if world > 1:
         dist.destroy_process_group()
     return out
+
+
+def precision_errors(mesh, stream, steps=1000):
+    """L2 / Linf error of the precision form against the FP64 path after
+    `steps` SSP-RK3 steps at CFL 0.5 from the Taylor-Green state (the FP64 GPU
+    path matches the FP64 oracle to 1e-12 per residual, tests/), with the FP64
+    conditioning floor: the FP64 path from the initial state rounded once to
+    FP32."""
+    from zhijian_b200 import meshgen as M
+    from zhijian_b200.norms import state_errors
+    s64, s32, sfl = make_solver(mesh, "ns"), make_solver(mesh, "ns32"), make_solver(mesh, "ns")
+    U0 = M.taylor_green(s64.solution_point_coords())
+    s64.copyToDevice(U0)
+    dt = s64.computeTimeStep()
+    for s, U in ((s64, U0), (s32, U0), (sfl, U0.astype(np.float32).astype(np.float64))):
+        s.set_stream(stream.cuda_stream)
+        s.copyToDevice(U)
+        s.advance(dt, steps)
+    U64, U32, Ufl = s64.copyToHost(), s32.copyToHost(), sfl.copyToHost()
+    for s in (s64, s32, sfl):
+        s.close()
+    e, fl = state_errors(U32, U64), state_errors(Ufl, U64)
+    return {"steps": steps, "dt": dt, "cfl": 0.5, "vars": ["rho", "rhou", "rhov", "rhoE"],
+            "against": "FP64 GPU path (= FP64 oracle to 1e-12 per residual)",
+            "l2": e["l2"], "linf": e["linf"], "l2_abs": e["l2_abs"], "linf_abs": e["linf_abs"],
+            "fp64_floor_l2": fl["l2"],
+            "fp64_floor": "FP64 run from the initial state rounded once to FP32"}
 
 
 def main():
@@ -358,6 +406,7 @@ def main():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
+    ap.add_argument("--no-error-run", action="store_true")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

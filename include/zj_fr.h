@@ -195,6 +195,40 @@ void* zj_get_stream(const zj_solver* s);
 #define ZJ_NOALLOC_SCRATCH_BYTES (32u * 1024u * 1024u)
 zj_status zj_rhs_noalloc(zj_solver* s, const double* U_dev, double* R_dev);
 
+/* ---- differentiation (physics mode, FP64) ----------------------------------
+ * No reference counterpart: the reference has no adjoint.  All pointers are
+ * device pointers to [E][n_sp][4] FP64 arrays, 16-byte aligned; the calls are
+ * asynchronous on the handle's stream.  Compat mode and the mixed-precision
+ * form return ZJ_ERR_UNSUPPORTED. */
+
+/* Jacobian-vector product: R_dev = R(U), JV_dev = dR/dU . V + dR/dRe * dRe
+ * (forward mode on dual numbers; exact to FP64 rounding).  R_dev may be NULL. */
+zj_status zj_rhs_jvp(zj_solver* s, const double* U_dev, const double* V_dev, double dRe,
+                     double* R_dev, double* JV_dev);
+
+/* Vector-Jacobian product: W_dev = (dR/dU)^T L_dev (hand-written transposed
+ * kernels).  If dRe_out is not NULL it receives L . dR/dRe (one extra dual
+ * launch). */
+zj_status zj_rhs_vjp(zj_solver* s, const double* U_dev, const double* L_dev, double* W_dev,
+                     double* dRe_out);
+
+/* Adjoint of one SSP-RK3 step of size dt taken from U_dev: given B_dev =
+ * dJ/dU(n+1), writes dJ/dU(n) into A_dev (may alias B_dev) and adds
+ * dJ/dRe contributions into *dRe_acc if it is not NULL.  The stage states
+ * are recomputed from U_dev. */
+zj_status zj_step_vjp(zj_solver* s, const double* U_dev, double dt, const double* B_dev,
+                      double* A_dev, double* dRe_acc);
+
+/* Discrete adjoint of nsteps SSP-RK3 steps of size dt from the handle's
+ * current state (which is left unchanged): checkpoints every k_ckpt steps
+ * on the device, segment recomputation, step adjoints backwards.
+ * G_dev holds dJ/dU(final) on entry and dJ/dU(initial) on return.  Optional
+ * outputs: *dRe = dJ/dRe, *bytes = device bytes the checkpoints and segment
+ * states took, *ms_forward / *ms_adjoint = device times of the checkpointed
+ * forward sweep and of the backward sweep (CUDA events). */
+zj_status zj_adjoint_run(zj_solver* s, double dt, int nsteps, int k_ckpt, double* G_dev,
+                         double* dRe, int64_t* bytes, double* ms_forward, double* ms_adjoint);
+
 /* ---- config-file convenience: parse + mesh from a Gmsh file ---------------- */
 /* Read an ASCII Gmsh MSH v2.2 / v4.1 quad mesh (src/mesh/gmsh_reader.cpp:161)
  * and create a solver.  Physical names map to boundary types as

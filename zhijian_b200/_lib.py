@@ -92,6 +92,10 @@ def lib():
         "zj_iteration": (ip, [vp]),
         "zj_set_stream": (ip, [vp, vp]),
         "zj_get_stream": (vp, [vp]),
+        "zj_rhs_jvp": (ip, [vp, vp, vp, C.c_double, vp, vp]),
+        "zj_rhs_vjp": (ip, [vp, vp, vp, vp, dp]),
+        "zj_step_vjp": (ip, [vp, vp, C.c_double, vp, vp, dp]),
+        "zj_adjoint_run": (ip, [vp, C.c_double, ip, ip, vp, dp, C.POINTER(C.c_int64), dp, dp]),
     }
     for name, (res, args) in sig.items():
         f = getattr(h, name)

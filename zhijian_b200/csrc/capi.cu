@@ -60,6 +60,33 @@ struct zj_solver {
     float* fOps = nullptr;
     float* fBC = nullptr;
     float4* fNrm = nullptr;
+    // differentiation: dual-number geometry and traces (Jacobian-vector
+    // products) and adjoint scratch, allocated on first use
+    size_t n_jinv = 0, n_j = 0, n_ops = 0, n_bcd = 0, n_nrm = 0;
+    bool diff_ready = false;
+    Dual* xJinv = nullptr;
+    Dual* xJ = nullptr;
+    Dual* xOps = nullptr;
+    Dual* xBC = nullptr;
+    Dual4* xNrm = nullptr;
+    Dual* xT = nullptr;
+    Dual* xTQ = nullptr;
+    double* xPart = nullptr;
+    double* aDb = nullptr;      // dFbar per flux point
+    double* aTb = nullptr;      // trace adjoint (NS)
+    double* aDUb = nullptr;     // gradient-jump adjoint (NS)
+    double* aW = nullptr;       // VJP output scratch
+    double* aS1 = nullptr;      // stage states U(1), U(2)
+    double* aS2 = nullptr;
+    double* aB0 = nullptr;      // stage adjoints
+    double* aB1 = nullptr;
+    double* aB2 = nullptr;
+    double* aR = nullptr;       // residual scratch of a JVP
+    double* aJV = nullptr;      // dR/dRe
+    double* aZero = nullptr;    // zero tangent
+    double* aDot = nullptr;     // dot-product partials
+    double* aScal = nullptr;    // [0] dJ/dRe accumulator, [1] dot result
+    double* aRePart = nullptr;  // per-CTA L . dR/dRe of the NS VJP
     int grid = 0;
     int cur = 0, tpar = 0;
     bool traces_valid = false;
@@ -109,6 +136,11 @@ void free_all(zj_solver* s) {
     for (auto pp : fs) { if (*pp) cudaFree(*pp); *pp = nullptr; }
     if (s->fNrm) cudaFree(s->fNrm);
     s->fNrm = nullptr;
+    void* xs[] = {s->xJinv, s->xJ, s->xOps, s->xBC, s->xNrm, s->xT, s->xTQ, s->xPart, s->aDb, s->aTb,
+                  s->aDUb, s->aW, s->aS1, s->aS2, s->aB0, s->aB1, s->aB2, s->aR, s->aJV, s->aZero,
+                  s->aDot, s->aScal, s->aRePart};
+    for (void* p : xs) if (p) cudaFree(p);
+    s->diff_ready = false;
     if (s->dFlag) cudaFree(s->dFlag);
     if (s->dEdges) cudaFree(s->dEdges);
     if (s->dNrm) cudaFree(s->dNrm);
@@ -288,6 +320,8 @@ zj_status zj_solver_create(const zj_mesh_desc* mesh, const zj_params* params, zj
     for (auto& a : area) a = std::sqrt(a);
     pack_ops(s->ops, packed);
 
+    s->n_jinv = Jinv.size(); s->n_j = J.size(); s->n_ops = packed.size();
+    s->n_bcd = bc.size(); s->n_nrm = rec.size();
     s->state_n = (size_t)s->E * s->nsp * 4;
     // element traces, then one ghost row per boundary slot (physics mode)
     s->trace_n = ((size_t)s->E * 4 + (size_t)s->mesh.n_bnd_faces) * s->n1 * 4;
@@ -561,6 +595,355 @@ zj_status zj_rhs_noalloc(zj_solver* s, const double* U_dev, double* R_dev) {
     }
     double* traces = scratch;
     return rhs_impl<double>(s, U_dev, R_dev, traces, is_ns(s) ? traces + s->trace_n : nullptr, partials);
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Differentiation (physics mode, FP64): Jacobian-vector products on dual
+// numbers (jvp.cu), vector-Jacobian products by the transposed kernels
+// (adjoint.cu), the adjoint of an SSP-RK3 step and the checkpointed discrete
+// adjoint of a run.
+namespace {
+
+zj_status diff_supported(zj_solver* s) {
+    if (s->prm.compat) return fail(s, ZJ_ERR_UNSUPPORTED, "differentiation needs physics mode (compat off)");
+    if (s->mixed) return fail(s, ZJ_ERR_UNSUPPORTED, "differentiation runs on the FP64 path (precision fp64)");
+    return ZJ_OK;
+}
+
+bool misaligned(const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15u) != 0; }
+
+zj_status ensure_diff(zj_solver* s) {
+    if (s->diff_ready) return ZJ_OK;
+    cudaError_t e = cudaSuccess;
+#define ZJ_ALLOC(ptr, n) \
+    if (e == cudaSuccess) e = dalloc(&(ptr), (n));
+    ZJ_ALLOC(s->xJinv, s->n_jinv);
+    ZJ_ALLOC(s->xJ, s->n_j);
+    ZJ_ALLOC(s->xOps, s->n_ops);
+    ZJ_ALLOC(s->xBC, s->n_bcd);
+    ZJ_ALLOC(s->xNrm, s->n_nrm);
+    ZJ_ALLOC(s->xT, s->trace_n);
+    ZJ_ALLOC(s->xTQ, 2 * s->trace_n);
+    ZJ_ALLOC(s->xPart, (size_t)dual_grid(s->P, s->E));
+    const size_t fpn = (size_t)s->E * 4 * s->n1 * 4;
+    ZJ_ALLOC(s->aDb, fpn);
+    ZJ_ALLOC(s->aTb, fpn);
+    ZJ_ALLOC(s->aDUb, fpn);
+    double** st[] = {&s->aW, &s->aS1, &s->aS2, &s->aB0, &s->aB1, &s->aB2, &s->aR, &s->aJV, &s->aZero};
+    for (auto pp : st) { ZJ_ALLOC(*pp, s->state_n); }
+    ZJ_ALLOC(s->aDot, (size_t)dot_grid());
+    ZJ_ALLOC(s->aScal, 8);
+    ZJ_ALLOC(s->aRePart, (size_t)adj_ns_grid(s->P, s->E));
+#undef ZJ_ALLOC
+    if (e == cudaSuccess) e = launch_to_dual(s->dJinv, s->xJinv, (long long)s->n_jinv, s->stream);
+    if (e == cudaSuccess) e = launch_to_dual(s->dJ, s->xJ, (long long)s->n_j, s->stream);
+    if (e == cudaSuccess) e = launch_to_dual(s->dOps, s->xOps, (long long)s->n_ops, s->stream);
+    if (e == cudaSuccess) e = launch_to_dual(s->dBC, s->xBC, (long long)s->n_bcd, s->stream);
+    if (e == cudaSuccess)
+        e = launch_to_dual(reinterpret_cast<const double*>(s->dNrm), reinterpret_cast<Dual*>(s->xNrm),
+                           (long long)s->n_nrm * 4, s->stream);
+    if (e == cudaSuccess) e = cudaMemsetAsync(s->aZero, 0, s->state_n * 8, s->stream);
+    if (e == cudaSuccess) e = cudaMemsetAsync(s->aScal, 0, 8 * 8, s->stream);
+    if (e != cudaSuccess) return cuda_fail(s, e, "differentiation buffers");
+    s->diff_ready = true;
+    return ZJ_OK;
+}
+
+// R (if R != NULL) and JV = dR/dU . V + dR/dRe dRe.
+zj_status jvp_core(zj_solver* s, const double* U, const double* V, double dRe, double* R, double* JV) {
+    StageArgsT<Dual> a{};
+    a.Jinv = s->xJinv; a.J = s->xJ; a.enrm = s->xNrm; a.bc = s->xBC; a.ops = s->xOps;
+    a.edges = s->dEdges; a.dt = s->dScal; a.n_elem = s->E; a.gamma = s->prm.gamma;
+    a.Re = s->prm.Re; a.Pr = s->prm.Pr; a.dRe = dRe;
+    a.U = U; a.U0 = U; a.dU = V; a.Tout = s->xT;
+    ZJ_CK(s, launch_phys_traces(s->P, a, s->stream), "jvp trace launch");
+    a.Tin = s->xT; a.TQ = s->xTQ; a.TQout = s->xTQ;
+    a.R = R ? R : s->aR; a.dR = JV; a.partials = s->xPart; a.stage = 0;
+    if (is_ns(s)) {
+        ZJ_CK(s, launch_ns_grad(s->P, a, s->stream), "jvp gradient launch");
+        ZJ_CK(s, launch_ns_stage(s->P, s->prm.riemann, a, s->stream), "jvp residual launch");
+    } else {
+        ZJ_CK(s, launch_phys_stage(s->P, s->prm.riemann, a, s->stream), "jvp residual launch");
+    }
+    return ZJ_OK;
+}
+
+// Fused output of a VJP: out = c0 X0 + c1 X1 + c2 X2 + cw (dR/dU)^T L.
+struct VjpOut {
+    double* out = nullptr;
+    const double* X0 = nullptr;
+    const double* X1 = nullptr;
+    const double* X2 = nullptr;
+    double c0 = 0.0, c1 = 0.0, c2 = 0.0, cw = 1.0;
+};
+
+// W = (dR/dU)^T L (or the fused update o); for Navier-Stokes with
+// re_weight != 0 also aScal[0] += re_weight * L . dR/dRe (reduced from the
+// VJP's per-CTA sums).
+zj_status vjp_core(zj_solver* s, const double* U, const double* L, double* W, double re_weight = 0.0,
+                   const VjpOut& o = VjpOut(), const double* T = nullptr, const double* TQ = nullptr) {
+    if (!T) {
+        // traces and gradient traces of U, unless the caller kept them from
+        // the forward recomputation
+        ZJ_CK(s, launch_trace_any(s, U, s->dT[2]), "vjp trace launch");
+        T = s->dT[2];
+        if (is_ns(s)) {
+            StageArgs a = stage_args<double>(s);
+            a.U = U; a.Tin = T; a.TQout = s->dTQ;
+            ZJ_CK(s, launch_ns_grad(s->P, a, s->stream), "vjp gradient launch");
+            TQ = s->dTQ;
+        }
+    }
+    AdjArgs g{};
+    g.U = U; g.L = L; g.W = W; g.T = T; g.TQ = TQ;
+    g.Db = s->aDb; g.Tb = s->aTb; g.DUb = s->aDUb;
+    g.Jinv = s->dJinv; g.J = s->dJ; g.edges = s->dEdges; g.enrm = s->dNrm; g.bc = s->dBC; g.ops = s->dOps;
+    g.n_elem = s->E; g.gamma = s->prm.gamma; g.Re = s->prm.Re; g.Pr = s->prm.Pr;
+    const bool re = is_ns(s) && re_weight != 0.0;
+    g.re_part = re ? s->aRePart : nullptr;
+    g.out = o.out; g.X0 = o.X0; g.X1 = o.X1; g.X2 = o.X2;
+    g.c0 = o.c0; g.c1 = o.c1; g.c2 = o.c2; g.cw = o.cw;
+    ZJ_CK(s, launch_rhs_vjp(s->P, s->prm.riemann, is_ns(s), g, s->stream), "vjp launch");
+    if (re) {
+        ZJ_CK(s, launch_reduce_sum(s->aRePart, adj_ns_grid(s->P, s->E), s->aScal + 1, s->stream), "re reduce");
+        ZJ_CK(s, launch_lincomb(s->aScal, 1.0, s->aScal, re_weight, s->aScal + 1, 0.0, nullptr, 1, s->stream),
+              "re accumulate");
+    }
+    return ZJ_OK;
+}
+
+zj_status set_dt(zj_solver* s, double dt) {
+    if (dt != s->last_dt) {
+        ZJ_CK(s, cudaMemcpyAsync(s->dScal, &dt, sizeof(double), cudaMemcpyHostToDevice, s->stream), "dt upload");
+        ZJ_CK(s, cudaStreamSynchronize(s->stream), "dt upload sync");
+        s->last_dt = dt;
+    }
+    return ZJ_OK;
+}
+
+// Per-stage traces and gradient traces kept from a forward recomputation
+// (T[k], TQ[k] of stage input state k = X, U(1), U(2)); NULL entries mean
+// the handle's scratch buffers.
+struct StageTraces {
+    double* T[3] = {nullptr, nullptr, nullptr};
+    double* TQ[3] = {nullptr, nullptr, nullptr};
+};
+
+// Stage launches of one SSP-RK3 step from X (handle's stage machinery on
+// caller buffers): U(1) into S1, U(2) into S2 and, if Xout != NULL, the new
+// state into Xout (may be X).  Without keep, uses the stepper's trace
+// buffers; with keep, writes every stage input's traces and gradient traces
+// into keep's buffers (the third stage's gradient traces even when Xout is
+// NULL).
+zj_status rk3_stages(zj_solver* s, const double* X, double* S1, double* S2, double* Xout,
+                     const StageTraces* keep = nullptr) {
+    double* T[3] = {s->dT[0], s->dT[1], s->dT[0]};
+    double* TQ[3] = {s->dTQ, s->dTQ, s->dTQ};
+    if (keep)
+        for (int k = 0; k < 3; ++k) { T[k] = keep->T[k]; TQ[k] = keep->TQ[k]; }
+    ZJ_CK(s, launch_trace_any(s, X, T[0]), "trace launch");
+    StageArgs a = stage_args<double>(s);
+    a.partials = s->dPartR;
+    a.U = X; a.U0 = X; a.Uout = S1; a.Tin = T[0]; a.Tout = T[1]; a.TQ = a.TQout = TQ[0]; a.stage = 1;
+    ZJ_CK(s, launch_stage(s, a), "stage 1 launch");
+    a.U = S1; a.Uout = S2; a.Tin = T[1]; a.Tout = T[2]; a.TQ = a.TQout = TQ[1]; a.stage = 2;
+    ZJ_CK(s, launch_stage(s, a), "stage 2 launch");
+    a.U = S2; a.Tin = T[2]; a.TQ = a.TQout = TQ[2];
+    if (Xout) {
+        a.Uout = Xout; a.Tout = s->dT[1]; a.stage = 3;
+        ZJ_CK(s, launch_stage(s, a), "stage 3 launch");
+    } else if (keep && is_ns(s)) {
+        ZJ_CK(s, launch_ns_grad(s->P, a, s->stream), "gradient launch");
+    }
+    s->traces_valid = false;   // the stepper's traces now hold this step's
+    return ZJ_OK;
+}
+
+// Adjoint of one SSP-RK3 step from U0 (dt already on the device):
+//   U1 = U0 + dt R(U0), U2 = 3/4 U0 + 1/4 U1 + 1/4 dt R(U1),
+//   U3 = 1/3 U0 + 2/3 U2 + 2/3 dt R(U2);
+// B = dJ/dU3 in, A = dJ/dU0 out (A may alias B).  S1, S2: the stage states
+// if the caller kept them, else NULL (recomputed here).  With re, w dt times
+// each stage's L . dR/dRe is added to aScal[0].
+zj_status step_vjp_core(zj_solver* s, const double* U0, const double* S1, const double* S2, double dt,
+                        const double* B, double* A, bool re, const StageTraces* kept = nullptr) {
+    zj_status st = ZJ_OK;
+    if (!S1) {
+        if ((st = rk3_stages(s, U0, s->aS1, s->aS2, nullptr)) != ZJ_OK) return st;
+        S1 = s->aS1;
+        S2 = s->aS2;
+    }
+    const double* T[3] = {nullptr, nullptr, nullptr};
+    const double* TQ[3] = {nullptr, nullptr, nullptr};
+    if (kept)
+        for (int k = 0; k < 3; ++k) { T[k] = kept->T[k]; TQ[k] = kept->TQ[k]; }
+    // stage 3: B2 = 2/3 B + 2/3 dt (dR/dU(U2))^T B
+    VjpOut o3;
+    o3.out = s->aB2; o3.X0 = B; o3.c0 = 2.0 / 3.0; o3.cw = 2.0 / 3.0 * dt;
+    if ((st = vjp_core(s, S2, B, s->aW, re ? 2.0 / 3.0 * dt : 0.0, o3, T[2], TQ[2])) != ZJ_OK) return st;
+    // stage 2: B1 = 1/4 B2 + 1/4 dt (dR/dU(U1))^T B2
+    VjpOut o2;
+    o2.out = s->aB1; o2.X0 = s->aB2; o2.c0 = 0.25; o2.cw = 0.25 * dt;
+    if ((st = vjp_core(s, S1, s->aB2, s->aW, re ? 0.25 * dt : 0.0, o2, T[1], TQ[1])) != ZJ_OK) return st;
+    // stage 1: A = 1/3 B + 3/4 B2 + B1 + dt (dR/dU(U0))^T B1
+    VjpOut o1;
+    o1.out = A; o1.X0 = B; o1.c0 = 1.0 / 3.0; o1.X1 = s->aB2; o1.c1 = 0.75; o1.X2 = s->aB1; o1.c2 = 1.0;
+    o1.cw = dt;
+    if ((st = vjp_core(s, U0, s->aB1, s->aW, re ? dt : 0.0, o1, T[0], TQ[0])) != ZJ_OK) return st;
+    return ZJ_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+zj_status zj_rhs_jvp(zj_solver* s, const double* U_dev, const double* V_dev, double dRe,
+                     double* R_dev, double* JV_dev) {
+    if (!s || !U_dev || !V_dev || !JV_dev) return ZJ_ERR_ARG;
+    if (misaligned(U_dev) || misaligned(V_dev) || misaligned(JV_dev) || (R_dev && misaligned(R_dev)))
+        return fail(s, ZJ_ERR_ARG, "device arrays must be 16-byte aligned");
+    zj_status st = diff_supported(s);
+    if (st == ZJ_OK) st = ensure_diff(s);
+    if (st == ZJ_OK) st = jvp_core(s, U_dev, V_dev, dRe, R_dev, JV_dev);
+    return st;
+}
+
+zj_status zj_rhs_vjp(zj_solver* s, const double* U_dev, const double* L_dev, double* W_dev,
+                     double* dRe_out) {
+    if (!s || !U_dev || !L_dev || !W_dev) return ZJ_ERR_ARG;
+    if (misaligned(U_dev) || misaligned(L_dev) || misaligned(W_dev))
+        return fail(s, ZJ_ERR_ARG, "device arrays must be 16-byte aligned");
+    zj_status st = diff_supported(s);
+    if (st == ZJ_OK) st = ensure_diff(s);
+    if (st != ZJ_OK) return st;
+    if (dRe_out) ZJ_CK(s, cudaMemsetAsync(s->aScal, 0, sizeof(double), s->stream), "clear");
+    if ((st = vjp_core(s, U_dev, L_dev, W_dev, dRe_out ? 1.0 : 0.0)) != ZJ_OK || !dRe_out) return st;
+    ZJ_CK(s, cudaMemcpyAsync(dRe_out, s->aScal, sizeof(double), cudaMemcpyDeviceToHost, s->stream), "dRe copy");
+    ZJ_CK(s, cudaStreamSynchronize(s->stream), "vjp sync");
+    return ZJ_OK;
+}
+
+zj_status zj_step_vjp(zj_solver* s, const double* U_dev, double dt, const double* B_dev,
+                      double* A_dev, double* dRe_acc) {
+    if (!s || !U_dev || !B_dev || !A_dev) return ZJ_ERR_ARG;
+    if (!std::isfinite(dt)) return fail(s, ZJ_ERR_ARG, "bad dt");
+    zj_status st = diff_supported(s);
+    if (st == ZJ_OK) st = ensure_diff(s);
+    if (st == ZJ_OK) st = set_dt(s, dt);
+    if (st != ZJ_OK) return st;
+    if (dRe_acc) ZJ_CK(s, cudaMemsetAsync(s->aScal, 0, sizeof(double), s->stream), "clear");
+    if ((st = step_vjp_core(s, U_dev, nullptr, nullptr, dt, B_dev, A_dev, dRe_acc != nullptr)) != ZJ_OK)
+        return st;
+    if (dRe_acc) {
+        double v = 0.0;
+        ZJ_CK(s, cudaMemcpyAsync(&v, s->aScal, sizeof(double), cudaMemcpyDeviceToHost, s->stream), "dRe copy");
+        ZJ_CK(s, cudaStreamSynchronize(s->stream), "step vjp sync");
+        *dRe_acc += v;
+    }
+    return ZJ_OK;
+}
+
+zj_status zj_adjoint_run(zj_solver* s, double dt, int nsteps, int k_ckpt, double* G_dev, double* dRe,
+                         int64_t* bytes, double* ms_forward, double* ms_adjoint) {
+    if (!s || !G_dev) return ZJ_ERR_ARG;
+    if (nsteps < 1 || k_ckpt < 1 || !std::isfinite(dt)) return fail(s, ZJ_ERR_ARG, "bad dt, nsteps or k_ckpt");
+    zj_status st = diff_supported(s);
+    if (st == ZJ_OK) st = ensure_diff(s);
+    if (st == ZJ_OK) st = set_dt(s, dt);
+    if (st != ZJ_OK) return st;
+    const int n_ck = (nsteps + k_ckpt - 1) / k_ckpt;
+    const int seg_n = std::min(k_ckpt, nsteps);
+    const size_t sb = s->state_n * sizeof(double);
+    double* ck = nullptr;    // checkpoints [n_ck][state]
+    double* seg = nullptr;   // step-start states of one segment [seg_n][state]
+    double* X = nullptr;     // forward work state
+    // per step of a segment: 3 states, and 3 trace sets (traces + gradient
+    // traces) of the stage inputs
+    const size_t tset = s->trace_n * (is_ns(s) ? 3 : 1);
+    double* trs = nullptr;
+    cudaError_t e = dalloc(&ck, (size_t)n_ck * s->state_n);
+    if (e == cudaSuccess) e = dalloc(&seg, (size_t)3 * seg_n * s->state_n);
+    if (e == cudaSuccess) e = dalloc(&trs, (size_t)3 * seg_n * tset);
+    if (e == cudaSuccess) e = dalloc(&X, s->state_n);
+    cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
+    for (int i = 0; i < 4 && e == cudaSuccess; ++i) e = cudaEventCreate(&ev[i]);
+    auto cleanup = [&]() {
+        for (auto x : ev) if (x) cudaEventDestroy(x);
+        if (ck) cudaFree(ck);
+        if (seg) cudaFree(seg);
+        if (trs) cudaFree(trs);
+        if (X) cudaFree(X);
+    };
+    if (e != cudaSuccess) { cleanup(); return cuda_fail(s, e, "adjoint checkpoint buffers"); }
+    const long long n = (long long)s->state_n;
+    auto run = [&]() -> zj_status {
+        zj_status r = ZJ_OK;
+        ZJ_CK(s, cudaMemsetAsync(s->aScal, 0, sizeof(double), s->stream), "clear");
+        ZJ_CK(s, cudaMemcpyAsync(X, s->dU[s->cur], sb, cudaMemcpyDeviceToDevice, s->stream), "state copy");
+        // forward sweep with checkpoints every k_ckpt steps
+        ZJ_CK(s, cudaEventRecord(ev[0], s->stream), "event");
+        for (int i = 0; i < nsteps; ++i) {
+            if (i % k_ckpt == 0)
+                ZJ_CK(s, cudaMemcpyAsync(ck + (size_t)(i / k_ckpt) * s->state_n, X, sb,
+                                         cudaMemcpyDeviceToDevice, s->stream), "checkpoint");
+            if ((r = rk3_stages(s, X, s->aS1, s->aS2, X)) != ZJ_OK) return r;
+        }
+        ZJ_CK(s, cudaEventRecord(ev[1], s->stream), "event");
+        // backward sweep: recompute each segment from its checkpoint, then
+        // the step adjoints in reverse
+        // segment layout: step m's start state, U(1), U(2) at seg + 3 m states
+        auto st_at = [&](int m, int which) { return seg + (size_t)(3 * m + which) * s->state_n; };
+        auto traces_at = [&](int m) {
+            StageTraces t;
+            for (int k = 0; k < 3; ++k) {
+                double* base = trs + (size_t)(3 * m + k) * tset;
+                t.T[k] = base;
+                t.TQ[k] = is_ns(s) ? base + s->trace_n : nullptr;
+            }
+            return t;
+        };
+        for (int c = n_ck - 1; c >= 0; --c) {
+            const int first = c * k_ckpt, len = std::min(k_ckpt, nsteps - first);
+            ZJ_CK(s, cudaMemcpyAsync(st_at(0, 0), ck + (size_t)c * s->state_n, sb, cudaMemcpyDeviceToDevice,
+                                     s->stream), "segment start");
+            for (int m = 0; m < len; ++m) {
+                const StageTraces t = traces_at(m);
+                if ((r = rk3_stages(s, st_at(m, 0), st_at(m, 1), st_at(m, 2),
+                                    (m + 1 < len) ? st_at(m + 1, 0) : nullptr, &t)) != ZJ_OK)
+                    return r;
+            }
+            for (int m = len - 1; m >= 0; --m) {
+                const StageTraces t = traces_at(m);
+                if ((r = step_vjp_core(s, st_at(m, 0), st_at(m, 1), st_at(m, 2), dt, G_dev, G_dev,
+                                       dRe != nullptr, &t)) != ZJ_OK)
+                    return r;
+            }
+        }
+        ZJ_CK(s, cudaEventRecord(ev[2], s->stream), "event");
+        (void)n;
+        return ZJ_OK;
+    };
+    st = run();
+    if (st == ZJ_OK) {
+        double v = 0.0;
+        e = cudaMemcpyAsync(&v, s->aScal, sizeof(double), cudaMemcpyDeviceToHost, s->stream);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(s->stream);
+        if (e != cudaSuccess) st = cuda_fail(s, e, "adjoint sync");
+        float f = 0.0f, b = 0.0f;
+        if (st == ZJ_OK) {
+            cudaEventElapsedTime(&f, ev[0], ev[1]);
+            cudaEventElapsedTime(&b, ev[1], ev[2]);
+            if (dRe) *dRe = v;
+            if (ms_forward) *ms_forward = f;
+            if (ms_adjoint) *ms_adjoint = b;
+            if (bytes)
+                *bytes = (int64_t)((size_t)(n_ck + 3 * seg_n + 1 + 9) * sb + (size_t)3 * seg_n * tset * 8);
+        }
+    }
+    cleanup();
+    return st;
 }
 
 zj_status zj_solver_create_from_gmsh(const char* msh_path, const zj_params* params, zj_solver** out) {

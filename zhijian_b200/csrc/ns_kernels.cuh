@@ -56,6 +56,7 @@ template <> struct NSMinBlocks<double> {
 template <> struct NSMinBlocks<float> {
     static constexpr int stage = ZJ_NS32_MIN_BLOCKS, grad = ZJ_NSG32_MIN_BLOCKS;
 };
+template <> struct NSMinBlocks<Dual> { static constexpr int stage = 1, grad = 1; };
 
 // Corrected gradient at solution point (i, j) of one element: su is the
 // element's state in the [var][row][col] shared layout, du its face jumps
@@ -118,9 +119,9 @@ __device__ __forceinline__ void load_face_point(const StageArgsT<T>& a, long lon
 }
 
 template <int P, typename T>
-__global__ void __launch_bounds__(Shape<P>::THREADS, NSMinBlocks<T>::grad)
+__global__ void __launch_bounds__(Shape<P, EbDiv<T>::value>::THREADS, NSMinBlocks<T>::grad)
 k_ns_grad(const StageArgsT<T> a) {
-    using S = Shape<P>;
+    using S = Shape<P, EbDiv<T>::value>;
     constexpr int N1 = S::N1, NSP = S::NSP, NFT = S::NFT, TPE = S::TPE, EB = S::EB;
     constexpr int RS = S::RS, VS = S::VS, FS = Tiles<P, T>::FS, DS = Tiles<P, T>::DS;
     constexpr int QS = Tiles<P, T>::QS;
@@ -151,7 +152,8 @@ k_ns_grad(const StageArgsT<T> a) {
             load_state(a.U + e * NSP * 4, ue);
             state_minus_ref(ud, ue, u);
         } else {
-            load_state(a.U + idx * 4, u);
+            double ud[4];
+            stage_state(a, idx, ud, u);
         }
         load4_nc(a.Jinv + idx * 4, ji);
         T* su = sU + el * FS + j * RS + i;
@@ -187,9 +189,9 @@ k_ns_grad(const StageArgsT<T> a) {
 }
 
 template <int P, int RIEM, typename T>
-__global__ void __launch_bounds__(Shape<P>::THREADS, NSMinBlocks<T>::stage)
+__global__ void __launch_bounds__(Shape<P, EbDiv<T>::value>::THREADS, NSMinBlocks<T>::stage)
 k_ns_stage(const StageArgsT<T> a) {
-    using S = Shape<P>;
+    using S = Shape<P, EbDiv<T>::value>;
     constexpr int N1 = S::N1, NSP = S::NSP, NFT = S::NFT, TPE = S::TPE, EB = S::EB;
     constexpr int RS = S::RS, VS = S::VS, FS = Tiles<P, T>::FS, DS = Tiles<P, T>::DS;
     __shared__ T sOps[S::NOPS];
@@ -205,7 +207,7 @@ k_ns_stage(const StageArgsT<T> a) {
     const long long e = (long long)blockIdx.x * EB + el;
     const bool valid = (el < EB) && (e < a.n_elem);
     const bool is_sp = valid && k < NSP, is_fp = valid && k < NFT;
-    const T g = T(a.gamma), Re = T(a.Re), Pr = T(a.Pr);
+    const T g = T(a.gamma), Re = reynolds(a), Pr = T(a.Pr);
     const int edge = k / N1, fp = k - edge * N1;
     const int i = k % N1, j = k / N1;
 
@@ -236,11 +238,9 @@ k_ns_stage(const StageArgsT<T> a) {
     if (is_sp) {
         const long long idx = e * NSP + k;
         double ud[4];
-        load4(a.U + idx * 4, ud);
-#pragma unroll
-        for (int v = 0; v < 4; ++v) u[v] = T(ud[v]);
+        stage_state(a, idx, ud, u);
         load4_nc(a.Jinv + idx * 4, ji);
-        Jd = __ldg(a.J + idx);
+        Jd = ldg_any(a.J + idx);
         if ((k & 3) == 0 && a.stage >= 2) prefetch_l2(a.U0 + idx * 4);
         T* su = sU + el * FS + j * RS + i;
         T w[4];
@@ -351,10 +351,7 @@ k_ns_stage(const StageArgsT<T> a) {
             res[v] = -(div + corr) * iJ;
         }
         if (a.stage == 0) {
-            double rd[4];
-#pragma unroll
-            for (int v = 0; v < 4; ++v) { rd[v] = double(res[v]); rsq += rd[v] * rd[v]; }
-            store4(a.R + idx * 4, rd);
+            store_residual(a, idx, res, rsq);
         } else {
             double us[4];
             if constexpr (sizeof(T) == 8) {
@@ -403,7 +400,7 @@ k_ns_stage(const StageArgsT<T> a) {
 
 template <int P, typename T>
 cudaError_t ns_grad_t(const StageArgsT<T>& a, cudaStream_t s) {
-    using S = Shape<P>;
+    using S = Shape<P, EbDiv<T>::value>;
     const long long grid = (a.n_elem + S::EB - 1) / S::EB;
     if (grid <= 0) return cudaSuccess;
     static bool set = false;
@@ -414,7 +411,7 @@ cudaError_t ns_grad_t(const StageArgsT<T>& a, cudaStream_t s) {
 
 template <int P, int RIEM, typename T>
 cudaError_t ns_stage_t(const StageArgsT<T>& a, cudaStream_t s) {
-    using S = Shape<P>;
+    using S = Shape<P, EbDiv<T>::value>;
     const long long grid = (a.n_elem + S::EB - 1) / S::EB;
     if (grid <= 0) return cudaSuccess;
     static bool set = false;

@@ -49,7 +49,7 @@ using namespace phys;
 // start on disjoint banks.
 template <int P, typename T>
 struct Tiles {
-    using S = Shape<P>;
+    using S = Shape<P, EbDiv<T>::value>;
     static constexpr int pad32(int base) {
         return base + ((((S::TPE + 3) & ~3) % 32) - base % 32 + 64) % 32;
     }
@@ -86,6 +86,45 @@ __device__ __forceinline__ void load_state(const double* p, T* u) {
     load4(p, d);
 #pragma unroll
     for (int v = 0; v < 4; ++v) u[v] = T(d[v]);
+}
+
+// Stage state of one solution point: FP64 copy in ud, arithmetic copy in u
+// (with the input tangent for the dual-number instantiation).
+template <typename T>
+__device__ __forceinline__ void stage_state(const StageArgsT<T>& a, long long idx, double* ud, T* u) {
+    load4(a.U + idx * 4, ud);
+    if constexpr (IsDual<T>::value) {
+        double t[4];
+        load4(a.dU + idx * 4, t);
+#pragma unroll
+        for (int v = 0; v < 4; ++v) u[v] = Dual(ud[v], t[v]);
+    } else {
+#pragma unroll
+        for (int v = 0; v < 4; ++v) u[v] = T(ud[v]);
+    }
+}
+
+// Stage-0 output: the FP64 residual (and its tangent for duals); adds the
+// residual's squares to rsq.
+template <typename T>
+__device__ __forceinline__ void store_residual(const StageArgsT<T>& a, long long idx, const T* res,
+                                               double& rsq) {
+    double rd[4];
+#pragma unroll
+    for (int v = 0; v < 4; ++v) { rd[v] = double(res[v]); rsq += rd[v] * rd[v]; }
+    store4(a.R + idx * 4, rd);
+    if constexpr (IsDual<T>::value) {
+        double td[4];
+#pragma unroll
+        for (int v = 0; v < 4; ++v) td[v] = res[v].d;
+        store4(a.dR + idx * 4, td);
+    }
+}
+
+template <typename T>
+__device__ __forceinline__ T reynolds(const StageArgsT<T>& a) {
+    if constexpr (IsDual<T>::value) return Dual(a.Re, a.dRe);
+    else return T(a.Re);
 }
 
 // SSP-RK3 stage update in FP64 from the stage state us, the base state u0
@@ -145,11 +184,12 @@ __device__ __forceinline__ void state_minus_ref(const double* U, const T* ue, T*
 template <typename T> struct PhysMinBlocks;
 template <> struct PhysMinBlocks<double> { static constexpr int value = ZJ_PHYS_MIN_BLOCKS; };
 template <> struct PhysMinBlocks<float> { static constexpr int value = ZJ_PHYS32_MIN_BLOCKS; };
+template <> struct PhysMinBlocks<Dual> { static constexpr int value = 1; };
 
 template <int P, int RIEM, typename T>
-__global__ void __launch_bounds__(Shape<P>::THREADS, PhysMinBlocks<T>::value)
+__global__ void __launch_bounds__(Shape<P, EbDiv<T>::value>::THREADS, PhysMinBlocks<T>::value)
 k_phys_stage(const StageArgsT<T> a) {
-    using S = Shape<P>;
+    using S = Shape<P, EbDiv<T>::value>;
     constexpr int N1 = S::N1, NSP = S::NSP, NFT = S::NFT, TPE = S::TPE, EB = S::EB;
     constexpr int RS = S::RS, VS = S::VS, FS = Tiles<P, T>::FS, DS = Tiles<P, T>::DS;
     __shared__ T sOps[S::NOPS];
@@ -185,10 +225,11 @@ k_phys_stage(const StageArgsT<T> a) {
     }
     if (is_sp) {
         const long long idx = e * NSP + k;
-        load_state(a.U + idx * 4, u);
+        double ud[4];
+        stage_state(a, idx, ud, u);
         T ji[4];
         load4_nc(a.Jinv + idx * 4, ji);
-        Jd = __ldg(a.J + idx);
+        Jd = ldg_any(a.J + idx);
         if ((k & 3) == 0 && a.stage >= 2) prefetch_l2(a.U0 + idx * 4);
         T F[4], G[4];
         euler_flux(u, g, F, G);
@@ -280,10 +321,7 @@ k_phys_stage(const StageArgsT<T> a) {
             res[v] = -(div + corr) * iJ;
         }
         if (a.stage == 0) {
-            double rd[4];
-#pragma unroll
-            for (int v = 0; v < 4; ++v) { rd[v] = double(res[v]); rsq += rd[v] * rd[v]; }
-            store4(a.R + idx * 4, rd);
+            store_residual(a, idx, res, rsq);
         } else {
             // The FP64 stage state: the registers of the FP64 path, a reload
             // (L1/L2-resident) for the mixed form.
@@ -335,9 +373,9 @@ k_phys_stage(const StageArgsT<T> a) {
 // Traces (and boundary ghost rows) of a state that did not come out of a
 // stage launch.  a.U: state, a.Tout: trace buffer.
 template <int P, typename T>
-__global__ void __launch_bounds__(Shape<P>::THREADS)
+__global__ void __launch_bounds__(Shape<P, EbDiv<T>::value>::THREADS)
 k_phys_traces(const StageArgsT<T> a) {
-    using S = Shape<P>;
+    using S = Shape<P, EbDiv<T>::value>;
     constexpr int N1 = S::N1, NSP = S::NSP, NFT = S::NFT, TPE = S::TPE, EB = S::EB;
     constexpr int RS = S::RS, VS = S::VS, FS = Tiles<P, T>::FS;
     __shared__ T sOps[S::NOPS];
@@ -352,14 +390,10 @@ k_phys_traces(const StageArgsT<T> a) {
     if (kRef && valid) load_state(a.U + e * NSP * 4, ue);
     if (valid && k < NSP) {
         double u[4];
-        load4_nc(a.U + (e * NSP + k) * 4, u);
-        T* su = sU + el * FS + (k / N1) * RS + (k % N1);
         T w[4];
+        stage_state(a, e * NSP + k, u, w);
+        T* su = sU + el * FS + (k / N1) * RS + (k % N1);
         if constexpr (kRef) state_minus_ref(u, ue, w);
-        else {
-#pragma unroll
-            for (int v = 0; v < 4; ++v) w[v] = T(u[v]);
-        }
 #pragma unroll
         for (int v = 0; v < 4; ++v) su[v * VS] = w[v];
     }
@@ -390,7 +424,7 @@ void prefer_shared(K kernel) {
 
 template <int P, int RIEM, typename T>
 cudaError_t phys_stage_t(const StageArgsT<T>& a, cudaStream_t s) {
-    using S = Shape<P>;
+    using S = Shape<P, EbDiv<T>::value>;
     const long long grid = (a.n_elem + S::EB - 1) / S::EB;
     if (grid <= 0) return cudaSuccess;
     static bool carveout_set = false;
@@ -411,7 +445,7 @@ cudaError_t phys_stage_p(int riemann, const StageArgsT<T>& a, cudaStream_t s) {
 
 template <int P, typename T>
 cudaError_t phys_traces_t(const StageArgsT<T>& a, cudaStream_t s) {
-    using S = Shape<P>;
+    using S = Shape<P, EbDiv<T>::value>;
     const long long grid = (a.n_elem + S::EB - 1) / S::EB;
     if (grid <= 0) return cudaSuccess;
     k_phys_traces<P, T><<<(unsigned)grid, S::THREADS, 0, s>>>(a);

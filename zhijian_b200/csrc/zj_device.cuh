@@ -10,13 +10,16 @@
 namespace zj {
 namespace dev {
 
-template <int P>
+// EBDIV > 1 packs fewer elements per CTA: the dual-number instantiation
+// (16-byte values) uses EBDIV = 3 so its shared tiles stay within the 48 KB
+// of static shared memory.
+template <int P, int EBDIV = 1>
 struct Shape {
     static constexpr int N1 = P + 1;
     static constexpr int NSP = N1 * N1;
     static constexpr int NFT = 4 * N1;                 // flux points per element
     static constexpr int TPE = NSP > NFT ? NSP : NFT;  // threads per element
-    static constexpr int EB = (256 / TPE) > 0 ? (256 / TPE) : 1;
+    static constexpr int EB = (256 / TPE / EBDIV) > 0 ? (256 / TPE / EBDIV) : 1;
     static constexpr int THREADS = EB * TPE;
     static constexpr int NOPS = N1 * N1 + 4 * N1;
     // Shared-memory layout of per-element fields (doubles): [var][eta row][xi]
@@ -29,6 +32,9 @@ struct Shape {
     static constexpr int FS = 4 * VS + (6 - (4 * VS) % 16 + 16) % 16;
     static constexpr int DS = 4 * NFT + 2;
 };
+
+template <typename T>
+struct EbDiv { static constexpr int value = sizeof(T) > 8 ? 3 : 1; };
 
 __device__ __forceinline__ void load4(const double* p, double* v) {
     const double2 a = *reinterpret_cast<const double2*>(p);
@@ -57,6 +63,9 @@ __device__ __forceinline__ void load4_nc(const float* p, float* v) {
 __device__ __forceinline__ void store4(float* p, const float* v) {
     *reinterpret_cast<float4*>(p) = make_float4(v[0], v[1], v[2], v[3]);
 }
+
+__device__ __forceinline__ double ldg_any(const double* p) { return __ldg(p); }
+__device__ __forceinline__ float ldg_any(const float* p) { return __ldg(p); }
 
 // (nx, ny, len) of an edge-normal record.
 __device__ __forceinline__ void load_normal(const double4* p, double* n) {
@@ -89,6 +98,10 @@ __device__ __forceinline__ float sqrt_any(float a) {
     asm("sqrt.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(a));
     return y;
 }
+// Correctly rounded square root (the reference's sqrt where it is not on a
+// hot path).
+__device__ __forceinline__ double sqrt_ieee(double a) { return sqrt(a); }
+__device__ __forceinline__ float sqrt_ieee(float a) { return sqrtf(a); }
 // a / b: IEEE division in FP64, a * (1/b) in FP32.
 __device__ __forceinline__ double div_any(double a, double b) { return a / b; }
 __device__ __forceinline__ float div_any(float a, float b) { return a * rcp_any(b); }

@@ -3,6 +3,7 @@
 
 #include <cuda_runtime.h>
 
+#include "zj_dual.cuh"
 #include "zj_internal.h"
 
 namespace zj {
@@ -14,6 +15,7 @@ namespace zj {
 template <typename T> struct Vec4Of;
 template <> struct Vec4Of<double> { using type = double4; };
 template <> struct Vec4Of<float> { using type = float4; };
+template <> struct Vec4Of<Dual> { using type = Dual4; };
 
 template <typename T>
 struct StageArgsT {
@@ -39,9 +41,15 @@ struct StageArgsT {
     const T* TQ;            // gradient traces of U, [E][4 edges][n1][8] = (dU/dx, dU/dy)
     T* TQout;               // gradient traces written by the gradient launch
     double Re, Pr;
+    // Jacobian-vector product (T = Dual): tangent of the stage state and of
+    // Re in, tangent of the residual out (stage 0)
+    const double* dU;
+    double* dR;
+    double dRe;
 };
 using StageArgs = StageArgsT<double>;
 using StageArgs32 = StageArgsT<float>;
+using StageArgsDual = StageArgsT<Dual>;
 
 // Packed operator block: D1[n1*n1], Lm[n1], Lp[n1], gL[n1], gR[n1].
 inline int ops_size(int n1) { return n1 * n1 + 4 * n1; }
@@ -61,9 +69,57 @@ cudaError_t launch_ns_grad(int P, const StageArgs& a, cudaStream_t s);
 cudaError_t launch_ns_grad(int P, const StageArgs32& a, cudaStream_t s);
 cudaError_t launch_ns_stage(int P, int riemann, const StageArgs& a, cudaStream_t s);
 cudaError_t launch_ns_stage(int P, int riemann, const StageArgs32& a, cudaStream_t s);
+// Jacobian-vector products: the stage-0 kernels on dual numbers.  Grid:
+// dual_grid(P, E) CTAs (partials sized for it).
+cudaError_t launch_phys_traces(int P, const StageArgsDual& a, cudaStream_t s);
+cudaError_t launch_phys_stage(int P, int riemann, const StageArgsDual& a, cudaStream_t s);
+cudaError_t launch_ns_grad(int P, const StageArgsDual& a, cudaStream_t s);
+cudaError_t launch_ns_stage(int P, int riemann, const StageArgsDual& a, cudaStream_t s);
+int dual_grid(int P, long long n_elem);
+// Elementwise helpers of the differentiation entry points (jvp.cu).
+cudaError_t launch_to_dual(const double* x, Dual* y, long long n, cudaStream_t s);
+cudaError_t launch_lincomb(double* out, double a, const double* x, double b, const double* y,
+                           double c, const double* z, long long n, cudaStream_t s);
+int dot_grid();
+// out[0] = x . y, deterministic (fixed grid; partials has dot_grid() entries).
+cudaError_t launch_dot(const double* x, const double* y, long long n, double* partials,
+                       double* out, cudaStream_t s);
 cudaError_t launch_traces(int P, const double* U, double* T, const double* ops,
                           long long n_elem, cudaStream_t s);
 int stage_grid(int P, long long n_elem);
+
+// Vector-Jacobian product of the physics-mode residual (adjoint.cu).  Device
+// pointers; T / TQ are the forward traces (with ghost rows) and gradient
+// traces of U; Db, Tb, DUb are [E][4][n1][4] scratch.
+struct AdjArgs {
+    const double* U;
+    const double* L;        // residual adjoint (lambda)
+    double* W;              // (dR/dU)^T L
+    const double* T;
+    const double* TQ;
+    double* Db;             // dFbar per flux point
+    double* Tb;             // trace adjoint before the neighbour gather (NS)
+    double* DUb;            // adjoint of the gradient's face jumps (NS)
+    const double* Jinv;
+    const double* J;
+    const EdgeRec* edges;
+    const double4* enrm;
+    const double* bc;
+    const double* ops;
+    long long n_elem;
+    double gamma, Re, Pr;
+    double* re_part;        // optional, Navier-Stokes: per-CTA L . dR/dRe, adj_ns_grid entries
+    // optional fused output: out = c0 X0 + c1 X1 + c2 X2 + cw (dR/dU)^T L
+    // (an SSP-RK3 stage's adjoint update; X* may be NULL when c* is 0, out may
+    // alias any X*); out == NULL writes (dR/dU)^T L into W
+    double* out;
+    const double* X0;
+    const double* X1;
+    const double* X2;
+    double c0, c1, c2, cw;
+};
+cudaError_t launch_rhs_vjp(int P, int riemann, bool viscous, const AdjArgs& a, cudaStream_t s);
+int adj_ns_grid(int P, long long n_elem);
 
 // Deterministic reduction of per-CTA partial sums into out[0].
 cudaError_t launch_reduce_sum(const double* partials, int n, double* out, cudaStream_t s);

@@ -211,10 +211,10 @@ __device__ __forceinline__ void ghost_phys(const T* Ui, T nx, T ny, int bct,
             const T pt = bcd[0], Tt = bcd[1], dx = bcd[2], dy = bcd[3];
             T M2 = div_any(T(2), g - T(1)) * (pow_any(div_any(p, pt), div_any(-(g - T(1)), g)) - T(1));
             M2 = max_any(M2, T(0));
-            const T Mn = sqrt(M2);
+            const T Mn = sqrt_ieee(M2);
             const T Tb = div_any(Tt, T(1) + T(0.5) * (g - T(1)) * M2);
             const T rb = div_any(p, Tb);
-            const T vel = Mn * sqrt(div_any(g * p, rb));
+            const T vel = Mn * sqrt_ieee(div_any(g * p, rb));
             prim2cons(rb, vel * dx, vel * dy, p, g, Ug);
             break;
         }

@@ -175,6 +175,37 @@ class FRSolver:
     def set_stream(self, stream_ptr: int):
         self._ck(L.lib().zj_set_stream(self.h, C.c_void_p(stream_ptr)))
 
+    # -- differentiation (physics mode, FP64; device pointers) ------------
+    def rhs_jvp(self, U_ptr: int, V_ptr: int, JV_ptr: int, R_ptr: int = 0, dRe: float = 0.0):
+        """JV = dR/dU . V + dR/dRe dRe (and R(U) into R_ptr if given)."""
+        self._ck(L.lib().zj_rhs_jvp(self.h, C.c_void_p(U_ptr), C.c_void_p(V_ptr), dRe,
+                                    C.c_void_p(R_ptr or None), C.c_void_p(JV_ptr)))
+
+    def rhs_vjp(self, U_ptr: int, L_ptr: int, W_ptr: int, with_re: bool = False):
+        """W = (dR/dU)^T L; returns L . dR/dRe when with_re."""
+        v = C.c_double()
+        self._ck(L.lib().zj_rhs_vjp(self.h, C.c_void_p(U_ptr), C.c_void_p(L_ptr), C.c_void_p(W_ptr),
+                                    C.byref(v) if with_re else None))
+        return v.value if with_re else None
+
+    def step_vjp(self, U_ptr: int, dt: float, B_ptr: int, A_ptr: int, with_re: bool = False):
+        """A = dJ/dU(n) from B = dJ/dU(n+1) for one SSP-RK3 step from U;
+        returns that step's dJ/dRe contribution when with_re."""
+        v = C.c_double(0.0)
+        self._ck(L.lib().zj_step_vjp(self.h, C.c_void_p(U_ptr), dt, C.c_void_p(B_ptr), C.c_void_p(A_ptr),
+                                     C.byref(v) if with_re else None))
+        return v.value if with_re else None
+
+    def adjoint_run(self, dt: float, nsteps: int, k_ckpt: int, G_ptr: int):
+        """Checkpointed discrete adjoint of nsteps steps from the current
+        state: G holds dJ/dU(final) in, dJ/dU(initial) out.  Returns
+        {dRe, bytes, ms_forward, ms_adjoint}."""
+        dre, fw, bw = C.c_double(), C.c_double(), C.c_double()
+        nb = C.c_int64()
+        self._ck(L.lib().zj_adjoint_run(self.h, dt, nsteps, k_ckpt, C.c_void_p(G_ptr), C.byref(dre),
+                                        C.byref(nb), C.byref(fw), C.byref(bw)))
+        return {"dRe": dre.value, "bytes": nb.value, "ms_forward": fw.value, "ms_adjoint": bw.value}
+
     @property
     def time(self) -> float:
         return L.lib().zj_time(self.h)
