@@ -347,6 +347,7 @@ def run_ours(args):
               "gpu_launches": 3 * args.steps}
 
     precision = precision_errors(mesh, stream) if not args.no_error_run else None
+    adjoint = adjoint_run(stream) if not args.no_adjoint else None
 
     out = None
     if rank == 0:
@@ -363,12 +364,77 @@ def run_ours(args):
                           "l2": "no flush: each stage streams > 200 MB > 126 MB L2"},
                "roofline": roofline, "e2e": e2e, "gpu_launches": launches, "clocks": clocks,
                "fp64": fp64, "speedup_vs_fp64": value / fp64["value"],
-               "precision_errors": precision, "compat": compat}
+               "precision_errors": precision,
+               "adjoint_forward_ratio": adjoint["ratio"] if adjoint else None,
+               "adjoint": adjoint, "compat": compat}
         if world == 1 and not args.no_cpu_baseline:
             out["cpu_baseline"] = cpu_baseline(mesh, args.cpu_seconds, "ns")
     if world > 1:
         dist.destroy_process_group()
     return out
+
+
+def adjoint_run(stream, steps=200, k_ckpt=20, n_fd=4):
+    """Discrete adjoint of the Taylor-Green case on 128x128 jittered quads
+    (seed 4), P3, Roe, Re 5000, 200 SSP-RK3 steps at CFL 0.5, checkpoints
+    every 20 steps; J = domain integral of the kinetic energy at the final
+    time.  Device times of the checkpointed forward sweep and of the backward
+    sweep (recomputation included), the device memory of the checkpoints and
+    segment states, and central differences (h = 1e-6) on n_fd smooth seeded
+    directions as a spot check (the 64-direction check is in tests/)."""
+    import math
+    import torch
+    from zhijian_b200 import meshgen as M
+    from zhijian_b200.objectives import kinetic_energy, quadrature_weights
+    from zhijian_b200.solver import FRSolver, make_params
+    mesh = M.tgv_mesh(128, seed=4)
+    prm = make_params(poly_order=P, gamma=GAMMA, rho_inf=1.0, p_inf=1.0 / (GAMMA * MACH * MACH), Mach=MACH,
+                      riemann="Roe", flux_type="HU", compat=False, viscous=True, Re=5000.0, Pr=0.72,
+                      bcs=[(1, "slipwall")])
+    s = FRSolver(mesh, prm)
+    s.set_stream(stream.cuda_stream)
+    U0 = M.taylor_green(s.solution_point_coords())
+    s.copyToDevice(U0)
+    dt = s.computeTimeStep()
+    wq = quadrature_weights(mesh, P)
+
+    def J_of(U):
+        s.copyToDevice(U)
+        s.advance(dt, steps)
+        return kinetic_energy(s.copyToHost(), wq)
+    _, Gf = J_of(U0)
+    runs = []
+    for _ in range(2):                       # the first call also builds the buffers
+        s.copyToDevice(U0)
+        G = torch.from_numpy(Gf.copy()).cuda()
+        torch.cuda.synchronize()
+        info = s.adjoint_run(dt, steps, k_ckpt, G.data_ptr())
+        runs.append(info)
+    g = G.cpu().numpy()
+    info = runs[-1]
+    n = 128
+    errs = []
+    for d in range(n_fd):
+        c = M.uniform01(5 + d, 64).reshape(4, 4, 4) * 2.0 - 1.0
+        ii, jj = np.meshgrid(np.arange(n), np.arange(n))
+        x = (ii.ravel() + 0.5) / n * math.pi
+        y = (jj.ravel() + 0.5) / n * math.pi
+        V = np.zeros_like(U0)
+        for v in range(4):
+            f = sum(c[v, a, b] * np.sin((a + 1) * x) * np.sin((b + 1) * y) for a in range(4) for b in range(4))
+            V[..., v] = f[:, None]
+        V *= np.abs(U0).max(axis=(0, 1))
+        h = 1e-6
+        fd = (J_of(U0 + h * V)[0] - J_of(U0 - h * V)[0]) / (2 * h)
+        errs.append(abs(float(np.sum(g * V)) - fd) / abs(fd))
+    s.close()
+    return {"workload": "TGV 128x128 jittered (seed 4) Q1 quads, P3, Roe, HU, Navier-Stokes Re 5000, "
+                        f"{steps} SSP-RK3 steps at CFL 0.5, checkpoints every {k_ckpt} steps, "
+                        "J = integral of 1/2 rho |u|^2 at the final time",
+            "ms_forward": info["ms_forward"], "ms_adjoint": info["ms_adjoint"],
+            "ratio": info["ms_adjoint"] / info["ms_forward"],
+            "device_bytes": info["bytes"], "dJ_dRe": info["dRe"],
+            "fd_check": {"h": 1e-6, "directions": n_fd, "max_rel_err": max(errs)}}
 
 
 def precision_errors(mesh, stream, steps=1000):
@@ -407,6 +473,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
     ap.add_argument("--no-error-run", action="store_true")
+    ap.add_argument("--no-adjoint", action="store_true")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

@@ -1,0 +1,45 @@
+"""A few SSP-RK3 steps of the benchmark's Taylor-Green case, for external
+profilers (ncu) that capture a handful of launches:
+
+    python -m zhijian_b200.profile_case {ns|ns32|euler|euler32|compat} [steps] [n]
+
+ns / ns32: Navier-Stokes (Re 5000, Pr 0.72, Roe, HU), FP64 / precision form;
+euler / euler32: the inviscid physics-mode residual; compat: the reference
+residual semantics.  256x256 jittered Q1 quads on [0,pi]^2 (seed 1), P3,
+slip walls, dt = 2e-4 (n overrides the mesh size)."""
+from __future__ import annotations
+
+import math
+import sys
+
+from . import meshgen as M
+from .solver import FRSolver, make_params
+
+GAMMA, MACH = 1.4, 0.3
+MODES = {
+    "ns": dict(compat=False, viscous=True, riemann="Roe", flux_type="HU", Re=5000.0, Pr=0.72),
+    "ns32": dict(compat=False, viscous=True, riemann="Roe", flux_type="HU", Re=5000.0, Pr=0.72,
+                 precision="mixed"),
+    "euler": dict(compat=False, viscous=False, riemann="Roe", flux_type="HU"),
+    "euler32": dict(compat=False, viscous=False, riemann="Roe", flux_type="HU", precision="mixed"),
+    "compat": dict(compat=True, viscous=False, riemann="Rusanov", flux_type="HU"),
+}
+
+
+def main(argv):
+    mode = argv[1] if len(argv) > 1 else "ns"
+    steps = int(argv[2]) if len(argv) > 2 else 4
+    n = int(argv[3]) if len(argv) > 3 else 256
+    mesh = M.tgv_mesh(n, seed=1)
+    prm = make_params(poly_order=3, gamma=GAMMA, rho_inf=1.0, p_inf=1.0 / (GAMMA * MACH * MACH),
+                      Mach=MACH, bcs=[(1, "slipwall")], **MODES[mode])
+    s = FRSolver(mesh, prm)
+    s.copyToDevice(M.taylor_green(s.solution_point_coords()))
+    s.advance(2.0e-4, steps)
+    s.check_state()
+    print(f"{mode}: {steps} steps on {mesh.n_elem} elements, residual norm {s.computeResidual():.6e}")
+    return 0 if math.isfinite(s.computeResidual()) else 1
+
+
+if __name__ == "__main__":
+    sys.exit(main(sys.argv))
