@@ -348,6 +348,7 @@ def run_ours(args):
 
     precision = precision_errors(mesh, stream) if not args.no_error_run else None
     adjoint = adjoint_run(stream) if not args.no_adjoint else None
+    p5 = p5_precision_case(stream, args) if not args.no_p5 else None
 
     out = None
     if rank == 0:
@@ -366,11 +367,67 @@ def run_ours(args):
                "fp64": fp64, "speedup_vs_fp64": value / fp64["value"],
                "precision_errors": precision,
                "adjoint_forward_ratio": adjoint["ratio"] if adjoint else None,
-               "adjoint": adjoint, "compat": compat}
+               "adjoint": adjoint, "p5_precision": p5, "compat": compat}
         if world == 1 and not args.no_cpu_baseline:
             out["cpu_baseline"] = cpu_baseline(mesh, args.cpu_seconds, "ns")
     if world > 1:
         dist.destroy_process_group()
+    return out
+
+
+def p5_precision_case(stream, args, n=512, steps_err=1000):
+    """The precision form of the Taylor-Green case on 512x512 jittered quads
+    (seed 2) at P5 (36 solution points, 9.4 M DOF per variable), Navier-Stokes
+    Re 5000, Roe, HU: DOF-RHS/s of the precision form and of the FP64 path
+    (CUDA events over args.steps steps after args.warmup), and the L2 / Linf
+    error of the precision form against the FP64 path after 1000 steps at
+    CFL 0.5, with the FP64 conditioning floor (FP64 from the initial state
+    rounded once to FP32)."""
+    import torch
+    from zhijian_b200 import meshgen as M
+    from zhijian_b200.norms import state_errors
+    from zhijian_b200.solver import FRSolver, make_params
+    mesh = M.tgv_mesh(n, seed=2)
+
+    def solver(prec):
+        prm = make_params(poly_order=5, gamma=GAMMA, rho_inf=1.0, p_inf=1.0 / (GAMMA * MACH * MACH),
+                          Mach=MACH, riemann="Roe", flux_type="HU", compat=False, viscous=True,
+                          Re=5000.0, Pr=0.72, bcs=[(1, "slipwall")], precision=prec)
+        sv = FRSolver(mesh, prm)
+        sv.set_stream(stream.cuda_stream)
+        return sv
+    out = {"workload": f"TGV {n}x{n} jittered (seed 2) Q1 quads, P5, Navier-Stokes Re 5000, Roe, HU, SSP-RK3"}
+    U0 = None
+    steps = min(args.steps, 100)
+    for prec in ("fp64", "mixed"):
+        sv = solver(prec)
+        if U0 is None:
+            U0 = M.taylor_green(sv.solution_point_coords())
+        sv.copyToDevice(U0)
+        sv.advance(DT / 4, args.warmup)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        sv.advance(DT / 4, steps, sync=False)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / steps
+        out[prec] = {"ms_per_step": ms, "value": sv.n_elem * sv.n_sp * 3 / (ms * 1e-3), "steps": steps}
+        sv.close()
+    out["speedup_vs_fp64"] = out["mixed"]["value"] / out["fp64"]["value"]
+    if not args.no_error_run:
+        s64, s32, sfl = solver("fp64"), solver("mixed"), solver("fp64")
+        s64.copyToDevice(U0)
+        dt = s64.computeTimeStep()
+        for sv, U in ((s64, U0), (s32, U0), (sfl, U0.astype(np.float32).astype(np.float64))):
+            sv.copyToDevice(U)
+            sv.advance(dt, steps_err)
+        U64, U32, Ufl = s64.copyToHost(), s32.copyToHost(), sfl.copyToHost()
+        for sv in (s64, s32, sfl):
+            sv.close()
+        e, fl = state_errors(U32, U64), state_errors(Ufl, U64)
+        out["errors"] = {"steps": steps_err, "dt": dt, "vars": ["rho", "rhou", "rhov", "rhoE"],
+                         "l2": e["l2"], "linf": e["linf"], "fp64_floor_l2": fl["l2"]}
     return out
 
 
@@ -474,6 +531,7 @@ def main():
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
     ap.add_argument("--no-error-run", action="store_true")
     ap.add_argument("--no-adjoint", action="store_true")
+    ap.add_argument("--no-p5", action="store_true")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
