@@ -229,11 +229,26 @@ zj_status zj_step_vjp(zj_solver* s, const double* U_dev, double dt, const double
 zj_status zj_adjoint_run(zj_solver* s, double dt, int nsteps, int k_ckpt, double* G_dev,
                          double* dRe, int64_t* bytes, double* ms_forward, double* ms_adjoint);
 
-/* ---- config-file convenience: parse + mesh from a Gmsh file ---------------- */
-/* Read an ASCII Gmsh MSH v2.2 / v4.1 quad mesh (src/mesh/gmsh_reader.cpp:161)
- * and create a solver.  Physical names map to boundary types as
- * GmshReader::inferBCType (gmsh_reader.cpp:117-155) unless the params' bc
- * table names the tag. */
+/* ---- Gmsh meshes -------------------------------------------------------------
+ * Read an ASCII Gmsh MSH v2.2 / v4.1 mesh (GmshReader::read,
+ * src/mesh/gmsh_reader.cpp:161-396) into library-owned arrays; no device is
+ * touched.  Failures return ZJ_ERR_IO (cannot open) or ZJ_ERR_ARG (format,
+ * unknown node tag, no 2D elements) with the reader's message in
+ * zj_last_error(NULL). */
+typedef struct zj_gmsh_mesh zj_gmsh_mesh;
+zj_status zj_gmsh_read(const char* msh_path, zj_gmsh_mesh** out);
+void zj_gmsh_free(zj_gmsh_mesh* m);
+/* The mesh as a solver descriptor (valid until zj_gmsh_free). */
+const zj_mesh_desc* zj_gmsh_desc(const zj_gmsh_mesh* m);
+/* Boundary groups (GmshReader::mapBoundaryConditions, gmsh_reader.cpp:651-709):
+ * physical tag, type inferred from the physical name (GmshReader::inferBCType,
+ * gmsh_reader.cpp:117-155) and the name ("BC_<tag>" when unnamed). */
+int zj_gmsh_num_groups(const zj_gmsh_mesh* m);
+zj_status zj_gmsh_group(const zj_gmsh_mesh* m, int i, int* tag, int* bc_type, const char** name);
+
+/* Read a Gmsh mesh and create a solver.  Boundary groups the params' bc table
+ * does not name get their inferred type (as the reference's reader stamps
+ * them on the faces, gmsh_reader.cpp:715-758). */
 zj_status zj_solver_create_from_gmsh(const char* msh_path, const zj_params* params,
                                      zj_solver** out);
 

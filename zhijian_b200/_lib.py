@@ -92,6 +92,11 @@ def lib():
         "zj_iteration": (ip, [vp]),
         "zj_set_stream": (ip, [vp, vp]),
         "zj_get_stream": (vp, [vp]),
+        "zj_gmsh_read": (ip, [C.c_char_p, C.POINTER(vp)]),
+        "zj_gmsh_free": (None, [vp]),
+        "zj_gmsh_desc": (C.POINTER(MeshDesc), [vp]),
+        "zj_gmsh_num_groups": (ip, [vp]),
+        "zj_gmsh_group": (ip, [vp, ip, C.POINTER(ip), C.POINTER(ip), C.POINTER(C.c_char_p)]),
         "zj_rhs_jvp": (ip, [vp, vp, vp, C.c_double, vp, vp]),
         "zj_rhs_vjp": (ip, [vp, vp, vp, vp, dp]),
         "zj_step_vjp": (ip, [vp, vp, C.c_double, vp, vp, dp]),

@@ -26,6 +26,11 @@
 
 using namespace zj;
 
+struct zj_gmsh_mesh {
+    GmshMesh g;
+    zj_mesh_desc desc{};
+};
+
 struct zj_solver {
     zj_params prm{};
     HostMesh mesh;
@@ -946,10 +951,67 @@ zj_status zj_adjoint_run(zj_solver* s, double dt, int nsteps, int k_ckpt, double
     return st;
 }
 
+zj_status zj_gmsh_read(const char* msh_path, zj_gmsh_mesh** out) {
+    if (!out) return fail(nullptr, ZJ_ERR_ARG, "out is NULL");
+    *out = nullptr;
+    if (!msh_path) return fail(nullptr, ZJ_ERR_ARG, "path is NULL");
+    zj_gmsh_mesh* m = new zj_gmsh_mesh();
+    std::string err;
+    if (!read_gmsh(msh_path, m->g, err)) {
+        delete m;
+        const bool io = err.rfind("Failed to open", 0) == 0;
+        return fail(nullptr, io ? ZJ_ERR_IO : ZJ_ERR_ARG, err);
+    }
+    m->desc.n_nodes = (int64_t)(m->g.xy.size() / 2);
+    m->desc.xy = m->g.xy.data();
+    m->desc.n_elem = (int64_t)m->g.etype.size();
+    m->desc.elem_type = m->g.etype.data();
+    m->desc.elem_order = m->g.eorder.data();
+    m->desc.conn_offsets = m->g.offs.data();
+    m->desc.conn = m->g.conn.data();
+    m->desc.n_bnd_edges = (int64_t)(m->g.bnd.size() / 3);
+    m->desc.bnd_edges = m->g.bnd.data();
+    *out = m;
+    return ZJ_OK;
+}
+
+void zj_gmsh_free(zj_gmsh_mesh* m) { delete m; }
+
+const zj_mesh_desc* zj_gmsh_desc(const zj_gmsh_mesh* m) { return m ? &m->desc : nullptr; }
+
+int zj_gmsh_num_groups(const zj_gmsh_mesh* m) { return m ? (int)m->g.groups.size() : 0; }
+
+zj_status zj_gmsh_group(const zj_gmsh_mesh* m, int i, int* tag, int* bc_type, const char** name) {
+    if (!m || i < 0 || i >= (int)m->g.groups.size()) return ZJ_ERR_ARG;
+    const GmshGroup& g = m->g.groups[(size_t)i];
+    if (tag) *tag = g.tag;
+    if (bc_type) *bc_type = g.type;
+    if (name) *name = g.name.c_str();
+    return ZJ_OK;
+}
+
 zj_status zj_solver_create_from_gmsh(const char* msh_path, const zj_params* params, zj_solver** out) {
-    (void)msh_path; (void)params;
     if (out) *out = nullptr;
-    return fail(nullptr, ZJ_ERR_UNSUPPORTED, "Gmsh reader not built yet");
+    if (!out || !params) return fail(nullptr, ZJ_ERR_ARG, "params or out is NULL");
+    zj_gmsh_mesh* m = nullptr;
+    zj_status st = zj_gmsh_read(msh_path, &m);
+    if (st != ZJ_OK) return st;
+    zj_params p = *params;
+    for (const GmshGroup& g : m->g.groups) {
+        bool named = false;
+        for (int k = 0; k < p.n_bc; ++k) named = named || p.bc[k].tag == g.tag;
+        if (named) continue;
+        if (p.n_bc >= ZJ_MAX_BC) { zj_gmsh_free(m); return fail(nullptr, ZJ_ERR_ARG, "too many boundary groups"); }
+        zj_bc_spec& b = p.bc[p.n_bc++];
+        b = zj_bc_spec{};
+        b.tag = g.tag;
+        b.type = g.type;
+        b.dir_x = 1.0;
+        b.dir_y = 0.0;
+    }
+    st = zj_solver_create(&m->desc, &p, out);
+    zj_gmsh_free(m);
+    return st;
 }
 
 }  // extern "C"

@@ -83,4 +83,21 @@ void element_areas(const HostMesh& m, std::vector<double>& area);
 void build_bc_data(const HostMesh& m, const zj_params* p, std::vector<double>& bc);
 void build_edge_records(const HostMesh& m, std::vector<EdgeRec>& rec, std::vector<double>& nrm);
 
+// Gmsh reader (gmsh.cpp).
+struct GmshGroup {
+    int tag = 0;
+    int type = 0;          // zj_bc_type inferred from the name
+    std::string name;
+};
+struct GmshMesh {
+    std::vector<double> xy;        // [n][2]
+    std::vector<int32_t> etype, eorder;
+    std::vector<int64_t> offs;     // [n_elem + 1]
+    std::vector<int64_t> conn;
+    std::vector<int64_t> bnd;      // [n_bnd][3] (v0, v1, physical tag)
+    std::vector<GmshGroup> groups; // boundary groups in tag order
+};
+bool read_gmsh(const std::string& path, GmshMesh& m, std::string& err);
+int infer_bc_type(const std::string& name);
+
 }  // namespace zj

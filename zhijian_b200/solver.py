@@ -87,6 +87,20 @@ class FRSolver:
         d.bnd_edges = bnd.ctypes.data_as(C.POINTER(C.c_int64))
         h = C.c_void_p()
         L.check(lib.zj_solver_create(C.byref(d), C.byref(params), C.byref(h)))
+        self._attach(h, params)
+
+    @classmethod
+    def from_gmsh(cls, path: str, params: L.Params) -> "FRSolver":
+        """A solver on an ASCII Gmsh mesh (zj_solver_create_from_gmsh)."""
+        h = C.c_void_p()
+        L.check(L.lib().zj_solver_create_from_gmsh(str(path).encode(), C.byref(params), C.byref(h)))
+        self = cls.__new__(cls)
+        self._keep = []
+        self._attach(h, params)
+        return self
+
+    def _attach(self, h, params):
+        lib = L.lib()
         self.h = h
         self.params = params
         self.n_elem = lib.zj_num_elements(h)
