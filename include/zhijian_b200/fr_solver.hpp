@@ -106,6 +106,12 @@ public:
     }
 
     double currentTime() const { return zj_time(s_); }
+    int currentIteration() const { return zj_iteration(s_); }
+
+    // RestartIO::write / read (src/io/restart.cpp:8-144) in the library's
+    // dependency-free restart format; reading resumes time and iteration.
+    void writeRestart(const std::string& path) { check(zj_restart_write(s_, path.c_str()), s_); }
+    void readRestart(const std::string& path) { check(zj_restart_read(s_, path.c_str()), s_); }
     int iteration() const { return zj_iteration(s_); }
 
     // FRSolver::copyToHost / copyToDevice (fr_solver.cpp:835-871): the flat

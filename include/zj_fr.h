@@ -229,6 +229,22 @@ zj_status zj_step_vjp(zj_solver* s, const double* U_dev, double dt, const double
 zj_status zj_adjoint_run(zj_solver* s, double dt, int nsteps, int k_ckpt, double* G_dev,
                          double* dRe, int64_t* bytes, double* ms_forward, double* ms_adjoint);
 
+/* ---- restart files ------------------------------------------------------------
+ * The fields of RestartIO (src/io/restart.cpp:8-144) -- attributes time,
+ * iteration, poly_order, gamma; datasets elem_n_sp [E] and solution
+ * [E][n_sp][4] f64 -- in a dependency-free little-endian binary file:
+ *   "ZJRESTRT" u32 version=1 u32 reserved=0 f64 time i32 iteration
+ *   i32 poly_order f64 gamma i64 n_elem i32 elem_n_sp[n_elem]
+ *   f64 solution[sum n_sp * 4] u64 FNV-1a-64 of every preceding byte.
+ * zj_restart_write stores the handle's current state, time and iteration
+ * (synchronises); zj_restart_read checks the file against the handle (magic,
+ * version, checksum, n_elem, n_sp, poly_order, gamma), loads the state and
+ * resumes time and iteration, which the reference's reader leaves unused
+ * (src/main.cpp:349-360).  ZJ_ERR_IO: cannot open/short file; ZJ_ERR_ARG:
+ * mismatch or corrupt file. */
+zj_status zj_restart_write(zj_solver* s, const char* path);
+zj_status zj_restart_read(zj_solver* s, const char* path);
+
 /* ---- Gmsh meshes -------------------------------------------------------------
  * Read an ASCII Gmsh MSH v2.2 / v4.1 mesh (GmshReader::read,
  * src/mesh/gmsh_reader.cpp:161-396) into library-owned arrays; no device is

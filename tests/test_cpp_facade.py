@@ -49,3 +49,20 @@ def test_driver_matches_python_binding(zjlib, tmp_path):
     U = s.copyToHost()
     assert abs(np.abs(U).sum() - chk) <= 1e-12 * chk
     assert abs(s.computeResidual() - res_cpp) <= 1e-9 * res_cpp
+
+
+@pytest.mark.gpu
+def test_driver_restart_resumes(zjlib, tmp_path):
+    """20 steps in one run equal 12 steps, a restart file, and 8 more steps
+    resumed from it (state, time and iteration)."""
+    exe = build.build_driver()
+    cfg = tmp_path / "c.txt"
+    cfg.write_text(CONFIG + "restart_freq 1000\n")
+    args = [exe, str(cfg), "8", "8", "-5", "5", "-5", "5"]
+    full = subprocess.run(args + ["20", "vortex"], capture_output=True, text=True, check=True).stdout
+    rst = tmp_path / "state.zjr"
+    subprocess.run(args + ["12", "vortex", "-w", str(rst)], capture_output=True, text=True, check=True)
+    resumed = subprocess.run(args + ["20", "vortex", "-r", str(rst)], capture_output=True, text=True,
+                             check=True).stdout
+    assert full.splitlines()[-1] == resumed.splitlines()[-1]          # bit-identical checksum
+    assert full.splitlines()[-2].split()[:2] == resumed.splitlines()[-2].split()[:2]   # iteration, time

@@ -92,6 +92,8 @@ def lib():
         "zj_iteration": (ip, [vp]),
         "zj_set_stream": (ip, [vp, vp]),
         "zj_get_stream": (vp, [vp]),
+        "zj_restart_write": (ip, [vp, C.c_char_p]),
+        "zj_restart_read": (ip, [vp, C.c_char_p]),
         "zj_gmsh_read": (ip, [C.c_char_p, C.POINTER(vp)]),
         "zj_gmsh_free": (None, [vp]),
         "zj_gmsh_desc": (C.POINTER(MeshDesc), [vp]),

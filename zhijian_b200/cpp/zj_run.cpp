@@ -4,12 +4,16 @@
 // initial state, then computeTimeStep -> advance -> computeResidual.
 //
 //   zj_run <config> <nx> <ny> <x0> <x1> <y0> <y1> [steps] [vortex]
+//          [-r <restart file>] [-w <restart file>]
 // prints "iter time dt residual" every 10 iterations and the final state
-// checksum (sum of |U|) on the last line.
+// checksum (sum of |U|) on the last line.  -r resumes from a restart file
+// (state, time, iteration; src/main.cpp:345-360), -w writes one every
+// restart_freq iterations and at the end (src/main.cpp:455-466).
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
 #include <string>
+#include <vector>
 
 #include "zhijian_b200/fr_solver.hpp"
 
@@ -49,8 +53,15 @@ int main(int argc, char** argv) {
         std::fprintf(stderr, "cannot read %s\n", argv[1]);
         return 1;
     }
-    const int steps = argc > 8 ? std::atoi(argv[8]) : p.max_iter;
-    const bool vortex = argc > 9 && std::string(argv[9]) == "vortex";
+    std::string restart_in, restart_out;
+    std::vector<std::string> pos;
+    for (int a = 8; a < argc; ++a) {
+        const std::string arg = argv[a];
+        if ((arg == "-r" || arg == "-w") && a + 1 < argc) (arg == "-r" ? restart_in : restart_out) = argv[++a];
+        else pos.push_back(arg);
+    }
+    const int steps = pos.size() > 0 ? std::atoi(pos[0].c_str()) : p.max_iter;
+    const bool vortex = pos.size() > 1 && pos[1] == "vortex";
     Mesh mesh = structured(std::atoi(argv[2]), std::atoi(argv[3]), std::atof(argv[4]), std::atof(argv[5]),
                            std::atof(argv[6]), std::atof(argv[7]));
     try {
@@ -73,12 +84,16 @@ int main(int argc, char** argv) {
             }
             return State{rho, rho * u, rho * v, pr / (g - 1.0) + 0.5 * rho * (u * u + v * v)};
         });
+        if (!restart_in.empty()) solver.readRestart(restart_in);
         const double dt = p.dt > 0 ? p.dt : solver.computeTimeStep();
-        for (int it = 0; it < steps; ++it) {
+        for (int it = solver.currentIteration(); it < steps; ++it) {
             solver.advance(dt);
             if (it % 10 == 0 || it == steps - 1)
                 std::printf("%6d %.6e %.6e %.10e\n", it, solver.currentTime(), dt, solver.computeResidual());
+            if (!restart_out.empty() && p.restart_freq > 0 && (it + 1) % p.restart_freq == 0)
+                solver.writeRestart(restart_out);
         }
+        if (!restart_out.empty()) solver.writeRestart(restart_out);
         solver.copyToHost();
         double sum = 0.0;
         for (double x : solver.solution()) sum += std::fabs(x);

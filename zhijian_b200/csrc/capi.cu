@@ -951,6 +951,105 @@ zj_status zj_adjoint_run(zj_solver* s, double dt, int nsteps, int k_ckpt, double
     return st;
 }
 
+}  // extern "C"
+
+// ------------------------------------------------------------- restart --
+namespace {
+
+constexpr char kRestartMagic[8] = {'Z', 'J', 'R', 'E', 'S', 'T', 'R', 'T'};
+constexpr uint32_t kRestartVersion = 1;
+
+uint64_t fnv1a(const unsigned char* p, size_t n, uint64_t h = 1469598103934665603ULL) {
+    for (size_t i = 0; i < n; ++i) { h ^= p[i]; h *= 1099511628211ULL; }
+    return h;
+}
+
+struct Bytes {
+    std::vector<unsigned char> b;
+    template <class T> void put(const T& v) {
+        const unsigned char* p = reinterpret_cast<const unsigned char*>(&v);
+        b.insert(b.end(), p, p + sizeof(T));
+    }
+    void put_raw(const void* p, size_t n) {
+        const unsigned char* c = static_cast<const unsigned char*>(p);
+        b.insert(b.end(), c, c + n);
+    }
+};
+
+}  // namespace
+
+extern "C" {
+
+zj_status zj_restart_write(zj_solver* s, const char* path) {
+    if (!s || !path) return ZJ_ERR_ARG;
+    std::vector<double> U(s->state_n);
+    zj_status st = zj_get_state(s, U.data());
+    if (st != ZJ_OK) return st;
+    Bytes f;
+    f.put_raw(kRestartMagic, 8);
+    f.put(kRestartVersion);
+    f.put(uint32_t(0));
+    f.put(s->time);
+    f.put(int32_t(s->iter));
+    f.put(int32_t(s->P));
+    f.put(s->prm.gamma);
+    f.put(int64_t(s->E));
+    std::vector<int32_t> nsp((size_t)s->E, s->nsp);
+    f.put_raw(nsp.data(), nsp.size() * sizeof(int32_t));
+    f.put_raw(U.data(), U.size() * sizeof(double));
+    f.put(fnv1a(f.b.data(), f.b.size()));
+    FILE* fp = std::fopen(path, "wb");
+    if (!fp) return fail(s, ZJ_ERR_IO, std::string("cannot create restart file ") + path);
+    const size_t w = std::fwrite(f.b.data(), 1, f.b.size(), fp);
+    const int c = std::fclose(fp);
+    if (w != f.b.size() || c != 0) return fail(s, ZJ_ERR_IO, std::string("short write to ") + path);
+    return ZJ_OK;
+}
+
+zj_status zj_restart_read(zj_solver* s, const char* path) {
+    if (!s || !path) return ZJ_ERR_ARG;
+    FILE* fp = std::fopen(path, "rb");
+    if (!fp) return fail(s, ZJ_ERR_IO, std::string("cannot open restart file ") + path);
+    std::vector<unsigned char> b;
+    unsigned char buf[1 << 16];
+    size_t n;
+    while ((n = std::fread(buf, 1, sizeof(buf), fp)) > 0) b.insert(b.end(), buf, buf + n);
+    std::fclose(fp);
+    const size_t head = 8 + 4 + 4 + 8 + 4 + 4 + 8 + 8;
+    if (b.size() < head + 8) return fail(s, ZJ_ERR_IO, "restart file too short");
+    if (std::memcmp(b.data(), kRestartMagic, 8) != 0) return fail(s, ZJ_ERR_ARG, "not a restart file");
+    size_t o = 8;
+    auto get = [&](auto& v) { std::memcpy(&v, b.data() + o, sizeof(v)); o += sizeof(v); };
+    uint32_t version = 0, reserved = 0;
+    double time = 0.0, gamma = 0.0;
+    int32_t iter = 0, order = 0;
+    int64_t ne = 0;
+    get(version); get(reserved); get(time); get(iter); get(order); get(gamma); get(ne);
+    if (version != kRestartVersion) return fail(s, ZJ_ERR_ARG, "unsupported restart version " + std::to_string(version));
+    if (ne != s->E)
+        return fail(s, ZJ_ERR_ARG, "restart file has " + std::to_string(ne) + " elements, the mesh " + std::to_string(s->E));
+    const size_t need = head + (size_t)ne * 4 + s->state_n * 8 + 8;
+    if (b.size() != need) return fail(s, ZJ_ERR_ARG, "restart file size does not match its element count");
+    uint64_t sum = 0;
+    std::memcpy(&sum, b.data() + b.size() - 8, 8);
+    if (sum != fnv1a(b.data(), b.size() - 8)) return fail(s, ZJ_ERR_ARG, "restart file checksum mismatch");
+    if (order != s->P)
+        return fail(s, ZJ_ERR_ARG, "restart file is poly_order " + std::to_string(order) + ", the solver " + std::to_string(s->P));
+    if (gamma != s->prm.gamma) return fail(s, ZJ_ERR_ARG, "restart file gamma differs from the solver's");
+    for (int64_t e = 0; e < ne; ++e) {
+        int32_t k = 0;
+        std::memcpy(&k, b.data() + head + (size_t)e * 4, 4);
+        if (k != s->nsp) return fail(s, ZJ_ERR_ARG, "restart file element " + std::to_string(e) + " has a different n_sp");
+    }
+    const double* U = reinterpret_cast<const double*>(b.data() + head + (size_t)ne * 4);
+    std::vector<double> Ua(U, U + s->state_n);     // aligned copy
+    zj_status st = zj_set_state(s, Ua.data());
+    if (st != ZJ_OK) return st;
+    s->time = time;      // resume
+    s->iter = iter;
+    return ZJ_OK;
+}
+
 zj_status zj_gmsh_read(const char* msh_path, zj_gmsh_mesh** out) {
     if (!out) return fail(nullptr, ZJ_ERR_ARG, "out is NULL");
     *out = nullptr;

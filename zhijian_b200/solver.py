@@ -189,6 +189,15 @@ class FRSolver:
     def set_stream(self, stream_ptr: int):
         self._ck(L.lib().zj_set_stream(self.h, C.c_void_p(stream_ptr)))
 
+    # -- restart files ----------------------------------------------------
+    def write_restart(self, path: str):
+        """State, time and iteration into a restart file (zj_restart_write)."""
+        self._ck(L.lib().zj_restart_write(self.h, str(path).encode()))
+
+    def read_restart(self, path: str):
+        """Load a restart file and resume its time and iteration."""
+        self._ck(L.lib().zj_restart_read(self.h, str(path).encode()))
+
     # -- differentiation (physics mode, FP64; device pointers) ------------
     def rhs_jvp(self, U_ptr: int, V_ptr: int, JV_ptr: int, R_ptr: int = 0, dRe: float = 0.0):
         """JV = dR/dU . V + dR/dRe dRe (and R(U) into R_ptr if given)."""
