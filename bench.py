@@ -16,7 +16,10 @@ the L2 / Linf error of rho, rho u, rho v, rho E after 1000 steps at CFL 0.5
 against the FP64 path (which matches the FP64 oracle to 1e-12 per residual)
 with the FP64 conditioning floor beside it.  The same mesh and state in the
 reference's residual semantics (compat: Rusanov, inviscid, clamps, FP64) is
-the `compat` object.
+the `compat` object.  `p5_precision` is the precision form of the same flow
+at P5 on 512x512 quads; `mixed_elements` the shear layer on 384x384 quads
+with 30% split into triangles (P2-P4, SD and GA, precision form against
+FP64).
 
 ours:      the CUDA path, timed with CUDA events on the solver's stream, max
            over ranks; N > 1 runs one independent replica per GPU (the path
@@ -349,6 +352,7 @@ def run_ours(args):
     precision = precision_errors(mesh, stream) if not args.no_error_run else None
     adjoint = adjoint_run(stream) if not args.no_adjoint else None
     p5 = p5_precision_case(stream, args) if not args.no_p5 else None
+    shear = shear_layer_sweep(stream, args) if not args.no_mixed else None
 
     out = None
     if rank == 0:
@@ -367,7 +371,7 @@ def run_ours(args):
                "fp64": fp64, "speedup_vs_fp64": value / fp64["value"],
                "precision_errors": precision,
                "adjoint_forward_ratio": adjoint["ratio"] if adjoint else None,
-               "adjoint": adjoint, "p5_precision": p5, "compat": compat}
+               "adjoint": adjoint, "p5_precision": p5, "mixed_elements": shear, "compat": compat}
         if world == 1 and not args.no_cpu_baseline:
             out["cpu_baseline"] = cpu_baseline(mesh, args.cpu_seconds, "ns")
     if world > 1:
@@ -429,6 +433,83 @@ def p5_precision_case(stream, args, n=512, steps_err=1000):
         out["errors"] = {"steps": steps_err, "dt": dt, "vars": ["rho", "rhou", "rhov", "rhoE"],
                          "l2": e["l2"], "linf": e["linf"], "fp64_floor_l2": fl["l2"]}
     return out
+
+
+# CFL per order for the shear layer: the reference's convective time step,
+# kept under the explicit viscous limit of the 384x384 mesh (P3 at CFL 0.5
+# diverges within 20 steps on quads alone; the SD correction at P4 needs the
+# smallest value).
+SHEAR_CFL = {2: 0.2, 3: 0.1, 4: 0.02}
+
+
+def shear_layer_sweep(stream, args, n=384, steps_err=100):
+    """The mixed-element case: 384x384 quads on [0,1]^2 with a seeded (seed 3)
+    30% split into two triangles each, the Navier-Stokes shear layer (Re 2000,
+    M 0.3), HLLC, slip walls at y = 0, 1 and a far field at rest at x = 0, 1
+    (meshgen.SHEAR_LAYER_PARAMS); P2, P3, P4
+    with the SD and GA corrections.  Per case: DOF-RHS/s of the precision form
+    and of the FP64 path (CUDA events, min(args.steps, 50) steps after
+    args.warmup), and the L2 / Linf error of the precision form against the
+    FP64 path after `steps_err` steps at SHEAR_CFL[P], over the solution
+    points in use (triangles hold (P+1)(P+2)/2 of their (P+1)^2 slots).  The
+    corners where the slip walls meet the far field diverge after 160-290
+    steps at these CFL numbers (on quads alone too, and a smaller CFL does not
+    remove it), so the error run stops at 100."""
+    import torch
+    from zhijian_b200 import meshgen as M
+    from zhijian_b200.norms import state_errors
+    from zhijian_b200.solver import FRSolver, make_params
+    mesh = M.shear_layer_mesh(n)
+    kinds = None
+    cases = []
+    for P in (2, 3, 4):
+        for flux in ("SD", "GA"):
+            def solver(prec):
+                prm = make_params(poly_order=P, flux_type=flux, CFL=SHEAR_CFL[P], precision=prec,
+                                  **M.SHEAR_LAYER_PARAMS)
+                sv = FRSolver(mesh, prm)
+                sv.set_stream(stream.cuda_stream)
+                return sv
+            case = {"P": P, "flux_type": flux, "cfl": SHEAR_CFL[P]}
+            U0 = dt = None
+            steps = min(args.steps, 50)
+            for prec in ("fp64", "mixed"):
+                sv = solver(prec)
+                if U0 is None:
+                    U0 = M.shear_layer(sv.solution_point_coords())
+                    kinds = sv.element_kinds()
+                    mask = sv.slot_mask()
+                    case["dof_per_var"] = int(mask.sum())
+                sv.copyToDevice(U0)
+                if dt is None:
+                    dt = sv.computeTimeStep()
+                sv.advance(dt, args.warmup)
+                torch.cuda.synchronize()
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record(stream)
+                sv.advance(dt, steps, sync=False)
+                e1.record(stream)
+                torch.cuda.synchronize()
+                ms = e0.elapsed_time(e1) / steps
+                case[prec] = {"ms_per_step": ms, "value": case["dof_per_var"] * 3 / (ms * 1e-3), "steps": steps}
+                sv.close()
+            case["speedup_vs_fp64"] = case["mixed"]["value"] / case["fp64"]["value"]
+            if not args.no_error_run:
+                s64, s32 = solver("fp64"), solver("mixed")
+                for sv in (s64, s32):
+                    sv.copyToDevice(U0)
+                    sv.advance(dt, steps_err)
+                U64, U32 = s64.copyToHost()[mask], s32.copyToHost()[mask]
+                for sv in (s64, s32):
+                    sv.close()
+                e = state_errors(U32, U64)
+                case["errors"] = {"steps": steps_err, "dt": dt, "finite": bool(np.isfinite(U64).all()),
+                                  "l2": e["l2"], "linf": e["linf"]}
+            cases.append(case)
+    return {"workload": f"shear layer {n}x{n} quads, seeded 30% split into triangles "
+                        f"({int((kinds == 0).sum())} triangles, {int((kinds == 1).sum())} quads), "
+                        "Navier-Stokes Re 2000 M 0.3, far field at rest, HLLC, SSP-RK3",
+            "unit": UNIT, "vars": ["rho", "rhou", "rhov", "rhoE"], "cases": cases}
 
 
 def adjoint_run(stream, steps=200, k_ckpt=20, n_fd=4):
@@ -532,6 +613,7 @@ def main():
     ap.add_argument("--no-error-run", action="store_true")
     ap.add_argument("--no-adjoint", action="store_true")
     ap.add_argument("--no-p5", action="store_true")
+    ap.add_argument("--no-mixed", action="store_true")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

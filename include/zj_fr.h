@@ -136,6 +136,12 @@ int64_t zj_state_size(const zj_solver* s);            /* E * n_sp * 4 */
 /* ---- initial condition (FRSolver::setInitialCondition, fr_solver.cpp:268-299)
  * A C ABI cannot carry std::function: fetch the physical coordinates of the
  * solution points, evaluate the initial state on the host, then set it. */
+/* Meshes with triangles (physics mode): every element has (P+1)^2 state slots;
+ * a triangle uses the first (P+1)(P+2)/2 of them (the reference's collapsed
+ * Gauss-Legendre points, SolutionPoints::getTriangle, basis.cpp:391-416) and
+ * its other slots are neither read nor written.  kinds[e] = zj_elem_type. */
+zj_status zj_element_kinds(const zj_solver* s, int32_t* kinds);
+int zj_num_triangle_points(const zj_solver* s);
 zj_status zj_solution_point_coords(const zj_solver* s, double* xy /* [E][n_sp][2] */);
 /* copyToDevice / copyToHost (fr_solver.cpp:835-871), host buffers.  Setting
  * the state resets time and iteration like setInitialCondition. */

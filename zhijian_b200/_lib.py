@@ -92,6 +92,8 @@ def lib():
         "zj_iteration": (ip, [vp]),
         "zj_set_stream": (ip, [vp, vp]),
         "zj_get_stream": (vp, [vp]),
+        "zj_element_kinds": (ip, [vp, C.POINTER(C.c_int32)]),
+        "zj_num_triangle_points": (ip, [vp]),
         "zj_restart_write": (ip, [vp, C.c_char_p]),
         "zj_restart_read": (ip, [vp, C.c_char_p]),
         "zj_gmsh_read": (ip, [C.c_char_p, C.POINTER(vp)]),

@@ -65,6 +65,16 @@ struct zj_solver {
     float* fOps = nullptr;
     float* fBC = nullptr;
     float4* fNrm = nullptr;
+    // meshes with triangles: element lists per kind, triangle operators
+    int64_t n_tri = 0, n_quad = 0;
+    int nt = 0;                     // triangle solution points
+    int grid_q = 0, grid_t = 0;
+    int32_t* dElistQ = nullptr;
+    int32_t* dElistT = nullptr;
+    double* dTriOps = nullptr;
+    float* fTriOps = nullptr;
+    int8_t* dEtype = nullptr;
+    std::vector<int8_t> etype;
     // differentiation: dual-number geometry and traces (Jacobian-vector
     // products) and adjoint scratch, allocated on first use
     size_t n_jinv = 0, n_j = 0, n_ops = 0, n_bcd = 0, n_nrm = 0;
@@ -141,6 +151,9 @@ void free_all(zj_solver* s) {
     for (auto pp : fs) { if (*pp) cudaFree(*pp); *pp = nullptr; }
     if (s->fNrm) cudaFree(s->fNrm);
     s->fNrm = nullptr;
+    void* ts[] = {s->dElistQ, s->dElistT, s->dTriOps, s->fTriOps, s->dEtype};
+    for (void* p : ts) if (p) cudaFree(p);
+    s->dElistQ = s->dElistT = nullptr; s->dTriOps = nullptr; s->fTriOps = nullptr; s->dEtype = nullptr;
     void* xs[] = {s->xJinv, s->xJ, s->xOps, s->xBC, s->xNrm, s->xT, s->xTQ, s->xPart, s->aDb, s->aTb,
                   s->aDUb, s->aW, s->aS1, s->aS2, s->aB0, s->aB1, s->aB2, s->aR, s->aJV, s->aZero,
                   s->aDot, s->aScal, s->aRePart};
@@ -177,6 +190,10 @@ template <typename T> T* tbuf(const zj_solver* s, int i);
 template <> double* tbuf<double>(const zj_solver* s, int i) { return s->dT[i]; }
 template <> float* tbuf<float>(const zj_solver* s, int i) { return s->fT[i]; }
 
+template <typename T> const T* tri_ops(const zj_solver* s);
+template <> const double* tri_ops<double>(const zj_solver* s) { return s->dTriOps; }
+template <> const float* tri_ops<float>(const zj_solver* s) { return s->fTriOps; }
+
 template <typename T> StageArgsT<T> base_args(const zj_solver* s);
 template <> StageArgsT<double> base_args<double>(const zj_solver* s) {
     StageArgsT<double> a{};
@@ -210,10 +227,29 @@ cudaError_t launch_stage(const zj_solver* s, const StageArgsT<T>& a) {
     if constexpr (sizeof(T) == 8) {
         if (s->prm.compat) return launch_compat_stage(s->P, a, s->stream, nullptr);
     }
-    if (!is_ns(s)) return launch_phys_stage(s->P, s->prm.riemann, a, s->stream);
-    cudaError_t e = launch_ns_grad(s->P, a, s->stream);
-    if (e != cudaSuccess) return e;
-    return launch_ns_stage(s->P, s->prm.riemann, a, s->stream);
+    if (s->n_tri == 0) {
+        if (!is_ns(s)) return launch_phys_stage(s->P, s->prm.riemann, a, s->stream);
+        cudaError_t e = launch_ns_grad(s->P, a, s->stream);
+        if (e != cudaSuccess) return e;
+        return launch_ns_stage(s->P, s->prm.riemann, a, s->stream);
+    }
+    // quads and triangles: every gradient trace before any stage (a face's
+    // neighbour may be of the other kind); the triangles' CTAs write their
+    // partial sums after the quads'
+    StageArgsT<T> q = a, t = a;
+    q.elist = s->dElistQ; q.n_list = s->n_quad;
+    t.ops = tri_ops<T>(s);
+    t.partials = a.partials ? a.partials + s->grid_q : nullptr;
+    cudaError_t e = cudaSuccess;
+    if (is_ns(s)) {
+        if (s->n_quad > 0) e = launch_ns_grad(s->P, q, s->stream);
+        if (e == cudaSuccess) e = launch_tri(1, s->P, s->prm.riemann, true, t, s->dElistT, s->n_tri, s->stream);
+        if (e == cudaSuccess && s->n_quad > 0) e = launch_ns_stage(s->P, s->prm.riemann, q, s->stream);
+    } else if (s->n_quad > 0) {
+        e = launch_phys_stage(s->P, s->prm.riemann, q, s->stream);
+    }
+    if (e == cudaSuccess) e = launch_tri(2, s->P, s->prm.riemann, is_ns(s), t, s->dElistT, s->n_tri, s->stream);
+    return e;
 }
 
 // Traces of U into Tb in the handle's mode (physics mode adds the ghost rows).
@@ -225,7 +261,16 @@ cudaError_t launch_trace_any(const zj_solver* s, const double* U, T* Tb) {
     StageArgsT<T> a = stage_args<T>(s);
     a.U = U;
     a.Tout = Tb;
-    return launch_phys_traces(s->P, a, s->stream);
+    if (s->n_tri == 0) return launch_phys_traces(s->P, a, s->stream);
+    cudaError_t e = cudaSuccess;
+    if (s->n_quad > 0) {
+        StageArgsT<T> q = a;
+        q.elist = s->dElistQ; q.n_list = s->n_quad;
+        e = launch_phys_traces(s->P, q, s->stream);
+    }
+    if (e != cudaSuccess) return e;
+    a.ops = tri_ops<T>(s);
+    return launch_tri(0, s->P, s->prm.riemann, is_ns(s), a, s->dElistT, s->n_tri, s->stream);
 }
 
 template <typename T>
@@ -316,9 +361,29 @@ zj_status zj_solver_create(const zj_mesh_desc* mesh, const zj_params* params, zj
     }
     if (params->compat) build_operators_compat(s->P, s->ops);
     else build_operators_vcjh(s->P, params->flux_type, s->ops);
+    s->n_tri = s->mesh.n_tri;
+    s->n_quad = s->E - s->n_tri;
+    TriOperators tri;
+    std::vector<double> tri_packed;
+    if (s->n_tri > 0) {
+        if (params->compat) {
+            delete s;
+            return fail(nullptr, ZJ_ERR_UNSUPPORTED, "triangles need physics mode (compat off): the reference's residual is quad-only");
+        }
+        if (!build_operators_tri(s->P, params->flux_type, tri, msg)) { delete s; return fail(nullptr, ZJ_ERR_ARG, msg); }
+        s->nt = tri.nt;
+        tri_packed = tri.Dr;
+        tri_packed.insert(tri_packed.end(), tri.Ds.begin(), tri.Ds.end());
+        tri_packed.insert(tri_packed.end(), tri.L.begin(), tri.L.end());
+        tri_packed.insert(tri_packed.end(), tri.Phi.begin(), tri.Phi.end());
+    }
+    s->etype = s->mesh.etype;
     std::vector<double> J, Jinv, bc, nrm, area, packed;
     std::vector<EdgeRec> rec;
-    if (!build_metrics(s->mesh, s->ops, J, Jinv, msg)) { delete s; return fail(nullptr, ZJ_ERR_ARG, msg); }
+    if (!build_metrics(s->mesh, s->ops, J, Jinv, msg, s->n_tri ? &tri : nullptr)) {
+        delete s;
+        return fail(nullptr, ZJ_ERR_ARG, msg);
+    }
     build_bc_data(s->mesh, params, bc);
     build_edge_records(s->mesh, rec, nrm);
     element_areas(s->mesh, area);
@@ -331,6 +396,14 @@ zj_status zj_solver_create(const zj_mesh_desc* mesh, const zj_params* params, zj
     // element traces, then one ghost row per boundary slot (physics mode)
     s->trace_n = ((size_t)s->E * 4 + (size_t)s->mesh.n_bnd_faces) * s->n1 * 4;
     s->grid = stage_grid(s->P, s->E);
+    std::vector<int32_t> listq, listt;
+    if (s->n_tri > 0) {
+        for (int64_t e2 = 0; e2 < s->E; ++e2)
+            (s->etype[(size_t)e2] == ZJ_ELEM_TRI ? listt : listq).push_back((int32_t)e2);
+        s->grid_q = quad_grid(s->P, s->n_quad);
+        s->grid_t = tri_grid(s->P, s->n_tri);
+        s->grid = s->grid_q + s->grid_t;
+    }
     s->scratch_n = 148 * 8;
     cudaError_t e = cudaSuccess;
 #define ZJ_ALLOC(ptr, n)                                                     \
@@ -363,6 +436,13 @@ zj_status zj_solver_create(const zj_mesh_desc* mesh, const zj_params* params, zj
     ZJ_ALLOC(s->dFlag, 1);
     ZJ_ALLOC(s->dEdges, rec.size());
     ZJ_ALLOC(s->dNrm, rec.size());
+    if (s->n_tri > 0) {
+        ZJ_ALLOC(s->dElistQ, listq.size());
+        ZJ_ALLOC(s->dElistT, listt.size());
+        ZJ_ALLOC(s->dTriOps, tri_packed.size());
+        ZJ_ALLOC(s->dEtype, (size_t)s->E);
+        if (s->mixed) { ZJ_ALLOC(s->fTriOps, tri_packed.size()); }
+    }
 #undef ZJ_ALLOC
     if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&s->own, cudaStreamNonBlocking);
     if (e == cudaSuccess) e = cudaMemcpy(s->dJinv, Jinv.data(), Jinv.size() * 8, cudaMemcpyHostToDevice);
@@ -384,7 +464,21 @@ zj_status zj_solver_create(const zj_mesh_desc* mesh, const zj_params* params, zj
         if (e == cudaSuccess) e = cudaMemcpy(s->fBC, fBC.data(), fBC.size() * 4, cudaMemcpyHostToDevice);
         if (e == cudaSuccess) e = cudaMemcpy(s->fNrm, fNrm.data(), fNrm.size() * 4, cudaMemcpyHostToDevice);
     }
-    if (e == cudaSuccess) e = cudaMemset(s->dU[0], 0, s->state_n * 8);
+    if (s->n_tri > 0) {
+        if (e == cudaSuccess && !listq.empty())
+            e = cudaMemcpy(s->dElistQ, listq.data(), listq.size() * 4, cudaMemcpyHostToDevice);
+        if (e == cudaSuccess) e = cudaMemcpy(s->dElistT, listt.data(), listt.size() * 4, cudaMemcpyHostToDevice);
+        if (e == cudaSuccess)
+            e = cudaMemcpy(s->dTriOps, tri_packed.data(), tri_packed.size() * 8, cudaMemcpyHostToDevice);
+        if (e == cudaSuccess) e = cudaMemcpy(s->dEtype, s->etype.data(), (size_t)s->E, cudaMemcpyHostToDevice);
+        if (e == cudaSuccess && s->mixed) {
+            const std::vector<float> f = narrow<float>(tri_packed);
+            e = cudaMemcpy(s->fTriOps, f.data(), f.size() * 4, cudaMemcpyHostToDevice);
+        }
+    }
+    // every state buffer starts at zero: slots no kernel writes (a
+    // triangle's unused ones) stay finite through the buffer rotation
+    for (int i = 0; i < 3 && e == cudaSuccess; ++i) e = cudaMemset(s->dU[i], 0, s->state_n * 8);
     if (e == cudaSuccess) e = cudaMemset(s->dScal, 0, 8 * 8);
     if (e == cudaSuccess) e = cudaDeviceSynchronize();
     if (e != cudaSuccess) {
@@ -415,10 +509,21 @@ int zj_iteration(const zj_solver* s) { return s ? s->iter : 0; }
 zj_status zj_solution_point_coords(const zj_solver* s, double* xy) {
     if (!s || !xy) return ZJ_ERR_ARG;
     std::vector<double> c;
-    sp_coords(s->mesh, s->ops, c);
+    TriOperators tri;
+    std::string msg;
+    if (s->n_tri > 0 && !build_operators_tri(s->P, s->prm.flux_type, tri, msg)) return fail(const_cast<zj_solver*>(s), ZJ_ERR_ARG, msg);
+    sp_coords(s->mesh, s->ops, c, s->n_tri ? &tri : nullptr);
     std::memcpy(xy, c.data(), c.size() * sizeof(double));
     return ZJ_OK;
 }
+
+zj_status zj_element_kinds(const zj_solver* s, int32_t* kinds) {
+    if (!s || !kinds) return ZJ_ERR_ARG;
+    for (int64_t e = 0; e < s->E; ++e) kinds[e] = s->etype[(size_t)e];
+    return ZJ_OK;
+}
+
+int zj_num_triangle_points(const zj_solver* s) { return s ? ((s->P + 1) * (s->P + 2) / 2) : 0; }
 
 zj_status zj_set_stream(zj_solver* s, void* stream) {
     if (!s) return ZJ_ERR_ARG;
@@ -514,7 +619,8 @@ zj_status zj_residual_norm(zj_solver* s, double* out) {
 zj_status zj_compute_dt(zj_solver* s, double* dt_out) {
     if (!s || !dt_out) return ZJ_ERR_ARG;
     ZJ_CK(s, launch_compute_dt(s->dU[s->cur], s->dH, s->E, s->nsp, s->prm.gamma, s->prm.CFL, s->P,
-                               s->dScratch, s->scratch_n, s->dScal + 2, s->stream), "dt launch");
+                               s->dScratch, s->scratch_n, s->dScal + 2, s->stream, s->dEtype, s->nt),
+          "dt launch");
     double v = 0.0;
     ZJ_CK(s, cudaMemcpyAsync(&v, s->dScal + 2, sizeof(double), cudaMemcpyDeviceToHost, s->stream), "dt copy");
     ZJ_CK(s, cudaStreamSynchronize(s->stream), "dt sync");
@@ -614,6 +720,7 @@ namespace {
 zj_status diff_supported(zj_solver* s) {
     if (s->prm.compat) return fail(s, ZJ_ERR_UNSUPPORTED, "differentiation needs physics mode (compat off)");
     if (s->mixed) return fail(s, ZJ_ERR_UNSUPPORTED, "differentiation runs on the FP64 path (precision fp64)");
+    if (s->n_tri > 0) return fail(s, ZJ_ERR_UNSUPPORTED, "differentiation runs on quadrilateral meshes");
     return ZJ_OK;
 }
 

@@ -410,11 +410,12 @@ __global__ void k_reduce_sum(const double* __restrict__ x, int n, double* out) {
 
 __global__ void k_dt_partial(const double* __restrict__ U, const double* __restrict__ h,
                              long long n_states, int n_sp, double g, double cfl, double cf,
-                             double* partial) {
+                             double* partial, const int8_t* __restrict__ etype, int nt) {
     __shared__ double red[32];
     double m = 1e20;
     for (long long s = (long long)blockIdx.x * blockDim.x + threadIdx.x; s < n_states;
          s += (long long)gridDim.x * blockDim.x) {
+        if (etype && etype[s / n_sp] == ZJ_ELEM_TRI && (int)(s % n_sp) >= nt) continue;   // unused slot
         double q[4];
         load4_nc(U + s * 4, q);
         const double u = q[1] / q[0], v = q[2] / q[0];
@@ -530,12 +531,12 @@ cudaError_t launch_reduce_sum(const double* partials, int n, double* out, cudaSt
 
 cudaError_t launch_compute_dt(const double* U, const double* h, long long n_elem, int n_sp,
                               double gamma, double cfl, int P, double* scratch, int scratch_n,
-                              double* out, cudaStream_t s) {
+                              double* out, cudaStream_t s, const int8_t* etype, int nt) {
     const long long n_states = n_elem * n_sp;
     int blocks = (int)((n_states + 255) / 256);
     if (blocks > scratch_n) blocks = scratch_n;
     if (blocks < 1) blocks = 1;
-    k_dt_partial<<<blocks, 256, 0, s>>>(U, h, n_states, n_sp, gamma, cfl, 2.0 * P + 1.0, scratch);
+    k_dt_partial<<<blocks, 256, 0, s>>>(U, h, n_states, n_sp, gamma, cfl, 2.0 * P + 1.0, scratch, etype, nt);
     cudaError_t err = cudaGetLastError();
     if (err != cudaSuccess) return err;
     k_min_reduce<<<1, 1024, 0, s>>>(scratch, blocks, out);

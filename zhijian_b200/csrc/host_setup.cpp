@@ -222,16 +222,17 @@ const zj_bc_spec* find_bc(const zj_params* p, int tag) {
 // mesh.cpp:159-183
 void face_normal(const HostMesh& m, int e, int lf, double& nx, double& ny, double& len) {
     const int64_t* nd = &m.conn[(size_t)e * m.nn];
+    const int nve = m.nv(e);
     const double* v0 = &m.xy[2 * nd[lf]];
-    const double* v1 = &m.xy[2 * nd[(lf + 1) % 4]];
+    const double* v1 = &m.xy[2 * nd[(lf + 1) % nve]];
     double tx = v1[0] - v0[0], ty = v1[1] - v0[1];
     len = std::sqrt(tx * tx + ty * ty);
     nx = ty / len;
     ny = -tx / len;
     double cx = 0.0, cy = 0.0;
-    for (int i = 0; i < 4; ++i) { cx = cx + m.xy[2 * nd[i]]; cy = cy + m.xy[2 * nd[i] + 1]; }
-    cx = cx / 4.0;
-    cy = cy / 4.0;
+    for (int i = 0; i < nve; ++i) { cx = cx + m.xy[2 * nd[i]]; cy = cy + m.xy[2 * nd[i] + 1]; }
+    cx = cx / (double)nve;
+    cy = cy / (double)nve;
     double fx = (v0[0] + v1[0]) * 0.5, fy = (v0[1] + v1[1]) * 0.5;
     if (nx * (fx - cx) + ny * (fy - cy) < 0) { nx = nx * (-1.0); ny = ny * (-1.0); }
 }
@@ -248,43 +249,57 @@ bool build_mesh(const zj_mesh_desc* d, const zj_params* p, HostMesh& m, std::str
     int order = d->elem_order ? d->elem_order[0] : 1;
     int nn = (order == 1) ? 4 : (order == 2) ? 9 : (order == 4) ? 25 : -1;
     if (nn < 0) { msg = "element order must be 1, 2 or 4"; return false; }
+    m.etype.assign((size_t)d->n_elem, (int8_t)ZJ_ELEM_QUAD);
+    m.n_tri = 0;
     for (int64_t e = 0; e < d->n_elem; ++e) {
-        if (d->elem_type && d->elem_type[e] != ZJ_ELEM_QUAD) {
-            msg = "element " + std::to_string(e) + " is a triangle: only quadrilaterals are supported";
+        const bool tri = d->elem_type && d->elem_type[e] == ZJ_ELEM_TRI;
+        if (d->elem_type && d->elem_type[e] != ZJ_ELEM_TRI && d->elem_type[e] != ZJ_ELEM_QUAD) {
+            msg = "element " + std::to_string(e) + " has an unknown type";
             return false;
         }
         if (d->elem_order && d->elem_order[e] != order) {
             msg = "mixed geometric orders are not supported";
             return false;
         }
-        if (d->conn_offsets[e + 1] - d->conn_offsets[e] != nn) {
+        if (tri && order != 1) {
+            msg = "element " + std::to_string(e) + " is a curved triangle: only straight-sided triangles are supported";
+            return false;
+        }
+        if (d->conn_offsets[e + 1] - d->conn_offsets[e] != (tri ? 3 : nn)) {
             msg = "element " + std::to_string(e) + " has a node count that does not match its order";
             return false;
         }
+        if (tri) { m.etype[(size_t)e] = (int8_t)ZJ_ELEM_TRI; ++m.n_tri; }
     }
     m.nn = nn;
     m.order = order;
     m.xy.assign(d->xy, d->xy + 2 * d->n_nodes);
-    m.conn.resize((size_t)m.n_elem * nn);
-    for (int64_t e = 0; e < m.n_elem; ++e)
-        for (int k = 0; k < nn; ++k) {
+    m.conn.assign((size_t)m.n_elem * nn, -1);
+    for (int64_t e = 0; e < m.n_elem; ++e) {
+        const int k_n = (int)(d->conn_offsets[e + 1] - d->conn_offsets[e]);
+        for (int k = 0; k < k_n; ++k) {
             int64_t v = d->conn[d->conn_offsets[e] + k];
             if (v < 0 || v >= m.n_nodes) { msg = "element " + std::to_string(e) + " references a bad node"; return false; }
             m.conn[(size_t)e * nn + k] = v;
         }
+    }
     for (double v : m.xy)
         if (!std::isfinite(v)) { msg = "non-finite node coordinate"; return false; }
 
     // Edge map keyed by the sorted vertex pair, first-seen element is the
     // left side (mesh.cpp:18-83).
-    std::vector<EdgeKey> ent((size_t)m.n_elem * 4);
-    for (int64_t e = 0; e < m.n_elem; ++e)
-        for (int l = 0; l < 4; ++l) {
-            int64_t v0 = m.conn[(size_t)e * nn + l], v1 = m.conn[(size_t)e * nn + (l + 1) % 4];
-            EdgeKey& k = ent[(size_t)e * 4 + l];
+    std::vector<EdgeKey> ent;
+    ent.reserve((size_t)m.n_elem * 4);
+    for (int64_t e = 0; e < m.n_elem; ++e) {
+        const int nve = m.nv(e);
+        for (int l = 0; l < nve; ++l) {
+            int64_t v0 = m.conn[(size_t)e * nn + l], v1 = m.conn[(size_t)e * nn + (l + 1) % nve];
+            EdgeKey k;
             k.a = std::min(v0, v1); k.b = std::max(v0, v1); k.seq = e * 4 + l;
             k.e = (int32_t)e; k.l = l;
+            ent.push_back(k);
         }
+    }
     std::sort(ent.begin(), ent.end(), key_less);
     std::vector<EdgeKey> bk;
     for (int64_t i = 0; i < d->n_bnd_edges; ++i) {
@@ -399,12 +414,37 @@ int shape(int order, double xi, double eta, double* N, double* dNx, double* dNe)
 }
 }  // namespace
 
+// Affine map of a triangle: x_r = (v1 - v0)/2, x_s = (v2 - v0)/2.
+static void tri_jacobian(const HostMesh& m, int64_t e, double& a, double& b, double& c, double& d) {
+    const int64_t* nd = &m.conn[(size_t)e * m.nn];
+    const double *p0 = &m.xy[2 * nd[0]], *p1 = &m.xy[2 * nd[1]], *p2 = &m.xy[2 * nd[2]];
+    a = 0.5 * (p1[0] - p0[0]); b = 0.5 * (p2[0] - p0[0]);   // x_r, x_s
+    c = 0.5 * (p1[1] - p0[1]); d = 0.5 * (p2[1] - p0[1]);   // y_r, y_s
+}
+
 bool build_metrics(const HostMesh& m, const Operators1D& ops, std::vector<double>& J,
-                   std::vector<double>& Jinv, std::string& msg) {
+                   std::vector<double>& Jinv, std::string& msg, const TriOperators* tri) {
     const int n1 = ops.n1, nsp = n1 * n1;
     J.assign((size_t)m.n_elem * nsp, 0.0);
     Jinv.assign((size_t)m.n_elem * nsp * 4, 0.0);
     for (int64_t e = 0; e < m.n_elem; ++e) {
+        if (m.etype[(size_t)e] == ZJ_ELEM_TRI) {
+            if (!tri) { msg = "triangle without triangle operators"; return false; }
+            double a, b, c, dd;
+            tri_jacobian(m, e, a, b, c, dd);
+            const double Jd = a * dd - b * c;
+            if (!(Jd > 0.0) || !std::isfinite(Jd)) {
+                msg = "element " + std::to_string(e) + " has a non-positive Jacobian (check node order: CCW)";
+                return false;
+            }
+            const double inv = 1.0 / Jd;
+            for (int sp = 0; sp < tri->nt; ++sp) {
+                J[(size_t)e * nsp + sp] = Jd;
+                double* Ji = &Jinv[((size_t)e * nsp + sp) * 4];
+                Ji[0] = dd * inv; Ji[1] = -b * inv; Ji[2] = -c * inv; Ji[3] = a * inv;
+            }
+            continue;
+        }
         const int64_t* nd = &m.conn[(size_t)e * m.nn];
         for (int sp = 0; sp < nsp; ++sp) {
             double N[25], dNx[25], dNe[25];
@@ -428,11 +468,22 @@ bool build_metrics(const HostMesh& m, const Operators1D& ops, std::vector<double
     return true;
 }
 
-void sp_coords(const HostMesh& m, const Operators1D& ops, std::vector<double>& out) {
+void sp_coords(const HostMesh& m, const Operators1D& ops, std::vector<double>& out, const TriOperators* tri) {
     const int n1 = ops.n1, nsp = n1 * n1;
     out.assign((size_t)m.n_elem * nsp * 2, 0.0);
     for (int64_t e = 0; e < m.n_elem; ++e) {
         const int64_t* nd = &m.conn[(size_t)e * m.nn];
+        if (m.etype[(size_t)e] == ZJ_ELEM_TRI) {
+            if (!tri) continue;
+            const double *p0 = &m.xy[2 * nd[0]], *p1 = &m.xy[2 * nd[1]], *p2 = &m.xy[2 * nd[2]];
+            for (int sp = 0; sp < tri->nt; ++sp) {
+                const double r = tri->r[sp], s = tri->s[sp];
+                const double w0 = -0.5 * (r + s), w1 = 0.5 * (1.0 + r), w2 = 0.5 * (1.0 + s);
+                out[((size_t)e * nsp + sp) * 2] = w0 * p0[0] + w1 * p1[0] + w2 * p2[0];
+                out[((size_t)e * nsp + sp) * 2 + 1] = w0 * p0[1] + w1 * p1[1] + w2 * p2[1];
+            }
+            continue;
+        }
         for (int sp = 0; sp < nsp; ++sp) {
             double N[25], dNx[25], dNe[25];
             int n = shape(m.order, ops.pts[sp % n1], ops.pts[sp / n1], N, dNx, dNe);
@@ -449,8 +500,10 @@ void element_areas(const HostMesh& m, std::vector<double>& area) {
     area.assign((size_t)m.n_elem, 0.0);
     for (int64_t e = 0; e < m.n_elem; ++e) {
         const int64_t* nd = &m.conn[(size_t)e * m.nn];
-        const double *p0 = &m.xy[2 * nd[0]], *p1 = &m.xy[2 * nd[1]], *p2 = &m.xy[2 * nd[2]], *p3 = &m.xy[2 * nd[3]];
+        const double *p0 = &m.xy[2 * nd[0]], *p1 = &m.xy[2 * nd[1]], *p2 = &m.xy[2 * nd[2]];
         double a1 = 0.5 * std::fabs((p1[0] - p0[0]) * (p2[1] - p0[1]) - (p2[0] - p0[0]) * (p1[1] - p0[1]));
+        if (m.etype[(size_t)e] == ZJ_ELEM_TRI) { area[(size_t)e] = a1; continue; }
+        const double* p3 = &m.xy[2 * nd[3]];
         double a2 = 0.5 * std::fabs((p2[0] - p0[0]) * (p3[1] - p0[1]) - (p3[0] - p0[0]) * (p2[1] - p0[1]));
         area[(size_t)e] = a1 + a2;
     }

@@ -133,8 +133,8 @@ k_ns_grad(const StageArgsT<T> a) {
     const int tid = threadIdx.x;
     for (int t = tid; t < S::NOPS; t += blockDim.x) sOps[t] = a.ops[t];
     const int el = tid / TPE, k = tid - el * TPE;
-    const long long e = (long long)blockIdx.x * EB + el;
-    const bool valid = (el < EB) && (e < a.n_elem);
+    bool valid;
+    const long long e = block_element(a, EB, el, valid);
     const bool is_sp = valid && k < NSP, is_fp = valid && k < NFT;
     const int edge = k / N1, fp = k - edge * N1;
     const int i = k % N1, j = k / N1;
@@ -204,8 +204,8 @@ k_ns_stage(const StageArgsT<T> a) {
     const int tid = threadIdx.x;
     for (int t = tid; t < S::NOPS; t += blockDim.x) sOps[t] = a.ops[t];
     const int el = tid / TPE, k = tid - el * TPE;
-    const long long e = (long long)blockIdx.x * EB + el;
-    const bool valid = (el < EB) && (e < a.n_elem);
+    bool valid;
+    const long long e = block_element(a, EB, el, valid);
     const bool is_sp = valid && k < NSP, is_fp = valid && k < NFT;
     const T g = T(a.gamma), Re = reynolds(a), Pr = T(a.Pr);
     const int edge = k / N1, fp = k - edge * N1;
@@ -401,7 +401,7 @@ k_ns_stage(const StageArgsT<T> a) {
 template <int P, typename T>
 cudaError_t ns_grad_t(const StageArgsT<T>& a, cudaStream_t s) {
     using S = Shape<P, EbDiv<T>::value>;
-    const long long grid = (a.n_elem + S::EB - 1) / S::EB;
+    const long long grid = ((a.elist ? a.n_list : a.n_elem) + S::EB - 1) / S::EB;
     if (grid <= 0) return cudaSuccess;
     static bool set = false;
     if (!set) { prefer_shared(k_ns_grad<P, T>); set = true; }
@@ -412,7 +412,7 @@ cudaError_t ns_grad_t(const StageArgsT<T>& a, cudaStream_t s) {
 template <int P, int RIEM, typename T>
 cudaError_t ns_stage_t(const StageArgsT<T>& a, cudaStream_t s) {
     using S = Shape<P, EbDiv<T>::value>;
-    const long long grid = (a.n_elem + S::EB - 1) / S::EB;
+    const long long grid = ((a.elist ? a.n_list : a.n_elem) + S::EB - 1) / S::EB;
     if (grid <= 0) return cudaSuccess;
     static bool set = false;
     if (!set) { prefer_shared(k_ns_stage<P, RIEM, T>); set = true; }

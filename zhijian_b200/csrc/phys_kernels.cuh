@@ -61,6 +61,19 @@ struct Tiles {
     static_assert(kD || (FS % 4 == 0 && DS % 4 == 0 && QS % 4 == 0), "16-byte float rows");
 };
 
+// Element of thread group el of this CTA: through the element list of a
+// mesh with several element kinds, else the CTA's contiguous block.
+template <typename T>
+__device__ __forceinline__ long long block_element(const StageArgsT<T>& a, int EB, int el, bool& valid) {
+    const long long g = (long long)blockIdx.x * EB + el;
+    if (a.elist) {
+        valid = (el < EB) && (g < a.n_list);
+        return valid ? (long long)a.elist[g] : 0;
+    }
+    valid = (el < EB) && (g < a.n_elem);
+    return g;
+}
+
 // Boundary ghost states live in extra rows of every trace buffer, after the
 // E*4 element edges: row E*4 + slot of boundary slot `slot`, stored at the
 // mirrored point n1-1-fp, so a boundary edge loads its ghost exactly like an
@@ -203,8 +216,8 @@ k_phys_stage(const StageArgsT<T> a) {
     for (int i = tid; i < S::NOPS; i += blockDim.x) sOps[i] = a.ops[i];
 
     const int el = tid / TPE, k = tid - el * TPE;
-    const long long e = (long long)blockIdx.x * EB + el;
-    const bool valid = (el < EB) && (e < a.n_elem);
+    bool valid;
+    const long long e = block_element(a, EB, el, valid);
     const bool is_sp = valid && k < NSP;
     const bool is_fp = valid && k < NFT;
     const T g = T(a.gamma);
@@ -383,8 +396,8 @@ k_phys_traces(const StageArgsT<T> a) {
     const int tid = threadIdx.x;
     for (int t = tid; t < S::NOPS; t += blockDim.x) sOps[t] = a.ops[t];
     const int el = tid / TPE, k = tid - el * TPE;
-    const long long e = (long long)blockIdx.x * EB + el;
-    const bool valid = (el < EB) && (e < a.n_elem);
+    bool valid;
+    const long long e = block_element(a, EB, el, valid);
     constexpr bool kRef = UsesRef<T>::value;
     T ue[4] = {T(0), T(0), T(0), T(0)};
     if (kRef && valid) load_state(a.U + e * NSP * 4, ue);
@@ -425,7 +438,7 @@ void prefer_shared(K kernel) {
 template <int P, int RIEM, typename T>
 cudaError_t phys_stage_t(const StageArgsT<T>& a, cudaStream_t s) {
     using S = Shape<P, EbDiv<T>::value>;
-    const long long grid = (a.n_elem + S::EB - 1) / S::EB;
+    const long long grid = ((a.elist ? a.n_list : a.n_elem) + S::EB - 1) / S::EB;
     if (grid <= 0) return cudaSuccess;
     static bool carveout_set = false;
     if (!carveout_set) { prefer_shared(k_phys_stage<P, RIEM, T>); carveout_set = true; }
@@ -446,7 +459,7 @@ cudaError_t phys_stage_p(int riemann, const StageArgsT<T>& a, cudaStream_t s) {
 template <int P, typename T>
 cudaError_t phys_traces_t(const StageArgsT<T>& a, cudaStream_t s) {
     using S = Shape<P, EbDiv<T>::value>;
-    const long long grid = (a.n_elem + S::EB - 1) / S::EB;
+    const long long grid = ((a.elist ? a.n_list : a.n_elem) + S::EB - 1) / S::EB;
     if (grid <= 0) return cudaSuccess;
     k_phys_traces<P, T><<<(unsigned)grid, S::THREADS, 0, s>>>(a);
     return cudaGetLastError();

@@ -54,12 +54,28 @@ double lagrange_eval(const std::vector<double>& nodes, int j, double x);
 double lagrange_deriv(const std::vector<double>& nodes, int j, double x);
 void gauss_legendre(int n, std::vector<double>& x, std::vector<double>& w);
 
-// Topology and geometry of a quad mesh, built on the host once.
+// FR operators of the straight-sided triangle (tri_setup.cpp), nt = (P+1)(P+2)/2
+// solution points, 3 (P+1) flux points (edge-major, counter-clockwise).
+struct TriOperators {
+    int P = 0, n1 = 0, nt = 0;
+    std::vector<double> r, s;       // solution points on the reference triangle
+    std::vector<double> Dr, Ds;     // [nt][nt]
+    std::vector<double> L;          // [3 n1][nt] interpolation to the flux points
+    std::vector<double> Phi;        // [nt][3 n1] correction fields at the solution points
+    std::vector<double> w;          // quadrature weights of the solution points
+};
+bool build_operators_tri(int P, int flux_type, TriOperators& t, std::string& msg);
+double vcjh_c(int P, int flux_type);
+
+// Topology and geometry of a quad (or quad/triangle) mesh, built on the host once.
 struct HostMesh {
     int64_t n_nodes = 0, n_elem = 0, n_faces = 0;
-    int nn = 4, order = 1;                 // nodes per element, geometric order
+    int nn = 4, order = 1;                 // node stride per element, geometric order
     std::vector<double> xy;                // [n_nodes][2]
-    std::vector<int64_t> conn;             // [E][nn]
+    std::vector<int64_t> conn;             // [E][nn] (a triangle's 4th entry is -1)
+    std::vector<int8_t> etype;             // [E] ZJ_ELEM_TRI / ZJ_ELEM_QUAD
+    int64_t n_tri = 0;
+    int nv(int64_t e) const { return etype[(size_t)e] == ZJ_ELEM_TRI ? 3 : 4; }
     // faces in the reference order (sorted vertex pair)
     std::vector<int32_t> fle, fll, fre, frl, fbct, ftag, fslot;
     std::vector<double> fnx, fny, flen;
@@ -74,9 +90,12 @@ bool build_mesh(const zj_mesh_desc* d, const zj_params* p, HostMesh& m, std::str
 
 // Metric terms at the solution points, [E][n_sp] J and [E][n_sp][4] Jinv =
 // (xi_x, xi_y, eta_x, eta_y), as fr_solver.cpp:85-129.
+// Triangles (tri != NULL) fill the first nt of their (P+1)^2 slots with the
+// constant metric terms of the affine map x = -(r+s)/2 v0 + (1+r)/2 v1 + (1+s)/2 v2.
 bool build_metrics(const HostMesh& m, const Operators1D& ops, std::vector<double>& J,
-                   std::vector<double>& Jinv, std::string& msg);
-void sp_coords(const HostMesh& m, const Operators1D& ops, std::vector<double>& xy);
+                   std::vector<double>& Jinv, std::string& msg, const TriOperators* tri = nullptr);
+void sp_coords(const HostMesh& m, const Operators1D& ops, std::vector<double>& xy,
+               const TriOperators* tri = nullptr);
 void element_areas(const HostMesh& m, std::vector<double>& area);
 
 // Boundary data, 8 doubles per boundary slot (fr_solver.cpp:432-482).

@@ -41,6 +41,10 @@ struct StageArgsT {
     const T* TQ;            // gradient traces of U, [E][4 edges][n1][8] = (dU/dx, dU/dy)
     T* TQout;               // gradient traces written by the gradient launch
     double Re, Pr;
+    // Element list of a mesh with several element kinds: the launch visits
+    // elist[0..n_list) (NULL: every element 0..n_elem)
+    const int32_t* elist;
+    long long n_list;
     // Jacobian-vector product (T = Dual): tangent of the stage state and of
     // Re in, tangent of the residual out (stage 0)
     const double* dU;
@@ -76,6 +80,16 @@ cudaError_t launch_phys_stage(int P, int riemann, const StageArgsDual& a, cudaSt
 cudaError_t launch_ns_grad(int P, const StageArgsDual& a, cudaStream_t s);
 cudaError_t launch_ns_stage(int P, int riemann, const StageArgsDual& a, cudaStream_t s);
 int dual_grid(int P, long long n_elem);
+// Triangles (tri_kernels.cuh): what = 0 traces (+ ghost rows) of a.U into
+// a.Tout, 1 gradient traces (Navier-Stokes), 2 residual / stage; over the
+// triangle list elist[0..n).  a.ops holds the packed triangle operators.
+cudaError_t launch_tri(int what, int P, int riemann, bool viscous, const StageArgs& a, const int32_t* elist,
+                       long long n, cudaStream_t s);
+cudaError_t launch_tri(int what, int P, int riemann, bool viscous, const StageArgs32& a,
+                       const int32_t* elist, long long n, cudaStream_t s);
+int tri_grid(int P, long long n);
+// Quad CTA count of a launch over n elements.
+int quad_grid(int P, long long n);
 // Elementwise helpers of the differentiation entry points (jvp.cu).
 cudaError_t launch_to_dual(const double* x, Dual* y, long long n, cudaStream_t s);
 cudaError_t launch_lincomb(double* out, double a, const double* x, double b, const double* y,
@@ -124,9 +138,10 @@ int adj_ns_grid(int P, long long n_elem);
 // Deterministic reduction of per-CTA partial sums into out[0].
 cudaError_t launch_reduce_sum(const double* partials, int n, double* out, cudaStream_t s);
 // out[0] = min over states of CFL*h/(ws*(2P+1)); h per element.
+// Triangles (etype[e] == ZJ_ELEM_TRI) count their first nt slots only.
 cudaError_t launch_compute_dt(const double* U, const double* h, long long n_elem, int n_sp,
                               double gamma, double cfl, int P, double* scratch, int scratch_n,
-                              double* out, cudaStream_t s);
+                              double* out, cudaStream_t s, const int8_t* etype = nullptr, int nt = 0);
 // flag[0] = 1 if any value of x[0..n) is NaN/Inf.
 cudaError_t launch_check_finite(const double* x, long long n, int* flag, cudaStream_t s);
 

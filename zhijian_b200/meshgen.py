@@ -54,6 +54,46 @@ class QuadMesh:
         return [(t, L.BC_TYPES[n]) for t, n in sorted(self.tag_names.items())]
 
 
+@dataclasses.dataclass
+class MixedMesh:
+    """Straight-sided quads and triangles: element e has etype[e] (0 triangle,
+    1 quadrilateral) and nodes conn[offsets[e]:offsets[e+1]], counter-clockwise."""
+    xy: np.ndarray            # [n_nodes, 2]
+    etype: np.ndarray         # [n_elem] int32
+    offsets: np.ndarray       # [n_elem + 1] int64
+    conn: np.ndarray          # flat int64
+    bnd: np.ndarray           # [n_bnd, 3] (v0, v1, tag)
+    tag_names: dict
+
+    @property
+    def n_elem(self) -> int:
+        return int(self.etype.shape[0])
+
+    def element(self, e: int) -> np.ndarray:
+        return self.conn[self.offsets[e]:self.offsets[e + 1]]
+
+    def bc_specs(self):
+        return [(t, L.BC_TYPES[n]) for t, n in sorted(self.tag_names.items())]
+
+
+def split_quads(mesh: QuadMesh, fraction: float, seed: int) -> MixedMesh:
+    """Split a seeded fraction of a Q1 quad mesh's elements into two
+    triangles along a random diagonal: per element, in element order, two
+    SplitMix64 draws u, w of the seed: split if u < fraction, along the
+    0-2 diagonal if w < 1/2, else along 1-3."""
+    r = uniform01(seed, 2 * mesh.n_elem).reshape(mesh.n_elem, 2)
+    et, conn, off = [], [], [0]
+    for e, (v0, v1, v2, v3) in enumerate(mesh.conn[:, :4].tolist()):
+        if r[e, 0] < fraction:
+            tris = ((v0, v1, v2), (v0, v2, v3)) if r[e, 1] < 0.5 else ((v0, v1, v3), (v1, v2, v3))
+            for t in tris:
+                et.append(0); conn += list(t); off.append(len(conn))
+        else:
+            et.append(1); conn += [v0, v1, v2, v3]; off.append(len(conn))
+    return MixedMesh(mesh.xy.copy(), np.array(et, np.int32), np.array(off, np.int64),
+                     np.array(conn, np.int64), mesh.bnd.copy(), dict(mesh.tag_names))
+
+
 def structured_quads(nx: int, ny: int, x0: float, x1: float, y0: float, y1: float,
                      jitter: float = 0.0, seed: int = 0,
                      side_tags=(1, 1, 1, 1), tag_names=None) -> QuadMesh:
@@ -104,6 +144,34 @@ def tgv_mesh(n: int = 256, seed: int = 1, jitter: float = 0.15) -> QuadMesh:
     """n x n Q1 quads on [0,pi]^2, interior nodes jittered, slip walls."""
     return structured_quads(n, n, 0.0, math.pi, 0.0, math.pi, jitter, seed,
                             (1, 1, 1, 1), {1: "slipwall"})
+
+
+# Solver keywords of the shear-layer configuration (make_params): Navier-Stokes
+# at Re 2000, Pr 0.72, HLLC, p = 1/(gamma M^2) with M = 0.3.  The far field is
+# at rest (Mach keyword 0: u_inf = v_inf = 0), matching the zero mean velocity
+# of the layer; a far field moving at M = 0.3 drives an inflow against the
+# lower half of the layer and the corners with the slip walls diverge several
+# times sooner.
+SHEAR_LAYER_PARAMS = dict(gamma=1.4, rho_inf=1.0, p_inf=1.0 / (1.4 * 0.09), Mach=0.0, riemann="HLLC",
+                          compat=False, viscous=True, Re=2000.0, Pr=0.72,
+                          bcs=[(1, "slipwall"), (2, "farfield")])
+
+
+def shear_layer_mesh(n: int = 384, seed: int = 3, fraction: float = 0.3) -> MixedMesh:
+    """n x n quads on [0,1]^2 with a seeded 30% split into triangles; slip
+    walls at y = 0, 1 (tag 1), far field at x = 0, 1 (tag 2)."""
+    q = structured_quads(n, n, 0.0, 1.0, 0.0, 1.0, 0.0, 0, (1, 2, 1, 2),
+                         {1: "slipwall", 2: "farfield"})
+    return split_quads(q, fraction, seed)
+
+
+def shear_layer(xy: np.ndarray, gamma: float = 1.4, mach: float = 0.3, delta: float = 0.02) -> np.ndarray:
+    """u = 0.5 tanh((y - 0.5)/delta), v = 0.01 sin(2 pi x), rho = 1,
+    p = 1/(gamma M^2)."""
+    x, y = xy[..., 0], xy[..., 1]
+    u = 0.5 * np.tanh((y - 0.5) / delta)
+    v = 0.01 * np.sin(2.0 * math.pi * x)
+    return prim_to_cons(np.ones_like(x), u, v, np.full_like(x, 1.0 / (gamma * mach * mach)), gamma)
 
 
 def isentropic_vortex(xy: np.ndarray, gamma: float = 1.4, beta: float = 5.0,

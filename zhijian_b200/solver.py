@@ -69,11 +69,18 @@ class FRSolver:
         lib = L.lib()
         self._keep = []
         xy = np.ascontiguousarray(mesh.xy, dtype=np.float64)
-        conn = np.ascontiguousarray(mesh.conn, dtype=np.int64)
-        ne, nn = conn.shape
-        et = np.ones(ne, dtype=np.int32)
-        eo = np.full(ne, {4: 1, 9: 2, 25: 4}[nn], dtype=np.int32)
-        off = (np.arange(ne + 1, dtype=np.int64) * nn)
+        if hasattr(mesh, "offsets"):          # MixedMesh: quads and triangles
+            conn = np.ascontiguousarray(mesh.conn, dtype=np.int64)
+            et = np.ascontiguousarray(mesh.etype, dtype=np.int32)
+            ne = et.shape[0]
+            eo = np.ones(ne, dtype=np.int32)
+            off = np.ascontiguousarray(mesh.offsets, dtype=np.int64)
+        else:
+            conn = np.ascontiguousarray(mesh.conn, dtype=np.int64)
+            ne, nn = conn.shape
+            et = np.ones(ne, dtype=np.int32)
+            eo = np.full(ne, {4: 1, 9: 2, 25: 4}[nn], dtype=np.int32)
+            off = (np.arange(ne + 1, dtype=np.int64) * nn)
         bnd = np.ascontiguousarray(mesh.bnd, dtype=np.int64)
         d = L.MeshDesc()
         d.n_nodes = xy.shape[0]
@@ -188,6 +195,21 @@ class FRSolver:
 
     def set_stream(self, stream_ptr: int):
         self._ck(L.lib().zj_set_stream(self.h, C.c_void_p(stream_ptr)))
+
+    def element_kinds(self) -> np.ndarray:
+        """[E] 0 triangle, 1 quadrilateral."""
+        k = np.zeros(self.n_elem, dtype=np.int32)
+        self._ck(L.lib().zj_element_kinds(self.h, k.ctypes.data_as(C.POINTER(C.c_int32))))
+        return k
+
+    def slot_mask(self) -> np.ndarray:
+        """[E][n_sp] True for the state slots an element uses (a triangle
+        uses its first (P+1)(P+2)/2)."""
+        k = self.element_kinds()
+        nt = L.lib().zj_num_triangle_points(self.h)
+        m = np.ones((self.n_elem, self.n_sp), dtype=bool)
+        m[k == 0, nt:] = False
+        return m
 
     # -- restart files ----------------------------------------------------
     def write_restart(self, path: str):
