@@ -1068,6 +1068,24 @@ void orc_viscous_flux(const double* s, const double* dx, const double* dy, doubl
     Gv[0] = 0.0; Gv[1] = txy; Gv[2] = tyy; Gv[3] = u * txy + v * tyy + k * dTdy;
 }
 
+/* Neumann data of the walls on the common normal viscous flux Fvn of a
+ * boundary face (the conditions the wall classes state,
+ * boundary_condition.hpp:60-67 and 146-155): slip and symmetry walls carry
+ * no shear stress and no heat flux (Fvn keeps tau_nn n), an adiabatic
+ * no-slip wall (T_wall = 0) no heat flux. */
+void orc_wall_viscous_closure(const orc_ctx* c, int bct, int tag, double nx, double ny, double* Fvn) {
+    if (bct == BC_SLIPWALL || bct == BC_SYMMETRY) {
+        double tnn = Fvn[1] * nx + Fvn[2] * ny;
+        Fvn[1] = tnn * nx;
+        Fvn[2] = tnn * ny;
+        Fvn[3] = 0.0;
+    } else if (bct == BC_WALL) {
+        int t = tag > 0 ? tag_slot(c, tag) : -1;
+        double Tw = (t >= 0) ? c->tag_Tw[t] : 0.0;
+        if (!(Tw > 0)) Fvn[3] = 0.0;
+    }
+}
+
 void orc_rhs_phys(orc_ctx* c, const double* U, double* R) {
     const int nsp = c->nsp, n1 = c->n1, nfp = c->nfp;
     const int64_t ne = c->n_elem, nf = c->n_faces;
@@ -1201,7 +1219,8 @@ void orc_rhs_phys(orc_ctx* c, const double* U, double* R) {
             if (c->viscous) {
                 /* BR2Scheme::commonFlux (navierstokes.hpp:177-204): average state
                  * and gradients; boundaries copy the interior gradient
-                 * (BoundaryCondition::ghostGradient) */
+                 * (BoundaryCondition::ghostGradient), walls impose their
+                 * Neumann data */
                 const double* QL = Qfp + (lo / 4) * 8;
                 const double* QR = (ro >= 0) ? Qfp + (ro / 4) * 8 : QL;
                 double Ua[4], dxa[4], dya[4], Fv[4], Gv[4];
@@ -1211,7 +1230,10 @@ void orc_rhs_phys(orc_ctx* c, const double* U, double* R) {
                     dya[v] = 0.5 * (QL[4 + v] + QR[4 + v]);
                 }
                 orc_viscous_flux(Ua, dxa, dya, g, c->Re, c->Pr, Fv, Gv);
-                for (int v = 0; v < 4; ++v) Fc[v] -= Fv[v] * nx + Gv[v] * ny;
+                double Fvn[4];
+                for (int v = 0; v < 4; ++v) Fvn[v] = Fv[v] * nx + Gv[v] * ny;
+                if (re < 0) orc_wall_viscous_closure(c, c->fbct[f], c->ftag[f], nx, ny, Fvn);
+                for (int v = 0; v < 4; ++v) Fc[v] -= Fvn[v];
             }
             for (int v = 0; v < 4; ++v) c->Fdiff[lo + v] = s * Fc[v] - FnD[lo + v];
             if (ro >= 0)

@@ -83,6 +83,9 @@ void orc_riemann_point(int which, const double* UL, const double* UR, double nx,
                        double g, double* F);
 void orc_ghost_point(const orc_ctx* c, int bc_type, int tag, const double* Ui, double nx,
                      double ny, double* Ug);
+/* the walls' Neumann data on a boundary face's common normal viscous flux */
+void orc_wall_viscous_closure(const orc_ctx* c, int bc_type, int tag, double nx, double ny,
+                              double* Fvn);
 
 #ifdef __cplusplus
 }

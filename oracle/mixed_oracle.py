@@ -356,7 +356,10 @@ class MixedOracle:
                             Qn = (TQ[e2][0][l2][n1 - 1 - fp], TQ[e2][1][l2][n1 - 1 - fp])
                         Fv, Gv = viscous_point(0.5 * (UL + UR), 0.5 * (Qo[0] + Qn[0]), 0.5 * (Qo[1] + Qn[1]),
                                                g, self.Re, self.Pr)
-                        Fc = Fc - (Fv * n[0] + Gv * n[1])
+                        Fvn = Fv * n[0] + Gv * n[1]
+                        if nb[0] == "bnd":
+                            Fvn = self._ctx.wall_closure(nb[1], nb[2], n[0], n[1], Fvn)
+                        Fc = Fc - Fvn
                     if nv == 3:
                         sf = ln / TRI_REFLEN[l]
                         Fn = trF[l][fp] * TRI_NREF[l, 0] + trG[l][fp] * TRI_NREF[l, 1]

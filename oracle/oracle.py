@@ -83,6 +83,7 @@ def lib():
         h.orc_step_phys.argtypes = [C.c_void_p, dp, C.c_double, C.c_int, dp]
         h.orc_riemann_point.argtypes = [C.c_int, dp, dp, C.c_double, C.c_double, C.c_double, dp]
         h.orc_ghost_point.argtypes = [C.c_void_p, C.c_int, C.c_int, dp, C.c_double, C.c_double, dp]
+        h.orc_wall_viscous_closure.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_double, C.c_double, dp]
         _lib = h
     return _lib
 
@@ -210,6 +211,13 @@ class Oracle:
         lib().orc_ghost_point(self.c, bc_type, tag, _d(Ui), nx, ny, _d(out))
         return out
 
+    def wall_closure(self, bc_type, tag, nx, ny, Fvn):
+        """The walls' Neumann data applied to a boundary face's common normal
+        viscous flux (orc_wall_viscous_closure)."""
+        out = np.array(Fvn, dtype=np.float64)
+        lib().orc_wall_viscous_closure(self.c, bc_type, tag, nx, ny, _d(out))
+        return out
+
     def sp_coords(self):
         xy = np.empty((self.n_elem, self.nsp, 2))
         lib().orc_sp_coords(self.c, _d(xy))
@@ -248,6 +256,20 @@ def read_ops_bin(path, P):
         n = int(np.prod(shp))
         out[k] = a[o:o + n].reshape(shp)
         o += n
+    return out
+
+
+def read_tri_bin(path, P):
+    """The reference's triangle FROperators as written by ref_cpu "tri"."""
+    n1, nt = P + 1, (P + 1) * (P + 2) // 2
+    a = np.fromfile(path, dtype=np.float64)
+    o, out = 0, {}
+    for k, shp in (("xi", (nt,)), ("eta", (nt,)), ("fp_loc", (3, n1)), ("interp", (3, n1, nt)),
+                   ("diff_xi", (nt, nt)), ("diff_eta", (nt, nt)), ("corr", (3, nt)), ("weights", (nt,))):
+        n = int(np.prod(shp))
+        out[k] = a[o:o + n].reshape(shp)
+        o += n
+    assert o == a.size
     return out
 
 

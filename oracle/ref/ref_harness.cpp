@@ -4,6 +4,7 @@
 // (nothing is copied); output binaries go to oracle/_ref/.  Two builds:
 //   ref_cpu : basis.cpp + mesh.cpp + gmsh_reader.cpp, runs on any host.
 //             "ops P out"            -> FROperators (basis.cpp:464-613)
+//             "tri P out"            -> FROperators on a triangle (basis.cpp:615-668)
 //             "mesh mesh.bin P out"  -> faces, normals (mesh.cpp:18-194) and
 //                                       J/Jinv exactly as fr_solver.cpp:85-129
 //             "gmsh file.msh out"    -> GmshReader::read (gmsh_reader.cpp:161)
@@ -137,6 +138,26 @@ int cmd_ops(int P, const char* out) {
     for (int e = 0; e < 4; ++e)
         for (int fp = 0; fp < n1; ++fp) wr.arr(ops.interpToFlux(e)[fp]);
     for (int e = 0; e < 4; ++e) wr.arr(ops.correctionDeriv()[e]);
+    return 0;
+}
+
+// FROperators on a triangle (basis.cpp:615-668): solution points
+// (SolutionPoints::getTriangle, basis.cpp:391-417), flux-point locations,
+// interpolation, differentiation, correction derivatives, weights.
+int cmd_tri(int P, const char* out) {
+    FROperators ops;
+    ops.init(ElementType::Triangle, P, FluxType::DG);
+    const int nt = ops.numSolutionPoints(), n1 = ops.numFluxPointsPerEdge();
+    Writer wr(out);
+    wr.arr(ops.solutionXi());
+    wr.arr(ops.solutionEta());
+    for (int e = 0; e < 3; ++e) wr.arr(ops.fluxPointLoc()[e]);
+    for (int e = 0; e < 3; ++e)
+        for (int fp = 0; fp < n1; ++fp) wr.arr(ops.interpToFlux(e)[fp]);
+    for (int i = 0; i < nt; ++i) wr.arr(ops.diffXi()[i]);
+    for (int i = 0; i < nt; ++i) wr.arr(ops.diffEta()[i]);
+    for (int e = 0; e < 3; ++e) wr.arr(ops.correctionDeriv()[e]);
+    wr.arr(ops.quadWeights());
     return 0;
 }
 
@@ -305,6 +326,7 @@ int main(int argc, char** argv) {
     if (argc < 2) { std::fprintf(stderr, "usage: see header\n"); return 1; }
     std::string cmd = argv[1];
     if (cmd == "ops" && argc == 4) return cmd_ops(std::atoi(argv[2]), argv[3]);
+    if (cmd == "tri" && argc == 4) return cmd_tri(std::atoi(argv[2]), argv[3]);
     if (cmd == "mesh" && argc == 5) return cmd_mesh(argv[2], std::atoi(argv[3]), argv[4]);
     if (cmd == "gmsh" && argc == 4) return cmd_gmsh(argv[2], argv[3]);
     if (cmd == "phys" && argc == 15) return cmd_phys(argv + 2);

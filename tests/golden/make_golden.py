@@ -119,6 +119,13 @@ def gen_cpu(out):
         for k, v in O.read_ops_bin(f, P).items():
             ops[f"P{P}_{k}"] = v
     np.savez_compressed(os.path.join(out, "ref_operators.npz"), **ops)
+    tri = {}
+    for P in range(1, 6):
+        f = os.path.join(tmp, f"tri{P}.bin")
+        run([O.REF_CPU, "tri", str(P), f])
+        for k, v in O.read_tri_bin(f, P).items():
+            tri[f"P{P}_{k}"] = v
+    np.savez_compressed(os.path.join(out, "ref_triangle.npz"), **tri)
     geo = {}
     for name, mesh, tags, P in (("mixed", mixed_mesh(), mixed_tags(0.9e5), 3),
                                 ("mixed", mixed_mesh(), mixed_tags(0.9e5), 5),

@@ -83,14 +83,13 @@ def test_mixed_tgv_euler_1000_steps(zjlib):
 
 
 def test_mixed_tgv_ns_1000_steps(zjlib):
-    """The Navier-Stokes case of the benchmark (Re 5000), 1000 steps at CFL 0.5.
-    The scheme amplifies perturbations near the slip walls in FP64 too: an
-    FP64 run from the initial state rounded once to FP32 departs from the
-    exact-FP64 run by ~1.3e-6 relative L2 in rho (the same at dt/2 and dt/4,
-    so a property of the spatial operator).  The precision form must stay
-    within 2.5x that FP64 conditioning floor (measured 1.7-2.3x) and 3e-6 per
-    variable, and within 1e-6 per variable in the interior (20 or more
-    elements from every wall)."""
+    """The Navier-Stokes case of the benchmark (Re 5000), 1000 steps at CFL 0.5:
+    the precision form within 1e-6 relative L2 of the FP64 path per variable,
+    in the whole domain and in the interior (20 or more elements from every
+    wall).  The FP64 run from the initial state rounded once to FP32 (the
+    conditioning floor) is printed beside it: with the walls' Neumann data on
+    the common viscous flux the scheme no longer amplifies perturbations at
+    the slip-walled corners, and the floor sits at the rounding level."""
     s64, s32, U0, dt = run_pair(True)
     U64, U32 = s64.copyToHost(), s32.copyToHost()
     e = state_errors(U32, U64)
@@ -101,14 +100,13 @@ def test_mixed_tgv_ns_1000_steps(zjlib):
     print("ns mixed vs fp64:", e)
     print("ns fp64 from the FP32-rounded initial state vs fp64:", floor)
     assert np.all(np.isfinite(U32))
-    assert max(e["l2"]) <= 3e-6, e
-    assert all(a <= 2.5 * b for a, b in zip(e["l2"], floor["l2"])), (e, floor)
+    assert max(e["l2"]) <= 1e-6, e
+    assert max(floor["l2"]) <= 1e-7, floor
     n = 256
     i = np.arange(n)
     d = np.minimum(i, n - 1 - i)
     interior = np.minimum(d[:, None], d[None, :]) >= 20
     inner = state_errors(U32.reshape(n, n, -1, 4)[interior], U64.reshape(n, n, -1, 4)[interior])
-    print("ns mixed vs fp64, interior:", inner)
     assert max(inner["l2"]) <= 1e-6, inner
     # the residual norms of the last step agree to the FP32 residual's own
     # rounding (up to ~1e-3 of the flux scale per point)

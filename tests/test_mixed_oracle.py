@@ -3,6 +3,7 @@ CPU: its quadrilateral path equals the C physics oracle, its triangle
 operators are exact on polynomials of degree P, its correction fields
 conserve, and the residual preserves a free stream on a mixed mesh."""
 import math
+import os
 
 import numpy as np
 import pytest
@@ -17,6 +18,38 @@ BCS = [(1, "farfield")]
 def small_mixed(n=4, seed=11, frac=0.5):
     q = M.structured_quads(n, n, 0.0, 1.0, 0.0, 1.0, 0.15, 5, (1, 1, 1, 1), {1: "farfield"})
     return M.split_quads(q, frac, seed)
+
+
+GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+
+
+@pytest.mark.parametrize("P", [1, 2, 3, 4, 5])
+def test_triangle_points_pinned_to_reference(P):
+    """The triangle solution points are the reference's
+    (SolutionPoints::getTriangle, basis.cpp:391-417, recorded from its own
+    build in ref_triangle.npz): the collapsed map of the (P+1)-point
+    Gauss-Legendre rule, row j taking the first P+1-j points.  The
+    reference's triangle interpolation, differentiation and correction
+    operators (FROperators::initTriangle, basis.cpp:615-668) are all zero:
+    there is no reference triangle residual to pin against, so the
+    operators here are checked by exactness and conservation instead."""
+    ref = np.load(os.path.join(GOLDEN, "ref_triangle.npz"))
+    gl = np.load(os.path.join(GOLDEN, "ref_operators.npz"))[f"P{P}_pts"]
+    xi, eta = [], []
+    for j in range(P + 1):
+        for i in range(P + 1 - j):
+            sc, tc = 0.5 * (1.0 + gl[i]), 0.5 * (1.0 + gl[j])
+            xi.append(sc * (1.0 - tc))
+            eta.append(tc)
+    assert np.array_equal(np.array(xi), ref[f"P{P}_xi"])
+    assert np.array_equal(np.array(eta), ref[f"P{P}_eta"])
+    r, s = MO.tri_points(P)
+    assert np.abs(0.5 * (r + 1.0) - ref[f"P{P}_xi"]).max() <= 1e-15      # numpy leggauss rounding
+    assert np.abs(0.5 * (s + 1.0) - ref[f"P{P}_eta"]).max() <= 1e-15
+    for e in range(3):
+        assert np.array_equal(ref[f"P{P}_fp_loc"][e], 0.5 * (1.0 + gl))
+    for k in ("interp", "diff_xi", "diff_eta", "corr"):
+        assert not ref[f"P{P}_{k}"].any()
 
 
 @pytest.mark.parametrize("P", [1, 2, 3, 4])

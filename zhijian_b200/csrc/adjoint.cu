@@ -319,15 +319,19 @@ k_adj_ns(const AdjArgs a) {
             const double* UR = right ? qo : qn;
             adj::riemann_vjp<RIEM>(UL, UR, nx, ny, g, Fcb, ULb, URb);
             // common viscous flux F_v(avg U, avg Q).n enters with a minus sign
-            double Ua[4], dxa[4], dya[4], Fvb[4], Gvb[4];
+            // (through the walls' closure, a symmetric projection)
+            double Ua[4], dxa[4], dya[4], Fvb[4], Gvb[4], Fnb[4];
             double Uab[4] = {0.0, 0.0, 0.0, 0.0}, dxb[4] = {0.0, 0.0, 0.0, 0.0}, dyb[4] = {0.0, 0.0, 0.0, 0.0};
+#pragma unroll
+            for (int v = 0; v < 4; ++v) Fnb[v] = Fcb[v];
+            boundary_viscous_closure(r, a.bc, nx, ny, Fnb);
 #pragma unroll
             for (int v = 0; v < 4; ++v) {
                 Ua[v] = 0.5 * (UL[v] + UR[v]);
                 dxa[v] = 0.5 * (Qo[v] + Qn[v]);
                 dya[v] = 0.5 * (Qo[4 + v] + Qn[4 + v]);
-                Fvb[v] = -Fcb[v] * nx;
-                Gvb[v] = -Fcb[v] * ny;
+                Fvb[v] = -Fnb[v] * nx;
+                Gvb[v] = -Fnb[v] * ny;
             }
             const double dv = adj::viscous_vjp(Ua, dxa, dya, g, Re, Pr, Fvb, Gvb, Uab, dxb, dyb);
             if (!right) re_acc -= dv / Re;   // once per face: on its left element

@@ -19,7 +19,8 @@
 // Viscous flux: the reference's computeViscousFluxSPKernel law
 // (kernels.cu:742-786); common viscous flux: average state and average
 // gradients (BR2Scheme::commonFlux, navierstokes.hpp:177-204); boundaries
-// copy the interior gradient (BoundaryCondition::ghostGradient).
+// copy the interior gradient (BoundaryCondition::ghostGradient) and walls
+// impose their Neumann data on the common flux (wall_viscous_closure).
 #pragma once
 
 #include <cuda_runtime.h>
@@ -302,6 +303,10 @@ k_ns_stage(const StageArgsT<T> a) {
                 dya[v] = T(0.5) * (Qo[4 + v] + Qn[4 + v]);
             }
             viscous_flux(Ua, dxa, dya, g, Re, Pr, Fv, Gv);
+            T Fvn[4];
+#pragma unroll
+            for (int v = 0; v < 4; ++v) Fvn[v] = Fv[v] * f.nx + Gv[v] * f.ny;
+            boundary_viscous_closure(f.r, a.bc, f.nx, f.ny, Fvn);
             const T ss = right ? T(-0.5) * f.len : T(0.5) * f.len;
             const bool along_eta = (edge == 0 || edge == 2);
             T Fn[4];
@@ -310,7 +315,7 @@ k_ns_stage(const StageArgsT<T> a) {
             const T sgn = (edge == 0 || edge == 3) ? T(-1) : T(1);
 #pragma unroll
             for (int v = 0; v < 4; ++v)
-                Fd[v] = ss * (Fc[v] - (Fv[v] * f.nx + Gv[v] * f.ny)) - sgn * Fn[v];
+                Fd[v] = ss * (Fc[v] - Fvn[v]) - sgn * Fn[v];
         }
         store4(sD + el * DS + k * 4, Fd);
     }

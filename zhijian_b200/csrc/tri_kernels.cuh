@@ -345,8 +345,12 @@ k_tri_stage(const StageArgsT<T> a, const int32_t* __restrict__ elist, long long 
                     dya[v] = T(0.5) * (Qo[4 + v] + Qn[4 + v]);
                 }
                 viscous_flux(Ua, dxa, dya, g, Re, Pr, Fv, Gv);
+                T Fvn[4];
 #pragma unroll
-                for (int v = 0; v < 4; ++v) Fc[v] -= Fv[v] * nr[0] + Gv[v] * nr[1];
+                for (int v = 0; v < 4; ++v) Fvn[v] = Fv[v] * nr[0] + Gv[v] * nr[1];
+                boundary_viscous_closure(r, a.bc, nr[0], nr[1], Fvn);
+#pragma unroll
+                for (int v = 0; v < 4; ++v) Fc[v] -= Fvn[v];
             }
             const T sf = nr[2] * T(1.0 / tri_ref_len(edge));
             const T ss = right ? -sf : sf;

@@ -251,5 +251,37 @@ __device__ __forceinline__ void viscous_flux(const T* s, const T* dx, const T* d
     Gv[0] = T(0); Gv[1] = txy; Gv[2] = tyy; Gv[3] = u * txy + v * tyy + k * dTdy;
 }
 
+// Neumann data of the walls imposed on the common normal viscous flux Fvn of
+// a boundary face (the gradient there is the interior one,
+// BoundaryCondition::ghostGradient, boundary_condition.hpp:25-31): a slip or
+// symmetry wall carries no shear stress and no heat flux (only tau_nn n
+// remains; its energy work vanishes with u.n = 0), an adiabatic no-slip wall
+// (T_wall = 0) no heat flux (its velocity is zero, so the energy flux is the
+// heat flux).  These are the conditions the reference's wall classes state
+// (boundary_condition.hpp:60-67, 146-155).  With the interior gradient and no
+// such data the face adds u q to the discrete energy (BR1, sign-indefinite),
+// which grows at the corners of slip-walled boxes.  The map is a symmetric
+// projection: its transpose is itself.
+template <typename T>
+__device__ __forceinline__ void wall_viscous_closure(int bc_type, bool adiabatic, T nx, T ny, T* Fvn) {
+    if (bc_type == ZJ_BC_SLIPWALL || bc_type == ZJ_BC_SYMMETRY) {
+        const T tnn = Fvn[1] * nx + Fvn[2] * ny;
+        Fvn[1] = tnn * nx;
+        Fvn[2] = tnn * ny;
+        Fvn[3] = T(0);
+    } else if (bc_type == ZJ_BC_WALL && adiabatic) {
+        Fvn[3] = T(0);
+    }
+}
+
+// The closure of boundary face r (no-op elsewhere); bc is the face data table.
+template <typename T, typename B>
+__device__ __forceinline__ void boundary_viscous_closure(const EdgeRec& r, const B* bc, T nx, T ny, T* Fvn) {
+    if (!(r.flags & kEdgeBoundary)) return;
+    const int bt = edge_bc_type(r.flags);
+    const bool adiabatic = bt == ZJ_BC_WALL && !(bc[(long long)r.nbr_edge * 8] > B(0));
+    wall_viscous_closure(bt, adiabatic, nx, ny, Fvn);
+}
+
 }  // namespace phys
 }  // namespace zj
