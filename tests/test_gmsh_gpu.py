@@ -1,7 +1,8 @@
 """Solvers created from Gmsh files (zj_solver_create_from_gmsh): the residual
 equals the residual of the same mesh given as arrays, and the oracle's, in
 compat mode (Q1, curved Q2, serendipity) and in physics mode (Navier-Stokes on
-Q1).  Boundary types come from the files' physical names."""
+Q1, and on a file of triangles and quads against the mixed-mesh oracle).
+Boundary types come from the files' physical names."""
 import os
 
 import numpy as np
@@ -48,3 +49,28 @@ def test_physics_ns_from_gmsh(zjlib, oracle_mod):
     orc.set_physics(1, 1, True, 50.0, 0.72, 8.5e4)
     Ro = orc.rhs_phys(U)
     assert T.rel_err(R, Ro, T.euler_flux_scale(U, orc.geometry()[1])) <= 1e-12
+
+
+def test_physics_ns_mixed_from_gmsh(zjlib):
+    """Triangles and quadrilaterals read from an MSH 4.1 file: the solver
+    from the file equals the one from the arrays bit for bit and the mixed
+    oracle to its bar (1e-11 of the flux scale)."""
+    from oracle import mixed_oracle as MO
+    from tests.test_mixed_mesh_gpu import smooth_state
+    path = os.path.join(GM, "triquad_v41.msh")
+    data = read_gmsh(path)
+    assert set(data.elem_type.tolist()) == {0, 1}
+    mesh = data.to_mixed_mesh()
+    P = 3
+    kw = dict(poly_order=P, compat=False, viscous=True, Re=50.0, Pr=0.72, riemann="Roe", flux_type="SD", **KW)
+    s_file = FRSolver.from_gmsh(path, make_params(**kw))
+    s_arr = FRSolver(mesh, make_params(bcs=[(t, n) for t, n in sorted(mesh.tag_names.items())], **kw))
+    U = smooth_state(s_arr, 29)
+    R = s_file.rhs(U)
+    assert np.array_equal(R, s_arr.rhs(U))
+    mo = MO.MixedOracle(mesh, P, 1.4, 1.2, 1.0e5, 0.4, 10.0, flux_type=1, riemann=1, viscous=True,
+                        Re=50.0, Pr=0.72, T_inf=8.5e4)
+    Ro = mo.rhs(U)
+    m = s_arr.slot_mask()
+    scale = T.euler_flux_scale(U[m], np.concatenate([mo.Ji[e] for e in range(mo.E)]))
+    assert T.rel_err(R[m], Ro[m], scale) <= 1e-11

@@ -8,7 +8,7 @@ import dataclasses
 import numpy as np
 
 from . import _lib as L
-from .meshgen import QuadMesh
+from .meshgen import MixedMesh, QuadMesh
 
 BC_NAMES = {v: k for k, v in L.BC_TYPES.items()}
 
@@ -33,6 +33,21 @@ class GmshData:
         nn = int(self.offsets[1] - self.offsets[0])
         return QuadMesh(self.xy.copy(), self.conn.reshape(-1, nn).copy(), self.bnd.copy(),
                         {t: BC_NAMES[ty] for t, ty, _ in self.groups})
+
+
+    def to_mixed_mesh(self) -> MixedMesh:
+        """The mesh as a MixedMesh (straight-sided triangles and quadrilaterals,
+        their first three / four nodes)."""
+        if np.any(self.elem_order != 1):
+            raise ValueError("not a straight-sided (order 1) mesh")
+        conn, off = [], [0]
+        for e in range(len(self.elem_type)):
+            nv = 3 if self.elem_type[e] == 0 else 4
+            conn.extend(self.element(e)[:nv].tolist())
+            off.append(len(conn))
+        return MixedMesh(self.xy.copy(), self.elem_type.astype(np.int32), np.array(off, dtype=np.int64),
+                         np.array(conn, dtype=np.int64), self.bnd.copy(),
+                         {t: BC_NAMES[ty] for t, ty, _ in self.groups})
 
 
 def read_gmsh(path: str) -> GmshData:

@@ -1,12 +1,15 @@
-"""A few SSP-RK3 steps of the benchmark's Taylor-Green case, for external
-profilers (ncu) that capture a handful of launches:
+"""A few SSP-RK3 steps of the benchmark's cases, for external profilers (ncu)
+that capture a handful of launches:
 
-    python -m zhijian_b200.profile_case {ns|ns32|euler|euler32|compat} [steps] [n]
+    python -m zhijian_b200.profile_case {ns|ns32|euler|euler32|compat|shear|shear32} [steps] [n]
 
 ns / ns32: Navier-Stokes (Re 5000, Pr 0.72, Roe, HU), FP64 / precision form;
 euler / euler32: the inviscid physics-mode residual; compat: the reference
 residual semantics.  256x256 jittered Q1 quads on [0,pi]^2 (seed 1), P3,
-slip walls, dt = 2e-4 (n overrides the mesh size)."""
+slip walls, dt = 2e-4 (n overrides the mesh size).
+shear / shear32: the mixed-element shear layer (n x n quads, default 384, a
+seeded 30% split into triangles; Navier-Stokes Re 2000, HLLC, GA, P3) at
+CFL 0.1, FP64 / precision form."""
 from __future__ import annotations
 
 import math
@@ -26,9 +29,23 @@ MODES = {
 }
 
 
+def shear(mode, steps, n):
+    mesh = M.shear_layer_mesh(n)
+    prm = make_params(poly_order=3, flux_type="GA", CFL=0.1,
+                      precision="mixed" if mode == "shear32" else "fp64", **M.SHEAR_LAYER_PARAMS)
+    s = FRSolver(mesh, prm)
+    s.setInitialCondition(M.shear_layer)
+    s.advance(s.computeTimeStep(), steps)
+    s.check_state()
+    print(f"{mode}: {steps} steps on {mesh.n_elem} elements, residual norm {s.computeResidual():.6e}")
+    return 0 if math.isfinite(s.computeResidual()) else 1
+
+
 def main(argv):
     mode = argv[1] if len(argv) > 1 else "ns"
     steps = int(argv[2]) if len(argv) > 2 else 4
+    if mode in ("shear", "shear32"):
+        return shear(mode, steps, int(argv[3]) if len(argv) > 3 else 384)
     n = int(argv[3]) if len(argv) > 3 else 256
     mesh = M.tgv_mesh(n, seed=1)
     prm = make_params(poly_order=3, gamma=GAMMA, rho_inf=1.0, p_inf=1.0 / (GAMMA * MACH * MACH),
