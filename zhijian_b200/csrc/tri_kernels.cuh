@@ -22,11 +22,17 @@
 #include "ns_kernels.cuh"
 
 #ifndef ZJ_TRI_MIN_BLOCKS
-#define ZJ_TRI_MIN_BLOCKS 1
+#define ZJ_TRI_MIN_BLOCKS 2       // FP64 stage kernel (128 registers; viscous: spills of 16-36 B)
+#endif
+#ifndef ZJ_TRI32_MIN_BLOCKS
+#define ZJ_TRI32_MIN_BLOCKS 3     // precision-form stage kernel (80 registers)
 #endif
 
 namespace zj {
 namespace {
+
+template <typename T> struct TriMinBlocks { static constexpr int stage = ZJ_TRI_MIN_BLOCKS; };
+template <> struct TriMinBlocks<float> { static constexpr int stage = ZJ_TRI32_MIN_BLOCKS; };
 
 template <int P, typename T>
 struct TriShape {
@@ -222,7 +228,7 @@ k_tri_grad(const StageArgsT<T> a, const int32_t* __restrict__ elist, long long n
 
 // ----------------------------------------------------------------- stage --
 template <int P, int RIEM, bool VISC, typename T>
-__global__ void __launch_bounds__(TriShape<P, T>::THREADS, ZJ_TRI_MIN_BLOCKS)
+__global__ void __launch_bounds__(TriShape<P, T>::THREADS, TriMinBlocks<T>::stage)
 k_tri_stage(const StageArgsT<T> a, const int32_t* __restrict__ elist, long long n_list) {
     using S = TriShape<P, T>;
     using Lo = TriLayout<P, T>;
