@@ -75,7 +75,7 @@ __device__ __forceinline__ double viscous_vjp(const double* s, const double* dx,
     const double dpdx = c * (dx[3] - 0.5 * dx[0] * q2 - s[0] * (u * dudx + v * dvdx));
     const double dpdy = c * (dy[3] - 0.5 * dy[0] * q2 - s[0] * (u * dudy + v * dvdy));
     const double dTdx = (dpdx - Tm * dx[0]) * ir, dTdy = (dpdy - Tm * dy[0]) * ir;
-    const double mu = pow(Tm, 0.7) / Re;
+    const double mu = zj_pow07(Tm) / Re;
     const double kc = g / (c * Pr);
     const double k = mu * kc;
     const double div = dudx + dvdy, lam = (-2.0 / 3.0) * mu;

@@ -107,6 +107,10 @@ __device__ __forceinline__ double div_any(double a, double b) { return a / b; }
 __device__ __forceinline__ float div_any(float a, float b) { return a * rcp_any(b); }
 __device__ __forceinline__ double pow_any(double a, double b) { return pow(a, b); }
 __device__ __forceinline__ float pow_any(float a, float b) { return __powf(a, b); }
+// T^0.7 of the viscosity law: the series routine of zj_math.h in FP64 (within
+// 2 ulp of pow(T, 0.7)), the hardware exp2/log2 form in FP32.
+__device__ __forceinline__ double visc_pow(double t) { return zj_pow07(t); }
+__device__ __forceinline__ float visc_pow(float t) { return __powf(t, 0.7f); }
 __device__ __forceinline__ double fma_any(double a, double b, double c) { return __fma_rn(a, b, c); }
 __device__ __forceinline__ float fma_any(float a, float b, float c) { return __fmaf_rn(a, b, c); }
 __device__ __forceinline__ double max_any(double a, double b) { return fmax(a, b); }

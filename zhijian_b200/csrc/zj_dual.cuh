@@ -63,6 +63,10 @@ __device__ __forceinline__ Dual pow_any(Dual a, Dual b) {
     if (b.d != 0.0) t += p * log(a.v) * b.d;
     return Dual(p, t);
 }
+__device__ __forceinline__ Dual visc_pow(Dual a) {
+    const double p = zj_pow07(a.v);
+    return Dual(p, (a.d != 0.0) ? 0.7 * p / a.v * a.d : 0.0);
+}
 __device__ __forceinline__ Dual div_any(Dual a, Dual b) { return a / b; }
 __device__ __forceinline__ Dual fma_any(Dual a, Dual b, Dual c) {
     return Dual(__fma_rn(a.v, b.v, c.v), fma(a.d, b.v, fma(a.v, b.d, c.d)));

@@ -242,7 +242,7 @@ __device__ __forceinline__ void viscous_flux(const T* s, const T* dx, const T* d
     const T dpdx = (g - T(1)) * (dx[3] - T(0.5) * dx[0] * (u * u + v * v) - s[0] * (u * dudx + v * dvdx));
     const T dpdy = (g - T(1)) * (dy[3] - T(0.5) * dy[0] * (u * u + v * v) - s[0] * (u * dudy + v * dvdy));
     const T dTdx = (dpdx - Tm * dx[0]) * ir, dTdy = (dpdy - Tm * dy[0]) * ir;
-    const T mu = div_any(pow_any(Tm, T(0.7)), Re);
+    const T mu = div_any(visc_pow(Tm), Re);
     const T k = div_any(mu * g, (g - T(1)) * Pr);
     const T div = dudx + dvdy, lam = T(-2.0 / 3.0) * mu;
     const T txx = T(2) * mu * dudx + lam * div, tyy = T(2) * mu * dvdy + lam * div;
