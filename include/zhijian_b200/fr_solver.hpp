@@ -123,6 +123,12 @@ public:
     void copyToDevice() { check(zj_set_state(s_, host_.data()), s_); }
     const std::vector<double>& solution() const { return host_; }
     std::vector<double>& solution() { return host_; }
+    // Queued copies of a caller's host buffer (zj_set_state_async /
+    // zj_get_state_async): the buffer stays alive and unchanged until
+    // synchronize(); page-locked buffers overlap the copy with other streams.
+    void copyToDeviceAsync(const double* U) { check(zj_set_state_async(s_, U), s_); }
+    void copyToHostAsync(double* U) { check(zj_get_state_async(s_, U), s_); }
+    void synchronize() { check(zj_synchronize(s_), s_); }
 
     const zj_params& params() const { return params_; }
     zj_solver* handle() { return s_; }

@@ -150,6 +150,15 @@ zj_status zj_get_state(zj_solver* s, double* U_host);
 /* Same with device buffers (no host copy). */
 zj_status zj_set_state_device(zj_solver* s, const double* U_dev);
 zj_status zj_get_state_device(zj_solver* s, double* U_dev);
+/* Host copies queued on the handle's stream without waiting (no reference
+ * counterpart: copyToDevice/copyToHost block).  The host buffer must stay
+ * valid, and unchanged for a set, until zj_synchronize; page-locked buffers
+ * (cudaHostAlloc / cudaHostRegister) let the copy run on a copy engine while
+ * other streams compute, so a caller streaming independent states through two
+ * handles on two streams overlaps one handle's copies with the other's steps.
+ * Setting the state resets time and iteration like zj_set_state. */
+zj_status zj_set_state_async(zj_solver* s, const double* U_host);
+zj_status zj_get_state_async(zj_solver* s, double* U_host);
 
 /* ---- the hot path ---------------------------------------------------------- */
 /* nsteps SSP-RK3 steps of size dt (FRSolver::advance, fr_solver.cpp:305-333),

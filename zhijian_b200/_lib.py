@@ -78,6 +78,8 @@ def lib():
         "zj_solution_point_coords": (ip, [vp, dp]),
         "zj_set_state": (ip, [vp, dp]),
         "zj_get_state": (ip, [vp, dp]),
+        "zj_set_state_async": (ip, [vp, vp]),
+        "zj_get_state_async": (ip, [vp, vp]),
         "zj_set_state_device": (ip, [vp, vp]),
         "zj_get_state_device": (ip, [vp, vp]),
         "zj_step": (ip, [vp, C.c_double, ip]),

@@ -551,6 +551,22 @@ zj_status zj_get_state(zj_solver* s, double* U) {
     return ZJ_OK;
 }
 
+zj_status zj_set_state_async(zj_solver* s, const double* U) {
+    if (!s || !U) return ZJ_ERR_ARG;
+    ZJ_CK(s, cudaMemcpyAsync(s->dU[s->cur], U, s->state_n * 8, cudaMemcpyHostToDevice, s->stream), "set_state_async copy");
+    s->traces_valid = false;
+    s->has_norm = false;
+    s->time = 0.0;
+    s->iter = 0;
+    return ZJ_OK;
+}
+
+zj_status zj_get_state_async(zj_solver* s, double* U) {
+    if (!s || !U) return ZJ_ERR_ARG;
+    ZJ_CK(s, cudaMemcpyAsync(U, s->dU[s->cur], s->state_n * 8, cudaMemcpyDeviceToHost, s->stream), "get_state_async copy");
+    return ZJ_OK;
+}
+
 zj_status zj_set_state_device(zj_solver* s, const double* U) {
     if (!s || !U) return ZJ_ERR_ARG;
     ZJ_CK(s, cudaMemcpyAsync(s->dU[s->cur], U, s->state_n * 8, cudaMemcpyDeviceToDevice, s->stream), "set_state_device copy");

@@ -160,6 +160,20 @@ class FRSolver:
 
     solution = copyToHost
 
+    def copyToDeviceAsync(self, U: np.ndarray):
+        """Queue the host-to-device copy of U (C-contiguous float64 of the
+        state's shape) on the handle's stream and return.  U must stay alive
+        and unchanged until synchronize(); page-locked memory lets the copy
+        overlap other streams' work."""
+        assert U.dtype == np.float64 and U.flags.c_contiguous and U.size == np.prod(self.shape)
+        self._ck(L.lib().zj_set_state_async(self.h, C.c_void_p(U.ctypes.data)))
+
+    def copyToHostAsync(self, out: np.ndarray):
+        """Queue the device-to-host copy of the state into out on the handle's
+        stream and return; out holds it after synchronize()."""
+        assert out.dtype == np.float64 and out.flags.c_contiguous and out.size == np.prod(self.shape)
+        self._ck(L.lib().zj_get_state_async(self.h, C.c_void_p(out.ctypes.data)))
+
     def advance(self, dt: float, nsteps: int = 1, sync: bool = True):
         self._ck(L.lib().zj_step(self.h, float(dt), int(nsteps)))
         if sync:
