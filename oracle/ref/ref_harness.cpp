@@ -11,8 +11,10 @@
 //   ref_gpu : + kernels.cu + fr_solver.cpp, needs a GPU.
 //             "rhs mesh.bin params state out"           -> computeResidual_GPU
 //             "step mesh.bin params state dt n out"     -> n x advance(dt)
+//             "time mesh.bin params state dt nw n out"  -> wall ms of n advance(dt)
 // Files are raw little-endian arrays; layouts are written by
 // oracle/oracle.py (write_mesh_bin) and read back by it.
+#include <chrono>
 #include <cstdint>
 #include <cstdio>
 #include <cstdlib>
@@ -304,6 +306,22 @@ int cmd_gpu(int argc, char** argv) {
         cudaDeviceSynchronize();
         s.gpu_data_->dUdt.copyToHost(out.data(), n);
         Writer(argv[10]).arr(out);
+    } else if (cmd == "time") {
+        // wall clock of nsteps advance() calls after nwarm, device idle at both
+        // ends: the reference's step includes host work and copies
+        double dt = std::atof(argv[10]);
+        int nwarm = std::atoi(argv[11]), ns = std::atoi(argv[12]);
+        for (int k = 0; k < nwarm; ++k) s.advance(dt);
+        cudaDeviceSynchronize();
+        auto t0 = std::chrono::steady_clock::now();
+        for (int k = 0; k < ns; ++k) s.advance(dt);
+        cudaDeviceSynchronize();
+        auto t1 = std::chrono::steady_clock::now();
+        double ms = std::chrono::duration<double, std::milli>(t1 - t0).count();
+        std::FILE* f = std::fopen(argv[13], "w");
+        if (!f) return 2;
+        std::fprintf(f, "%d %.6f\n", ns, ms);
+        std::fclose(f);
     } else {
         double dt = std::atof(argv[10]);
         int ns = std::atoi(argv[11]);
@@ -331,7 +349,8 @@ int main(int argc, char** argv) {
     if (cmd == "gmsh" && argc == 4) return cmd_gmsh(argv[2], argv[3]);
     if (cmd == "phys" && argc == 15) return cmd_phys(argv + 2);
 #ifdef ZJ_REF_GPU
-    if ((cmd == "rhs" && argc == 11) || (cmd == "step" && argc == 13)) return cmd_gpu(argc, argv);
+    if ((cmd == "rhs" && argc == 11) || (cmd == "step" && argc == 13) || (cmd == "time" && argc == 14))
+        return cmd_gpu(argc, argv);
 #endif
     std::fprintf(stderr, "bad command\n");
     return 1;
