@@ -252,30 +252,66 @@ LAUNCHES_PER_RHS = {"ns": 2, "ns32": 2, "compat": 1}
 E2E_HANDLES = 3
 
 
+class Ranks:
+    """One process per GPU (torchrun): rank and world from the environment, a
+    process group with a short timeout when world > 1, a barrier and the
+    maximum of a per-rank number (the timing rule: the job takes as long as
+    its slowest rank).  backend "nccl" with a CUDA device in the bench; the
+    tests run the same code with "gloo" on the CPU."""
+
+    def __init__(self, backend="nccl", device=None, timeout_s=120):
+        import torch
+        import torch.distributed as dist
+        self.dist = dist
+        self.world = int(os.environ.get("WORLD_SIZE", "1"))
+        self.rank = int(os.environ.get("RANK", "0"))
+        self.local = int(os.environ.get("LOCAL_RANK", "0"))
+        self.device = device if device is not None else torch.device("cpu")
+        self.backend = backend
+        if self.world > 1:
+            import datetime
+            dist.init_process_group(backend, timeout=datetime.timedelta(seconds=timeout_s))
+
+    def barrier(self):
+        if self.world > 1:
+            if self.backend == "nccl":
+                self.dist.barrier(device_ids=[self.local])
+            else:
+                self.dist.barrier()
+
+    def max(self, x):
+        if self.world == 1:
+            return x
+        import torch
+        t = torch.tensor([x], dtype=torch.float64, device=self.device)
+        self.dist.all_reduce(t, op=self.dist.ReduceOp.MAX)
+        return float(t.item())
+
+    def close(self):
+        if self.world > 1:
+            self.dist.destroy_process_group()
+
+
+def whole_job_rate(units_per_rank, world, ms):
+    """Units all ranks processed per second over the slowest rank's time
+    (replicas: every rank processes the same units)."""
+    return world * units_per_rank / (ms * 1e-3)
+
+
 def run_ours(args):
     import torch
-    import torch.distributed as dist
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
-    if world > 1:
-        import datetime
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
+    ranks = Ranks("nccl", dev)
+    world, rank = ranks.world, ranks.rank
 
     def barrier_sync():
         torch.cuda.synchronize()
-        if world > 1:
-            dist.barrier(device_ids=[local])
+        ranks.barrier()
         torch.cuda.synchronize()
 
-    def max_over_ranks(x):
-        if world == 1:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+    max_over_ranks = ranks.max
 
     from zhijian_b200 import meshgen as M
     mesh = build_case()
@@ -314,7 +350,7 @@ def run_ours(args):
 
     head = "ns32"
     s, U0, dof, ms, roofline = timed(head)
-    value = world * dof * 3 * args.steps / (ms * 1e-3)
+    value = whole_job_rate(dof * 3 * args.steps, world, ms)
     launches = 3 * args.steps * LAUNCHES_PER_RHS[head]
 
     # end to end through the C-ABI with host buffers: per step a state goes
@@ -369,25 +405,25 @@ def run_ours(args):
         ends.append(ev)
     barrier_sync()
     ems = max_over_ranks(max(g0.elapsed_time(ev) for ev in ends))
-    e2e = {"value": world * dof * 3 * n_e2e / (ems * 1e-3), "unit": UNIT,
+    e2e = {"value": whole_job_rate(dof * 3 * n_e2e, world, ems), "unit": UNIT,
            "h2d_bytes_per_step": int(U0.nbytes), "d2h_bytes_per_step": int(U0.nbytes),
            "steps": n_e2e,
            "mode": f"independent states over {nh} handles on {nh} streams, queued copies from pinned memory",
-           "serial": {"value": world * dof * 3 * n_e2e / (ems_serial * 1e-3),
+           "serial": {"value": whole_job_rate(dof * 3 * n_e2e, world, ems_serial),
                       "mode": "one handle, blocking copies"}}
     for h, _ in pairs:
         h.close()
 
     s64, _, _, ms64, roof64 = timed("ns")
     s64.close()
-    fp64 = {"workload": workload_name("ns") + ", FP64", "value": world * dof * 3 * args.steps / (ms64 * 1e-3),
+    fp64 = {"workload": workload_name("ns") + ", FP64", "value": whole_job_rate(dof * 3 * args.steps, world, ms64),
             "ms_per_step": ms64 / args.steps, "roofline": roof64,
             "gpu_launches": 3 * args.steps * LAUNCHES_PER_RHS["ns"]}
     clocks = sampler.stop()
 
     sc, _, dofc, msc, roofc = timed("compat")
     sc.close()
-    compat = {"workload": workload_name("compat"), "value": world * dofc * 3 * args.steps / (msc * 1e-3),
+    compat = {"workload": workload_name("compat"), "value": whole_job_rate(dofc * 3 * args.steps, world, msc),
               "ms_per_step": msc / args.steps, "roofline": roofc,
               "gpu_launches": 3 * args.steps}
 
@@ -416,8 +452,7 @@ def run_ours(args):
                "adjoint": adjoint, "p5_precision": p5, "mixed_elements": shear, "compat": compat}
         if world == 1 and not args.no_cpu_baseline:
             out["cpu_baseline"] = cpu_baseline(mesh, args.cpu_seconds, "ns")
-    if world > 1:
-        dist.destroy_process_group()
+    ranks.close()
     return out
 
 
