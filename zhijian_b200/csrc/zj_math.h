@@ -2,16 +2,20 @@
 //
 // An FP64 division or square root is a long dependent instruction sequence
 // with a special-case path; the residual kernels take several per state.
-// These two functions use Newton-Raphson iterations from integer-arithmetic
-// seeds, so they are short branch-free chains of FP64 FMAs and integer ops:
-//   reciprocal: seed = bits(0x7FDE623822FC16E6 - bits(x)) (relative error
-//     below 1/8 for normal x), then e = 1 - x*y, y += y*e five times
-//     (error squares each step: 2^-3 -> below 2^-60);
-//   inverse square root: Lomont's seed bits(0x5FE6EB50C7B537A9 - bits(a)/2)
-//     (relative error below 4%), then y += y/2 * (1 - a*y*y) four times;
+// These two functions use Newton-Raphson iterations, so they are short
+// branch-free chains of FP64 FMAs:
+//   reciprocal: e = 1 - x*y, y += y*e (the error squares each step) from the
+//     hardware's approximate FP64 reciprocal (rcp.approx.ftz.f64) on the
+//     device, two steps; on the host from the integer seed
+//     bits(0x7FDE623822FC16E6 - bits(x)) (relative error below 1/8), five
+//     steps (2^-3 -> below 2^-60);
+//   inverse square root: y += y/2 * (1 - a*y*y) from rsqrt.approx.ftz.f64 on
+//     the device, two steps; on the host from Lomont's seed
+//     bits(0x5FE6EB50C7B537A9 - bits(a)/2) (relative error below 4%), four;
 //   square root: s = a*y and one Newton correction s += (a - s*s) * y/2.
 // Results are within 2 ulp of the correctly rounded value on the domains
-// below (tests/test_zj_math.py checks the bound over 2^20 samples).
+// below (tests/test_zj_math.py checks the host side, tests/test_zj_math_gpu.py
+// the device side, over 2^20 samples each).
 // zj_rcp: 2^-1020 < x < 2^1020 (the residual passes floored densities).
 // zj_sqrt: any a >= 0; sqrt(0) = 0, NaN and +inf propagate, a < 0 gives NaN.
 #pragma once
@@ -57,6 +61,16 @@ ZJ_MATH_HD double zj_fma(double a, double b, double c) {
 
 // 1/x for positive normal x (the floored densities of the residual).
 ZJ_MATH_HD double zj_rcp(double x) {
+#ifdef __CUDA_ARCH__
+    double y;
+    asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(y) : "d"(x));
+#pragma unroll
+    for (int it = 0; it < 2; ++it) {
+        const double e = zj_fma(-x, y, 1.0);
+        y = zj_fma(y, e, y);
+    }
+    return y;
+#else
     double y = zj_from_bits(0x7FDE623822FC16E6LL - zj_bits(x));
 #pragma unroll
     for (int it = 0; it < 5; ++it) {
@@ -64,6 +78,7 @@ ZJ_MATH_HD double zj_rcp(double x) {
         y = zj_fma(y, e, y);
     }
     return y;
+#endif
 }
 
 // sqrt(a) for a >= 0.
@@ -72,9 +87,16 @@ ZJ_MATH_HD double zj_sqrt(double a) {
         if (a == 0.0) return 0.0;
         return (a < 0.0) ? zj_from_bits(0x7FF8000000000000LL) : a + a;
     }
+#ifdef __CUDA_ARCH__
+    double y;
+    asm("rsqrt.approx.ftz.f64 %0, %1;" : "=d"(y) : "d"(a));
+    constexpr int kIt = 2;
+#else
     double y = zj_from_bits(0x5FE6EB50C7B537A9LL - (zj_bits(a) >> 1));
+    constexpr int kIt = 4;
+#endif
 #pragma unroll
-    for (int it = 0; it < 4; ++it) {
+    for (int it = 0; it < kIt; ++it) {
         const double e = zj_fma(-a, y * y, 1.0);
         y = zj_fma(0.5 * y, e, y);
     }
