@@ -205,6 +205,8 @@ k_compat_stage(const StageArgs a) {
 
     const int tid = threadIdx.x;
     for (int i = tid; i < S::NOPS; i += blockDim.x) sOps[i] = a.ops[i];
+    pdl_launch_dependents();
+    pdl_wait();   // the state and traces come from the previous stage
 
     const int el = tid / TPE, k = tid - el * TPE;
     const long long e = (long long)blockIdx.x * EB + el;
@@ -472,8 +474,7 @@ cudaError_t launch_stage_t(const StageArgs& a, cudaStream_t s, int* grid_out) {
                              cudaSharedmemCarveoutMaxShared);
         carveout_set = true;
     }
-    k_compat_stage<P><<<(unsigned)grid, S::THREADS, 0, s>>>(a);
-    return cudaGetLastError();
+    return launch_programmatic(k_compat_stage<P>, (unsigned)grid, S::THREADS, s, a);
 }
 
 template <int P>

@@ -133,6 +133,8 @@ k_ns_grad(const StageArgsT<T> a) {
 
     const int tid = threadIdx.x;
     for (int t = tid; t < S::NOPS; t += blockDim.x) sOps[t] = a.ops[t];
+    pdl_launch_dependents();
+    pdl_wait();   // the state and traces come from the previous stage
     const int el = tid / TPE, k = tid - el * TPE;
     bool valid;
     const long long e = block_element(a, EB, el, valid);
@@ -204,6 +206,8 @@ k_ns_stage(const StageArgsT<T> a) {
 
     const int tid = threadIdx.x;
     for (int t = tid; t < S::NOPS; t += blockDim.x) sOps[t] = a.ops[t];
+    pdl_launch_dependents();
+    pdl_wait();   // the gradient traces come from k_ns_grad, the state from the previous stage
     const int el = tid / TPE, k = tid - el * TPE;
     bool valid;
     const long long e = block_element(a, EB, el, valid);
@@ -410,8 +414,7 @@ cudaError_t ns_grad_t(const StageArgsT<T>& a, cudaStream_t s) {
     if (grid <= 0) return cudaSuccess;
     static bool set = false;
     if (!set) { prefer_shared(k_ns_grad<P, T>); set = true; }
-    k_ns_grad<P, T><<<(unsigned)grid, S::THREADS, 0, s>>>(a);
-    return cudaGetLastError();
+    return launch_programmatic(k_ns_grad<P, T>, (unsigned)grid, S::THREADS, s, a);
 }
 
 template <int P, int RIEM, typename T>
@@ -421,8 +424,7 @@ cudaError_t ns_stage_t(const StageArgsT<T>& a, cudaStream_t s) {
     if (grid <= 0) return cudaSuccess;
     static bool set = false;
     if (!set) { prefer_shared(k_ns_stage<P, RIEM, T>); set = true; }
-    k_ns_stage<P, RIEM, T><<<(unsigned)grid, S::THREADS, 0, s>>>(a);
-    return cudaGetLastError();
+    return launch_programmatic(k_ns_stage<P, RIEM, T>, (unsigned)grid, S::THREADS, s, a);
 }
 
 template <int P, typename T>

@@ -214,6 +214,8 @@ k_phys_stage(const StageArgsT<T> a) {
 
     const int tid = threadIdx.x;
     for (int i = tid; i < S::NOPS; i += blockDim.x) sOps[i] = a.ops[i];
+    pdl_launch_dependents();
+    pdl_wait();   // the state and traces come from the previous stage
 
     const int el = tid / TPE, k = tid - el * TPE;
     bool valid;
@@ -442,8 +444,7 @@ cudaError_t phys_stage_t(const StageArgsT<T>& a, cudaStream_t s) {
     if (grid <= 0) return cudaSuccess;
     static bool carveout_set = false;
     if (!carveout_set) { prefer_shared(k_phys_stage<P, RIEM, T>); carveout_set = true; }
-    k_phys_stage<P, RIEM, T><<<(unsigned)grid, S::THREADS, 0, s>>>(a);
-    return cudaGetLastError();
+    return launch_programmatic(k_phys_stage<P, RIEM, T>, (unsigned)grid, S::THREADS, s, a);
 }
 
 template <int P, typename T>

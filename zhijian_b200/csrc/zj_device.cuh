@@ -173,6 +173,36 @@ __device__ __forceinline__ void trace_point(const T* s, const T* Lm, const T* Lp
     }
 }
 
+// Programmatic dependent launch (sm_90+): a kernel launched with
+// cudaLaunchAttributeProgrammaticStreamSerialization may start while the
+// previous kernel in its stream finishes.  pdl_launch_dependents lets the
+// next such kernel's CTAs start once every CTA of this grid has run it;
+// pdl_wait returns once the previous grid has completed and its memory
+// operations are visible, so nothing a kernel reads before it may come from
+// a kernel (only operators, geometry and kernel parameters).  Both are no-ops
+// for a kernel launched without the attribute.
+__device__ __forceinline__ void pdl_launch_dependents() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+
+// Launch with programmatic stream serialisation: the kernel (which calls
+// pdl_wait before reading anything a kernel writes) may start while the
+// previous kernel in the stream drains.
+template <typename A>
+cudaError_t launch_programmatic(void (*kernel)(A), unsigned grid, unsigned threads, cudaStream_t s,
+                                const A& a) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(grid);
+    cfg.blockDim = dim3(threads);
+    cfg.dynamicSmemBytes = 0;
+    cfg.stream = s;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, kernel, a);
+}
+
 // Block-wide deterministic sum; result valid in thread 0.
 __device__ __forceinline__ double block_sum(double x, double* red) {
 #pragma unroll
