@@ -171,6 +171,8 @@ k_tri_grad(const StageArgsT<T> a, const int32_t* __restrict__ elist, long long n
     __shared__ __align__(16) T sQ[EB * 2 * ES];
     const int tid = threadIdx.x;
     for (int t = tid; t < S::NOPS; t += blockDim.x) sOps[t] = a.ops[t];
+    pdl_launch_dependents();
+    pdl_wait();   // the state and traces come from the previous launches
     const int el = tid / TPE, k = tid - el * TPE;
     const long long e = (el < EB) ? tri_element(elist, n_list, EB, el) : -1;
     const bool valid = e >= 0;
@@ -242,6 +244,8 @@ k_tri_stage(const StageArgsT<T> a, const int32_t* __restrict__ elist, long long 
     __shared__ double sRed[32];
     const int tid = threadIdx.x;
     for (int t = tid; t < S::NOPS; t += blockDim.x) sOps[t] = a.ops[t];
+    pdl_launch_dependents();
+    pdl_wait();   // the state and traces come from the previous launches
     const int el = tid / TPE, k = tid - el * TPE;
     const long long e = (el < EB) ? tri_element(elist, n_list, EB, el) : -1;
     const bool valid = e >= 0;
@@ -456,8 +460,7 @@ cudaError_t tri_grad_t(const StageArgsT<T>& a, const int32_t* elist, long long n
     using S = TriShape<P, T>;
     const long long grid = (n + S::EB - 1) / S::EB;
     if (grid <= 0) return cudaSuccess;
-    k_tri_grad<P, T><<<(unsigned)grid, S::THREADS, 0, s>>>(a, elist, n);
-    return cudaGetLastError();
+    return launch_programmatic(k_tri_grad<P, T>, (unsigned)grid, S::THREADS, s, a, elist, n);
 }
 
 template <int P, int RIEM, bool VISC, typename T>
@@ -465,8 +468,7 @@ cudaError_t tri_stage_t(const StageArgsT<T>& a, const int32_t* elist, long long 
     using S = TriShape<P, T>;
     const long long grid = (n + S::EB - 1) / S::EB;
     if (grid <= 0) return cudaSuccess;
-    k_tri_stage<P, RIEM, VISC, T><<<(unsigned)grid, S::THREADS, 0, s>>>(a, elist, n);
-    return cudaGetLastError();
+    return launch_programmatic(k_tri_stage<P, RIEM, VISC, T>, (unsigned)grid, S::THREADS, s, a, elist, n);
 }
 
 template <int P, bool VISC, typename T>

@@ -187,9 +187,9 @@ __device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;"
 // Launch with programmatic stream serialisation: the kernel (which calls
 // pdl_wait before reading anything a kernel writes) may start while the
 // previous kernel in the stream drains.
-template <typename A>
-cudaError_t launch_programmatic(void (*kernel)(A), unsigned grid, unsigned threads, cudaStream_t s,
-                                const A& a) {
+template <typename... KA, typename... AA>
+cudaError_t launch_programmatic(void (*kernel)(KA...), unsigned grid, unsigned threads, cudaStream_t s,
+                                AA&&... args) {
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3(grid);
     cfg.blockDim = dim3(threads);
@@ -200,7 +200,7 @@ cudaError_t launch_programmatic(void (*kernel)(A), unsigned grid, unsigned threa
     attr[0].val.programmaticStreamSerializationAllowed = 1;
     cfg.attrs = attr;
     cfg.numAttrs = 1;
-    return cudaLaunchKernelEx(&cfg, kernel, a);
+    return cudaLaunchKernelEx(&cfg, kernel, static_cast<AA&&>(args)...);
 }
 
 // Block-wide deterministic sum; result valid in thread 0.
