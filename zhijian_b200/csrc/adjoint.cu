@@ -123,6 +123,8 @@ k_adj_dfbar(const AdjArgs a) {
     const int tid = threadIdx.x;
     if (tid < N1) sW[tid] = -a.ops[N1 * N1 + 2 * N1 + tid];
     else if (tid < 2 * N1) sW[tid] = a.ops[N1 * N1 + 3 * N1 + tid - N1];
+    pdl_launch_dependents();
+    pdl_wait();   // the adjoint input comes from the previous launches
     const int el = tid / TPE, k = tid - el * TPE;
     const long long e = (long long)blockIdx.x * EB + el;
     const bool valid = (el < EB) && (e < a.n_elem);
@@ -149,6 +151,8 @@ k_adj_euler(const AdjArgs a) {
     __shared__ __align__(16) double sTb[EB * DS];
     const int tid = threadIdx.x;
     for (int t = tid; t < S::NOPS; t += blockDim.x) sOps[t] = a.ops[t];
+    pdl_launch_dependents();
+    pdl_wait();   // states, traces and adjoints come from the previous launches
     const int el = tid / TPE, k = tid - el * TPE;
     const long long e = (long long)blockIdx.x * EB + el;
     const bool valid = (el < EB) && (e < a.n_elem);
@@ -234,6 +238,8 @@ k_adj_ns(const AdjArgs a) {
     __shared__ double sRed[32];
     const int tid = threadIdx.x;
     for (int t = tid; t < S::NOPS; t += blockDim.x) sOps[t] = a.ops[t];
+    pdl_launch_dependents();
+    pdl_wait();   // states, traces and adjoints come from the previous launches
     const int el = tid / TPE, k = tid - el * TPE;
     const long long e = (long long)blockIdx.x * EB + el;
     const bool valid = (el < EB) && (e < a.n_elem);
@@ -425,6 +431,8 @@ k_adj_ns_gather(const AdjArgs a) {
     __shared__ __align__(16) double sTb[EB * DS];
     const int tid = threadIdx.x;
     for (int t = tid; t < S::NOPS; t += blockDim.x) sOps[t] = a.ops[t];
+    pdl_launch_dependents();
+    pdl_wait();   // states, traces and adjoints come from the previous launches
     const int el = tid / TPE, k = tid - el * TPE;
     const long long e = (long long)blockIdx.x * EB + el;
     const bool valid = (el < EB) && (e < a.n_elem);
@@ -455,8 +463,7 @@ cudaError_t dfbar_t(const AdjArgs& a, cudaStream_t s) {
     using S = Shape<P>;
     const long long grid = (a.n_elem + S::EB - 1) / S::EB;
     if (grid <= 0) return cudaSuccess;
-    k_adj_dfbar<P><<<(unsigned)grid, S::THREADS, 0, s>>>(a);
-    return cudaGetLastError();
+    return launch_programmatic(k_adj_dfbar<P>, (unsigned)grid, S::THREADS, s, a);
 }
 
 template <int P, int RIEM>
@@ -464,8 +471,7 @@ cudaError_t euler_t(const AdjArgs& a, cudaStream_t s) {
     using S = Shape<P>;
     const long long grid = (a.n_elem + S::EB - 1) / S::EB;
     if (grid <= 0) return cudaSuccess;
-    k_adj_euler<P, RIEM><<<(unsigned)grid, S::THREADS, 0, s>>>(a);
-    return cudaGetLastError();
+    return launch_programmatic(k_adj_euler<P, RIEM>, (unsigned)grid, S::THREADS, s, a);
 }
 
 template <int P, int RIEM>
@@ -473,13 +479,11 @@ cudaError_t ns_t(const AdjArgs& a, cudaStream_t s) {
     using S = Shape<P, 2>;
     const long long grid = (a.n_elem + S::EB - 1) / S::EB;
     if (grid <= 0) return cudaSuccess;
-    k_adj_ns<P, RIEM><<<(unsigned)grid, S::THREADS, 0, s>>>(a);
-    cudaError_t e = cudaGetLastError();
+    cudaError_t e = launch_programmatic(k_adj_ns<P, RIEM>, (unsigned)grid, S::THREADS, s, a);
     if (e != cudaSuccess) return e;
     using S1 = Shape<P>;
     const long long g1 = (a.n_elem + S1::EB - 1) / S1::EB;
-    k_adj_ns_gather<P><<<(unsigned)g1, S1::THREADS, 0, s>>>(a);
-    return cudaGetLastError();
+    return launch_programmatic(k_adj_ns_gather<P>, (unsigned)g1, S1::THREADS, s, a);
 }
 
 template <int P>

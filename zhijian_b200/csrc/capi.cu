@@ -1010,17 +1010,6 @@ zj_status zj_adjoint_run(zj_solver* s, double dt, int nsteps, int k_ckpt, double
         zj_status r = ZJ_OK;
         ZJ_CK(s, cudaMemsetAsync(s->aScal, 0, sizeof(double), s->stream), "clear");
         ZJ_CK(s, cudaMemcpyAsync(X, s->dU[s->cur], sb, cudaMemcpyDeviceToDevice, s->stream), "state copy");
-        // forward sweep with checkpoints every k_ckpt steps
-        ZJ_CK(s, cudaEventRecord(ev[0], s->stream), "event");
-        for (int i = 0; i < nsteps; ++i) {
-            if (i % k_ckpt == 0)
-                ZJ_CK(s, cudaMemcpyAsync(ck + (size_t)(i / k_ckpt) * s->state_n, X, sb,
-                                         cudaMemcpyDeviceToDevice, s->stream), "checkpoint");
-            if ((r = rk3_stages(s, X, s->aS1, s->aS2, X)) != ZJ_OK) return r;
-        }
-        ZJ_CK(s, cudaEventRecord(ev[1], s->stream), "event");
-        // backward sweep: recompute each segment from its checkpoint, then
-        // the step adjoints in reverse
         // segment layout: step m's start state, U(1), U(2) at seg + 3 m states
         auto st_at = [&](int m, int which) { return seg + (size_t)(3 * m + which) * s->state_n; };
         auto traces_at = [&](int m) {
@@ -1032,15 +1021,42 @@ zj_status zj_adjoint_run(zj_solver* s, double dt, int nsteps, int k_ckpt, double
             }
             return t;
         };
+        // forward sweep with checkpoints every k_ckpt steps; the last
+        // segment's steps write their stage states and traces straight into
+        // the segment buffers (the same kernels with other outputs), so the
+        // backward sweep starts without recomputing it
+        const int last_first = (n_ck - 1) * k_ckpt, last_len = nsteps - last_first;
+        ZJ_CK(s, cudaEventRecord(ev[0], s->stream), "event");
+        for (int i = 0; i < nsteps; ++i) {
+            if (i < last_first) {
+                if (i % k_ckpt == 0)
+                    ZJ_CK(s, cudaMemcpyAsync(ck + (size_t)(i / k_ckpt) * s->state_n, X, sb,
+                                             cudaMemcpyDeviceToDevice, s->stream), "checkpoint");
+                if ((r = rk3_stages(s, X, s->aS1, s->aS2, X)) != ZJ_OK) return r;
+                continue;
+            }
+            const int m = i - last_first;
+            if (m == 0)
+                ZJ_CK(s, cudaMemcpyAsync(st_at(0, 0), X, sb, cudaMemcpyDeviceToDevice, s->stream), "segment start");
+            const StageTraces t = traces_at(m);
+            if ((r = rk3_stages(s, st_at(m, 0), st_at(m, 1), st_at(m, 2),
+                                (m + 1 < last_len) ? st_at(m + 1, 0) : X, &t)) != ZJ_OK)
+                return r;
+        }
+        ZJ_CK(s, cudaEventRecord(ev[1], s->stream), "event");
+        // backward sweep: recompute each earlier segment from its checkpoint,
+        // then the step adjoints in reverse
         for (int c = n_ck - 1; c >= 0; --c) {
             const int first = c * k_ckpt, len = std::min(k_ckpt, nsteps - first);
-            ZJ_CK(s, cudaMemcpyAsync(st_at(0, 0), ck + (size_t)c * s->state_n, sb, cudaMemcpyDeviceToDevice,
-                                     s->stream), "segment start");
-            for (int m = 0; m < len; ++m) {
-                const StageTraces t = traces_at(m);
-                if ((r = rk3_stages(s, st_at(m, 0), st_at(m, 1), st_at(m, 2),
-                                    (m + 1 < len) ? st_at(m + 1, 0) : nullptr, &t)) != ZJ_OK)
-                    return r;
+            if (c < n_ck - 1) {
+                ZJ_CK(s, cudaMemcpyAsync(st_at(0, 0), ck + (size_t)c * s->state_n, sb,
+                                         cudaMemcpyDeviceToDevice, s->stream), "segment start");
+                for (int m = 0; m < len; ++m) {
+                    const StageTraces t = traces_at(m);
+                    if ((r = rk3_stages(s, st_at(m, 0), st_at(m, 1), st_at(m, 2),
+                                        (m + 1 < len) ? st_at(m + 1, 0) : nullptr, &t)) != ZJ_OK)
+                        return r;
+                }
             }
             for (int m = len - 1; m >= 0; --m) {
                 const StageTraces t = traces_at(m);
