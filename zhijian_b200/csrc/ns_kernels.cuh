@@ -93,6 +93,41 @@ __device__ __forceinline__ void corrected_gradient(const T* su, const T* du, con
     }
 }
 
+// The same gradient with the element's tile also held transposed (sut:
+// [var][xi][eta]), so the eta-line of point (i, j) is a row: vector loads
+// instead of N1 strided ones; the sums run in the same order.
+template <int N1, int RS, int VS, typename T>
+__device__ __forceinline__ void corrected_gradient_tr(const T* su, const T* sut, const T* du, const T* ops,
+                                                      int i, int j, const T* ji, T* Qx, T* Qy) {
+    const T* gL = ops + N1 * N1 + 2 * N1;
+    const T* gR = gL + N1;
+    T Di[N1], Dj[N1];
+#pragma unroll
+    for (int m = 0; m < N1; ++m) { Di[m] = ops[i * N1 + m]; Dj[m] = ops[j * N1 + m]; }
+    T d1[4], d3[4], d0[4], d2[4];
+    load4(du + (1 * N1 + j) * 4, d1);
+    load4(du + (3 * N1 + (N1 - 1 - j)) * 4, d3);
+    load4(du + (0 * N1 + i) * 4, d0);
+    load4(du + (2 * N1 + (N1 - 1 - i)) * 4, d2);
+    const T gRi = gR[i], gLi = gL[i], gRj = gR[j], gLj = gL[j];
+#pragma unroll
+    for (int v = 0; v < 4; ++v) {
+        T row[N1], col[N1];
+        load_row<N1>(su + v * VS + j * RS, row);
+        load_row<N1>(sut + v * VS + i * RS, col);
+        T dxi = T(0), deta = T(0);
+#pragma unroll
+        for (int m = 0; m < N1; ++m) {
+            dxi = fma_any(Di[m], row[m], dxi);
+            deta = fma_any(Dj[m], col[m], deta);
+        }
+        dxi += gRi * d1[v] + gLi * d3[v];
+        deta += gLj * d0[v] + gRj * d2[v];
+        Qx[v] = ji[0] * dxi + ji[2] * deta;
+        Qy[v] = ji[1] * dxi + ji[3] * deta;
+    }
+}
+
 // Loads of a flux-point thread: edge record, normal, own trace, the
 // neighbour's coinciding trace point or the ghost state.
 template <typename T>
@@ -128,6 +163,7 @@ k_ns_grad(const StageArgsT<T> a) {
     constexpr int QS = Tiles<P, T>::QS;
     __shared__ T sOps[S::NOPS];
     __shared__ __align__(16) T sU[EB * FS];
+    __shared__ __align__(16) T sUt[EB * FS];   // the same tile transposed
     __shared__ __align__(16) T sDU[EB * DS];
     __shared__ __align__(16) T sQ[EB * QS];
 
@@ -160,8 +196,9 @@ k_ns_grad(const StageArgsT<T> a) {
         }
         load4_nc(a.Jinv + idx * 4, ji);
         T* su = sU + el * FS + j * RS + i;
+        T* sut = sUt + el * FS + i * RS + j;
 #pragma unroll
-        for (int v = 0; v < 4; ++v) su[v * VS] = u[v];
+        for (int v = 0; v < 4; ++v) { su[v * VS] = u[v]; sut[v * VS] = u[v]; }
     }
     if (is_fp) {
         FacePoint<T> f;
@@ -174,7 +211,7 @@ k_ns_grad(const StageArgsT<T> a) {
     __syncthreads();
     if (is_sp) {
         T Qx[4], Qy[4];
-        corrected_gradient<N1, RS, VS>(sU + el * FS, sDU + el * DS, sOps, i, j, ji, Qx, Qy);
+        corrected_gradient_tr<N1, RS, VS>(sU + el * FS, sUt + el * FS, sDU + el * DS, sOps, i, j, ji, Qx, Qy);
         T* sq = sQ + el * QS + j * RS + i;
 #pragma unroll
         for (int v = 0; v < 4; ++v) { sq[v * VS] = Qx[v]; sq[(4 + v) * VS] = Qy[v]; }
