@@ -147,7 +147,19 @@ def test_null_arguments(zjlib):
     assert zjlib.zj_last_error(None)
     assert zjlib.zj_step(None, 0.1, 1) == L.ERR_ARG
     assert zjlib.zj_rhs(None, None, None) == L.ERR_ARG
+    assert zjlib.zj_set_state_async(None, None) == L.ERR_ARG
+    assert zjlib.zj_get_state_async(None, None) == L.ERR_ARG
     zjlib.zj_solver_destroy(None)
+
+
+def test_empty_mesh_rejected(zjlib):
+    """A mesh without elements (or without nodes) is refused with an argument
+    error before any device work."""
+    m = M.vortex_mesh(2)
+    empty = M.QuadMesh(m.xy, m.conn[:0].copy(), m.bnd[:0].copy(), m.tag_names)
+    with pytest.raises(L.ZJError) as e:
+        _create(empty, make_params())
+    assert e.value.code == L.ERR_ARG and "empty mesh" in str(e.value)
 
 
 def _has_gpu():
