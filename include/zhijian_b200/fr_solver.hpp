@@ -75,6 +75,17 @@ public:
         n_elem_ = zj_num_elements(s_);
     }
 
+    // The mesh from a Gmsh file (GmshReader::read, gmsh_reader.cpp:161-760, as
+    // main.cpp's -m option loads it), boundary types from its physical names.
+    void initializeFromGmsh(const std::string& path, const zj_params& params) {
+        zj_solver_destroy(s_);
+        s_ = nullptr;
+        check(zj_solver_create_from_gmsh(path.c_str(), &params, &s_), nullptr);
+        params_ = params;
+        n_sp_ = zj_num_solution_points(s_);
+        n_elem_ = zj_num_elements(s_);
+    }
+
     // FRSolver::setInitialCondition(std::function<State(Vec2)>) (fr_solver.cpp:268-299)
     void setInitialCondition(const std::function<State(Vec2)>& ic) {
         std::vector<double> xy((size_t)n_elem_ * n_sp_ * 2);

@@ -66,3 +66,35 @@ def test_driver_restart_resumes(zjlib, tmp_path):
                              check=True).stdout
     assert full.splitlines()[-1] == resumed.splitlines()[-1]          # bit-identical checksum
     assert full.splitlines()[-2].split()[:2] == resumed.splitlines()[-2].split()[:2]   # iteration, time
+
+
+@pytest.mark.gpu
+def test_driver_reads_gmsh_mesh(zjlib, tmp_path):
+    """zj_run -m <file.msh>: the mesh from a Gmsh file (triangles and quads, in
+    physics mode), the same steps and state as the Python binding's
+    FRSolver.from_gmsh with the same parameters."""
+    from zhijian_b200.solver import FRSolver, make_params
+    exe = build.build_driver()
+    msh = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "gmsh", "triquad_v41.msh")
+    cfg = tmp_path / "c.txt"
+    cfg.write_text("gamma 1.4\nrho_inf 1.2\np_inf 100000.0\nMach 0.3\nAoA 5.0\npoly_order 3\n"
+                   "flux_type SD\nriemann Roe\ncompat off\nviscous true\nRe 200\nPr 0.72\ndt 1e-6\n")
+    out = subprocess.run([exe, str(cfg), "-m", msh, "4"], capture_output=True, text=True,
+                         check=True).stdout.splitlines()
+    chk = float(out[-1].split()[1])
+    prm = make_params(poly_order=3, rho_inf=1.2, p_inf=1.0e5, Mach=0.3, AoA=5.0, flux_type="SD",
+                      riemann="Roe", compat=False, viscous=True, Re=200.0, Pr=0.72)
+    s = FRSolver.from_gmsh(msh, prm)
+    s.setInitialCondition(lambda xy: _uniform(xy, 1.2, 1.0e5, 0.3, 5.0))
+    s.advance(1e-6, 4)
+    U = s.copyToHost()
+    assert abs(np.abs(U).sum() - chk) <= 1e-12 * chk
+
+
+def _uniform(xy, rho, p, mach, aoa, g=1.4):
+    import math
+    from zhijian_b200 import meshgen as M
+    c = math.sqrt(g * p / rho)
+    u, v = mach * c * math.cos(math.radians(aoa)), mach * c * math.sin(math.radians(aoa))
+    shp = xy.shape[:-1]
+    return M.prim_to_cons(np.full(shp, rho), np.full(shp, u), np.full(shp, v), np.full(shp, p), g)

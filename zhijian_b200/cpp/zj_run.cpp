@@ -3,8 +3,10 @@
 // reference grammar, a structured quad mesh, uniform-flow or isentropic-vortex
 // initial state, then computeTimeStep -> advance -> computeResidual.
 //
-//   zj_run <config> <nx> <ny> <x0> <x1> <y0> <y1> [steps] [vortex]
+//   zj_run <config> (<nx> <ny> <x0> <x1> <y0> <y1> | -m <mesh.msh>) [steps] [vortex]
 //          [-r <restart file>] [-w <restart file>]
+// -m reads the mesh from a Gmsh file as the reference's -m does (boundary
+// types from the physical names); otherwise a structured quad mesh.
 // prints "iter time dt residual" every 10 iterations and the final state
 // checksum (sum of |U|) on the last line.  -r resumes from a restart file
 // (state, time, iteration; src/main.cpp:345-360), -w writes one every
@@ -43,8 +45,10 @@ static Mesh structured(int nx, int ny, double x0, double x1, double y0, double y
 }
 
 int main(int argc, char** argv) {
-    if (argc < 8) {
-        std::fprintf(stderr, "usage: zj_run <config> <nx> <ny> <x0> <x1> <y0> <y1> [steps] [vortex]\n");
+    const bool from_file = argc >= 4 && std::string(argv[2]) == "-m";
+    if (!from_file && argc < 8) {
+        std::fprintf(stderr, "usage: zj_run <config> (<nx> <ny> <x0> <x1> <y0> <y1> | -m <mesh.msh>) "
+                             "[steps] [vortex] [-r <restart>] [-w <restart>]\n");
         return 1;
     }
     zj_params p;
@@ -55,18 +59,22 @@ int main(int argc, char** argv) {
     }
     std::string restart_in, restart_out;
     std::vector<std::string> pos;
-    for (int a = 8; a < argc; ++a) {
+    for (int a = from_file ? 4 : 8; a < argc; ++a) {
         const std::string arg = argv[a];
         if ((arg == "-r" || arg == "-w") && a + 1 < argc) (arg == "-r" ? restart_in : restart_out) = argv[++a];
         else pos.push_back(arg);
     }
     const int steps = pos.size() > 0 ? std::atoi(pos[0].c_str()) : p.max_iter;
     const bool vortex = pos.size() > 1 && pos[1] == "vortex";
-    Mesh mesh = structured(std::atoi(argv[2]), std::atoi(argv[3]), std::atof(argv[4]), std::atof(argv[5]),
-                           std::atof(argv[6]), std::atof(argv[7]));
     try {
         FRSolver solver;
-        solver.initialize(mesh, p);
+        if (from_file) {
+            solver.initializeFromGmsh(argv[3], p);
+        } else {
+            Mesh mesh = structured(std::atoi(argv[2]), std::atoi(argv[3]), std::atof(argv[4]),
+                                   std::atof(argv[5]), std::atof(argv[6]), std::atof(argv[7]));
+            solver.initialize(mesh, p);
+        }
         const double g = p.gamma;
         const double c = std::sqrt(g * p.p_inf / p.rho_inf);
         const double u_inf = p.Mach * c * std::cos(p.AoA * M_PI / 180.0);
