@@ -1,12 +1,12 @@
 """A few SSP-RK3 steps of the benchmark's cases, for external profilers (ncu)
 that capture a handful of launches:
 
-    python -m zhijian_b200.profile_case {ns|ns32|euler|euler32|compat|shear|shear32} [steps] [n]
+    python -m zhijian_b200.profile_case {ns|ns32|euler|euler32|compat|shear|shear32} [steps] [n] [P]
 
 ns / ns32: Navier-Stokes (Re 5000, Pr 0.72, Roe, HU), FP64 / precision form;
 euler / euler32: the inviscid physics-mode residual; compat: the reference
 residual semantics.  256x256 jittered Q1 quads on [0,pi]^2 (seed 1), P3,
-slip walls, dt = 2e-4 (n overrides the mesh size).
+slip walls, dt = 2e-4 (n overrides the mesh size, P the order; above P3 dt = 3e-5).
 shear / shear32: the mixed-element shear layer (n x n quads, default 384, a
 seeded 30% split into triangles; Navier-Stokes Re 2000, HLLC, GA, P3) at
 CFL 0.1, FP64 / precision form."""
@@ -47,12 +47,13 @@ def main(argv):
     if mode in ("shear", "shear32"):
         return shear(mode, steps, int(argv[3]) if len(argv) > 3 else 384)
     n = int(argv[3]) if len(argv) > 3 else 256
+    order = int(argv[4]) if len(argv) > 4 else 3
     mesh = M.tgv_mesh(n, seed=1)
-    prm = make_params(poly_order=3, gamma=GAMMA, rho_inf=1.0, p_inf=1.0 / (GAMMA * MACH * MACH),
+    prm = make_params(poly_order=order, gamma=GAMMA, rho_inf=1.0, p_inf=1.0 / (GAMMA * MACH * MACH),
                       Mach=MACH, bcs=[(1, "slipwall")], **MODES[mode])
     s = FRSolver(mesh, prm)
     s.copyToDevice(M.taylor_green(s.solution_point_coords()))
-    s.advance(2.0e-4, steps)
+    s.advance(2.0e-4 if order <= 3 else 3.0e-5, steps)
     s.check_state()
     print(f"{mode}: {steps} steps on {mesh.n_elem} elements, residual norm {s.computeResidual():.6e}")
     return 0 if math.isfinite(s.computeResidual()) else 1
