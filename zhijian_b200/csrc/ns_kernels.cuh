@@ -235,6 +235,9 @@ k_ns_stage(const StageArgsT<T> a) {
     constexpr int N1 = S::N1, NSP = S::NSP, NFT = S::NFT, TPE = S::TPE, EB = S::EB;
     constexpr int RS = S::RS, VS = S::VS, FS = Tiles<P, T>::FS, DS = Tiles<P, T>::DS;
     __shared__ T sOps[S::NOPS];
+    // From P4 up the G~ tile is held transposed ([var][xi][eta]), so its
+    // eta-lines (divergence, traces of edges 0 and 2) are row loads
+    constexpr bool kTrG = P >= 4;
     __shared__ __align__(16) T sF[EB * FS];
     __shared__ __align__(16) T sG[EB * FS];
     __shared__ __align__(16) T sD[EB * DS];   // face jumps of U, then flux differences
@@ -312,7 +315,7 @@ k_ns_stage(const StageArgsT<T> a) {
 #pragma unroll
         for (int v = 0; v < 4; ++v) { F[v] -= Fv[v]; G[v] -= Gv[v]; }
         T* fo = sF + el * FS + j * RS + i;
-        T* ho = sG + el * FS + j * RS + i;
+        T* ho = sG + el * FS + (kTrG ? i * RS + j : j * RS + i);
 #pragma unroll
         for (int v = 0; v < 4; ++v) {
             fo[v * VS] = Jd * (ji[0] * F[v] + ji[1] * G[v]);
@@ -351,8 +354,13 @@ k_ns_stage(const StageArgsT<T> a) {
             const T ss = right ? T(-0.5) * f.len : T(0.5) * f.len;
             const bool along_eta = (edge == 0 || edge == 2);
             T Fn[4];
-            trace_point<N1, RS, VS>((along_eta ? sG : sF) + el * FS, sOps + N1 * N1,
-                                    sOps + N1 * N1 + N1, edge, fp, Fn);
+            if constexpr (kTrG)
+                trace_row<N1, RS, VS>((along_eta ? sG : sF) + el * FS,
+                                      (edge == 0 || edge == 3) ? sOps + N1 * N1 : sOps + N1 * N1 + N1,
+                                      (edge >= 2) ? (N1 - 1 - fp) : fp, Fn);
+            else
+                trace_point<N1, RS, VS>((along_eta ? sG : sF) + el * FS, sOps + N1 * N1,
+                                        sOps + N1 * N1 + N1, edge, fp, Fn);
             const T sgn = (edge == 0 || edge == 3) ? T(-1) : T(1);
 #pragma unroll
             for (int v = 0; v < 4; ++v)
@@ -391,8 +399,15 @@ k_ns_stage(const StageArgsT<T> a) {
             T div = T(0);
 #pragma unroll
             for (int m = 0; m < N1; ++m) div = fma_any(Di[m], fr[m], div);
+            if constexpr (kTrG) {
+                T gc[N1];
+                load_row<N1>(ho + v * VS + i * RS, gc);
 #pragma unroll
-            for (int m = 0; m < N1; ++m) div = fma_any(Dj[m], ho[v * VS + m * RS + i], div);
+                for (int m = 0; m < N1; ++m) div = fma_any(Dj[m], gc[m], div);
+            } else {
+#pragma unroll
+                for (int m = 0; m < N1; ++m) div = fma_any(Dj[m], ho[v * VS + m * RS + i], div);
+            }
             const T corr = gRi * c1[v] - gLi * c3[v] + gRj * c2[v] - gLj * c0[v];
             res[v] = -(div + corr) * iJ;
         }

@@ -203,6 +203,25 @@ cudaError_t launch_programmatic(void (*kernel)(KA...), unsigned grid, unsigned t
     return cudaLaunchKernelEx(&cfg, kernel, static_cast<AA&&>(args)...);
 }
 
+// Trace of one flux point from row `line` of a [var][row][col] tile (weights W
+// over the columns), with the row loads of load_row; the sum runs in the
+// order of trace_point, so the two agree bit for bit on the same values.
+template <int N1, int RS, int VS, typename T>
+__device__ __forceinline__ void trace_row(const T* s, const T* W, int line, T* out) {
+    T w[N1];
+#pragma unroll
+    for (int m = 0; m < N1; ++m) w[m] = W[m];
+#pragma unroll
+    for (int v = 0; v < 4; ++v) {
+        T r[N1];
+        load_row<N1>(s + v * VS + line * RS, r);
+        T t = T(0);
+#pragma unroll
+        for (int m = 0; m < N1; ++m) t = fma_any(w[m], r[m], t);
+        out[v] = t;
+    }
+}
+
 // Block-wide deterministic sum; result valid in thread 0.
 __device__ __forceinline__ double block_sum(double x, double* red) {
 #pragma unroll
