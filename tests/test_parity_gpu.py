@@ -1,7 +1,7 @@
 """Parity of the CUDA path (through the C-ABI) with the oracle and with the
 reference's own CUDA build, FP64 compat mode.
 
-Bar (north star): max |R - R_ref| / max(max|R_ref|, s_F) <= 1e-12 per
+Bar: max |R - R_ref| / max(max|R_ref|, s_F) <= 1e-12 per
 variable per residual evaluation, s_F = max|F| * max|metric|.
 """
 import os
