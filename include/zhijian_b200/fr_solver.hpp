@@ -140,6 +140,8 @@ public:
     void copyToDeviceAsync(const double* U) { check(zj_set_state_async(s_, U), s_); }
     void copyToHostAsync(double* U) { check(zj_get_state_async(s_, U), s_); }
     void synchronize() { check(zj_synchronize(s_), s_); }
+    // Blocks of six steps replayed from captured CUDA graphs (default on).
+    void setStepGraphs(bool enable) { check(zj_set_step_graphs(s_, enable ? 1 : 0), s_); }
 
     const zj_params& params() const { return params_; }
     zj_solver* handle() { return s_; }

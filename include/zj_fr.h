@@ -165,6 +165,14 @@ zj_status zj_get_state_async(zj_solver* s, double* U_host);
  * queued on the handle's stream; returns once the steps are enqueued and
  * checked for launch errors.  zj_synchronize waits for them. */
 zj_status zj_step(zj_solver* s, double dt, int nsteps);
+/* Step graphs (no reference counterpart): zj_step replays blocks of six steps
+ * from CUDA graphs captured on the handle's stream at first use (one graph per
+ * phase of the rotating stage and trace buffers, at most six per handle), so a
+ * long zj_step costs one launch per six steps instead of six to twelve; the
+ * handle's first step, remainders, the legacy default stream and a stream the
+ * caller is capturing launch kernels directly, with identical results.
+ * enable = 0 turns the graphs off for this handle. */
+zj_status zj_set_step_graphs(zj_solver* s, int enable);
 zj_status zj_synchronize(zj_solver* s);
 /* One residual R = dU/dt on device buffers of E*n_sp*4 doubles, on the
  * handle's stream (computeResidual_GPU, fr_solver.cpp:335-608).  Borrowed. */

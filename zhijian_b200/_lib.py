@@ -79,6 +79,7 @@ def lib():
         "zj_set_state": (ip, [vp, dp]),
         "zj_get_state": (ip, [vp, dp]),
         "zj_set_state_async": (ip, [vp, vp]),
+        "zj_set_step_graphs": (ip, [vp, ip]),
         "zj_get_state_async": (ip, [vp, vp]),
         "zj_set_state_device": (ip, [vp, vp]),
         "zj_get_state_device": (ip, [vp, vp]),

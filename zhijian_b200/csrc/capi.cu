@@ -105,6 +105,13 @@ struct zj_solver {
     int grid = 0;
     int cur = 0, tpar = 0;
     bool traces_valid = false;
+    // Step graphs: the stage buffers rotate with period 3 and the trace
+    // buffers with period 2, so six steps return to the starting (cur, tpar);
+    // one captured 6-step block per starting phase, replayed by zj_step.
+    cudaGraphExec_t gexec[6] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
+    bool graphs_on = true;      // zj_set_step_graphs
+    bool graphs_failed = false; // a capture failed: plain launches from then on
+    bool stepped = false;       // a plain step ran (the kernels' one-time attributes are set)
     bool has_norm = false;
     cudaStream_t own = nullptr, stream = nullptr;
     double time = 0.0;
@@ -163,6 +170,7 @@ void free_all(zj_solver* s) {
     if (s->dEdges) cudaFree(s->dEdges);
     if (s->dNrm) cudaFree(s->dNrm);
     s->dFlag = nullptr; s->dEdges = nullptr; s->dNrm = nullptr;
+    for (auto& g : s->gexec) { if (g) cudaGraphExecDestroy(g); g = nullptr; }
     if (s->own) cudaStreamDestroy(s->own);
     s->own = nullptr;
 }
@@ -295,17 +303,68 @@ zj_status enqueue_step(zj_solver* s) {
     return ZJ_OK;
 }
 
+constexpr int kGraphSteps = 6;
+
+// The 6-step block starting at the handle's (cur, tpar), captured on first
+// use; nullptr where graphs cannot be used: the legacy default stream (not
+// capturable), a stream the caller is capturing (the plain launches join the
+// caller's graph), or a failed capture (plain launches from then on).
+template <typename T>
+cudaGraphExec_t step_graph(zj_solver* s) {
+    if (!s->graphs_on || s->graphs_failed || !s->stepped || s->stream == nullptr) return nullptr;
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    if (cudaStreamIsCapturing(s->stream, &cs) != cudaSuccess || cs != cudaStreamCaptureStatusNone) return nullptr;
+    const int idx = s->cur * 2 + s->tpar;
+    if (s->gexec[idx]) return s->gexec[idx];
+    const int cur0 = s->cur, tpar0 = s->tpar;
+    const std::string err0 = s->err;
+    if (cudaStreamBeginCapture(s->stream, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
+        (void)cudaGetLastError();
+        s->graphs_failed = true;
+        return nullptr;
+    }
+    zj_status st = ZJ_OK;
+    for (int k = 0; k < kGraphSteps && st == ZJ_OK; ++k) st = enqueue_step<T>(s);
+    cudaGraph_t graph = nullptr;
+    cudaError_t e = cudaStreamEndCapture(s->stream, &graph);
+    s->cur = cur0;       // six steps come back to the starting phase; nothing ran yet
+    s->tpar = tpar0;
+    cudaGraphExec_t exec = nullptr;
+    if (st == ZJ_OK && e == cudaSuccess && graph) e = cudaGraphInstantiate(&exec, graph, 0);
+    if (graph) cudaGraphDestroy(graph);
+    if (st != ZJ_OK || e != cudaSuccess || !exec) {
+        (void)cudaGetLastError();
+        if (exec) cudaGraphExecDestroy(exec);
+        s->err = err0;
+        s->graphs_failed = true;
+        return nullptr;
+    }
+    s->gexec[idx] = exec;
+    return exec;
+}
+
 template <typename T>
 zj_status step_impl(zj_solver* s, int nsteps, double dt) {
     if (!s->traces_valid) {
         ZJ_CK(s, launch_trace_any(s, s->dU[s->cur], tbuf<T>(s, s->tpar)), "trace launch");
         s->traces_valid = true;
     }
-    for (int k = 0; k < nsteps; ++k) {
-        zj_status st = enqueue_step<T>(s);
-        if (st != ZJ_OK) return st;
-        s->time += dt;
-        s->iter += 1;
+    // blocks of six steps replay a captured graph (one launch instead of six
+    // to twelve); the rest, and the handle's first step, launch directly
+    for (int k = 0; k < nsteps;) {
+        cudaGraphExec_t g = (nsteps - k >= kGraphSteps) ? step_graph<T>(s) : nullptr;
+        if (g) {
+            ZJ_CK(s, cudaGraphLaunch(g, s->stream), "step graph launch");
+            for (int i = 0; i < kGraphSteps; ++i) { s->time += dt; s->iter += 1; }
+            k += kGraphSteps;
+        } else {
+            zj_status st = enqueue_step<T>(s);
+            if (st != ZJ_OK) return st;
+            s->time += dt;
+            s->iter += 1;
+            s->stepped = true;
+            ++k;
+        }
     }
     return ZJ_OK;
 }
@@ -532,6 +591,12 @@ zj_status zj_set_stream(zj_solver* s, void* stream) {
 }
 
 void* zj_get_stream(const zj_solver* s) { return s ? static_cast<void*>(s->stream) : nullptr; }
+
+zj_status zj_set_step_graphs(zj_solver* s, int enable) {
+    if (!s) return ZJ_ERR_ARG;
+    s->graphs_on = enable != 0;
+    return ZJ_OK;
+}
 
 zj_status zj_set_state(zj_solver* s, const double* U) {
     if (!s || !U) return ZJ_ERR_ARG;

@@ -179,6 +179,10 @@ class FRSolver:
         if sync:
             self.synchronize()
 
+    def set_step_graphs(self, enable: bool):
+        """Replay blocks of six steps from captured CUDA graphs (default on)."""
+        self._ck(L.lib().zj_set_step_graphs(self.h, int(bool(enable))))
+
     def synchronize(self):
         self._ck(L.lib().zj_synchronize(self.h))
 
