@@ -76,3 +76,22 @@ def test_steps_inside_a_caller_graph(zjlib):
         res.append(s.copyToHost())
         s.close()
     assert np.array_equal(res[0], res[1])
+
+
+def test_legacy_default_stream_steps_plainly(zjlib):
+    """On the legacy default stream (not capturable) zj_step launches
+    directly; the result equals the graphs-off handle's."""
+    mesh, prm = cases()["ns_fp64"]
+    res = []
+    for legacy in (True, False):
+        s = FRSolver(mesh, prm)
+        if legacy:
+            s.set_stream(0)
+        else:
+            s.set_step_graphs(False)
+        s.setInitialCondition(M.taylor_green)
+        dt = 0.2 * s.computeTimeStep()
+        s.advance(dt, 14)
+        res.append((s.copyToHost(), s.iteration))
+        s.close()
+    assert np.array_equal(res[0][0], res[1][0]) and res[0][1] == res[1][1] == 14
