@@ -184,13 +184,6 @@ def make_oracle(mesh, mode, threads):
     return orc, step
 
 
-def sample_block():
-    """A 64x64-element block of the benchmark mesh's density (the CPU sample)."""
-    from zhijian_b200 import meshgen as M
-    return M.structured_quads(64, 64, 0.0, math.pi / 4, 0.0, math.pi / 4, 0.15, 1, (1, 1, 1, 1),
-                              {1: "slipwall"})
-
-
 def cpu_model():
     try:
         with open("/proc/cpuinfo") as f:
@@ -202,71 +195,67 @@ def cpu_model():
     return "unknown"
 
 
-def oracle_rate(mode, seconds, runs=5):
-    """Median DOF-RHS/s of `runs` timed runs (each up to seconds/runs, at
-    most 200 steps) of the oracle on the sample block, after one warm-up step."""
+def oracle_rate(mesh, mode, warmup=1, runs=5, run_seconds=2.0, min_steps=1):
+    """The oracle (FP64, all host threads) on the full benchmark mesh: `warmup`
+    untimed SSP-RK3 steps, then `runs` timed runs of at least `min_steps`
+    steps and `run_seconds` seconds each; returns the median DOF-RHS/s, the
+    per-run rates, the median ms per step, the steps timed and the threads."""
     from zhijian_b200 import meshgen as M
     threads = os.cpu_count() or 1
-    sub = sample_block()
-    orc, step = make_oracle(sub, mode, threads)
+    orc, step = make_oracle(mesh, mode, threads)
     U = M.taylor_green(orc.sp_coords())
-    U, _ = step(U, DT, 1)  # warm-up
-    dof = sub.n_elem * (P + 1) ** 2
-    rates, steps = [], 0
+    for _ in range(max(1, warmup)):
+        U, _ = step(U, DT, 1)
+    dof = mesh.n_elem * (P + 1) ** 2
+    rates, ms, steps = [], [], 0
     for _ in range(runs):
         n, t0 = 0, time.perf_counter()
         while True:
             U, _ = step(U, DT, 1)
             n += 1
             el = time.perf_counter() - t0
-            if el >= seconds / runs or n >= 200:
+            if n >= min_steps and el >= run_seconds:
                 break
         rates.append(dof * 3 * n / el)
+        ms.append(1e3 * el / n)
         steps += n
-    return statistics.median(rates), rates, steps, sub.n_elem, threads
+    return statistics.median(rates), rates, statistics.median(ms), steps, threads
 
 
 def cpu_baseline(mesh, seconds=10.0, mode="ns"):
-    """The oracle (FP64, the benchmark's mode) on the host cores over a
-    bounded sample -- SSP-RK3 steps on a 64x64-element block of the same mesh
-    density -- as the median of five runs after a warm-up; beside it the same
-    for the reference's residual semantics (compat mode), and the CPU model."""
-    v, rates, steps, ne, threads = oracle_rate(mode, seconds)
-    vc, _, steps_c, _, _ = oracle_rate("compat", seconds / 2)
+    """The oracle (FP64 Navier-Stokes, the benchmark's scheme) on the host
+    cores over the full benchmark mesh: median of five runs of about
+    seconds/5 each after a warm-up step, with the spread and the CPU model;
+    beside it the same for the reference's residual semantics (compat)."""
+    v, rates, _, steps, threads = oracle_rate(mesh, mode, run_seconds=seconds / 5)
+    vc, _, _, steps_c, _ = oracle_rate(mesh, "compat", run_seconds=seconds / 10)
     return {"value": v, "unit": UNIT, "cores": threads, "kind": "port",
-            "sample": f"median of 5 runs ({steps} SSP-RK3 steps in all) of a 64x64 jittered P{P} TGV "
-                      f"block ({ne} elements, {mode}); spread {min(rates):.3g}-{max(rates):.3g}",
-            "cpu": cpu_model(), "compat_value": vc,
-            "compat_sample": f"median of 5 runs ({steps_c} steps), same block, reference residual semantics"}
+            "sample": f"median of 5 runs ({steps} SSP-RK3 steps in all) on the full mesh; "
+                      f"spread {min(rates):.3g}-{max(rates):.3g}",
+            "cpu": cpu_model(), "compat_value": vc}
 
 
 def run_reference(args):
-    """--impl reference: the oracle port with all host threads, rank 0 only."""
+    """--impl reference: the oracle port (the reference has no CPU path) with
+    all host threads on the benchmark's workload, rank 0 only: W warm-up
+    steps, then the median of five timed runs of at least max(K/5, 1) steps
+    and 2 s each."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return None
-    from zhijian_b200 import meshgen as M
-    threads = os.cpu_count() or 1
-    sub = sample_block()
-    orc, step = make_oracle(sub, "ns", threads)
-    U = M.taylor_green(orc.sp_coords())
-    for _ in range(args.warmup):
-        U, _ = step(U, DT, 1)
-    t0 = time.perf_counter()
-    for _ in range(args.steps):
-        U, _ = step(U, DT, 1)
-    el = time.perf_counter() - t0
-    dof = sub.n_elem * (P + 1) ** 2
-    v = dof * 3 * args.steps / el
+    mesh = build_case()
+    v, rates, ms, steps, threads = oracle_rate(mesh, "ns", warmup=args.warmup,
+                                               run_seconds=getattr(args, "run_seconds", 2.0),
+                                               min_steps=max(1, args.steps // 5))
     return {"metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": 1e3 * el / args.steps, "higher_is_better": True,
+            "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
             "impl": "reference",
-            "config": {"workload": workload_name() + " (CPU sample: 64x64 block per step)",
-                       "mode": "ns", "precision": "fp64"},
+            "config": {"workload": workload_name("ns"), "precision": "fp64",
+                       "elements": mesh.n_elem, "dof_per_var": mesh.n_elem * (P + 1) ** 2},
             "cpu_baseline": {"value": v, "unit": UNIT, "cores": threads, "kind": "port",
-                             "sample": f"each step: one SSP-RK3 step of a 64x64 jittered block "
-                                       f"({sub.n_elem} elements, P{P})"},
+                             "sample": f"median of 5 runs ({steps} SSP-RK3 steps in all) on the full "
+                                       f"mesh; spread {min(rates):.3g}-{max(rates):.3g}"},
             "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
 
 
@@ -461,24 +450,43 @@ def run_ours(args):
 
     out = None
     if rank == 0:
+        detail = {"fp64": fp64, "compat": compat, "precision_errors": precision, "adjoint": adjoint,
+                  "p5_precision": p5, "mixed_elements": shear, "e2e": e2e, "roofline": roofline}
         out = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
                "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
                "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
                "dtype": "f32", "data": "synthetic",
                "config": {"workload": workload_name("ns") + ", precision form", "elements": mesh.n_elem,
-                          "dof_per_var": dof, "rhs_per_step": 3, "mode": head,
-                          "precision": "mixed: FP32 volume/face/gradient/operator work; FP64 state, "
-                                       "SSP-RK3 accumulation, norm reductions, metrics built in FP64",
-                          "dt": DT,
+                          "dof_per_var": dof, "rhs_per_step": 3,
+                          "precision": "FP32 volume/face/gradient/operator work; FP64 state, RK, norms",
                           "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
                           "l2": "no flush: each stage streams > 200 MB > 126 MB L2"},
-               "roofline": roofline, "e2e": e2e, "gpu_launches": launches, "clocks": clocks,
-               "fp64": fp64, "speedup_vs_fp64": value / fp64["value"],
-               "precision_errors": precision,
-               "adjoint_forward_ratio": adjoint["ratio"] if adjoint else None,
-               "adjoint": adjoint, "p5_precision": p5, "mixed_elements": shear, "compat": compat}
+               "roofline": {k: roofline[k] for k in ("bound", "achieved", "peak", "unit", "frac", "traffic",
+                                                     "peak_kind", "kernel")},
+               "e2e": {k: e2e[k] for k in ("value", "unit", "h2d_bytes_per_step", "d2h_bytes_per_step")},
+               "e2e_serial": e2e["serial"]["value"],
+               "gpu_launches": launches, "clocks": clocks,
+               "fp64_value": fp64["value"], "fp64_frac": roof64["frac"],
+               "speedup_vs_fp64": value / fp64["value"],
+               "compat_value": compat["value"], "compat_frac": roofc["frac"]}
+        if precision:
+            out["l2_err_1000"] = precision["l2"]
+            out["linf_err_1000"] = precision["linf"]
+        if adjoint:
+            out["adjoint_forward_ratio"] = adjoint["ratio"]
+            out["adjoint_fd_err"] = adjoint["fd_check"]["max_rel_err"]
+        if p5:
+            out["p5_value"] = p5["mixed"]["value"]
+            out["p5_speedup_vs_fp64"] = p5["speedup_vs_fp64"]
+            if "errors" in p5:
+                out["p5_l2_err_1000"] = p5["errors"]["l2"]
+        if shear:
+            out["mixed_mesh_speedups"] = [round(c["speedup_vs_fp64"], 3) for c in shear["cases"]]
         if world == 1 and not args.no_cpu_baseline:
             out["cpu_baseline"] = cpu_baseline(mesh, args.cpu_seconds, "ns")
+        if args.detail:
+            with open(args.detail, "w") as f:
+                json.dump(dict(out, detail=detail), f, indent=1)
     ranks.close()
     return out
 
@@ -722,6 +730,7 @@ def main():
     ap.add_argument("--no-adjoint", action="store_true")
     ap.add_argument("--no-p5", action="store_true")
     ap.add_argument("--no-mixed", action="store_true")
+    ap.add_argument("--detail", default=None, help="also write every sub-result to this JSON file")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

@@ -163,13 +163,16 @@ zj_status zj_get_state_async(zj_solver* s, double* U_host);
 /* ---- the hot path ---------------------------------------------------------- */
 /* nsteps SSP-RK3 steps of size dt (FRSolver::advance, fr_solver.cpp:305-333),
  * queued on the handle's stream; returns once the steps are enqueued and
- * checked for launch errors.  zj_synchronize waits for them. */
+ * checked for launch errors.  zj_synchronize waits for them.  dt reaches the
+ * device as a kernel argument, so zj_step may be captured into a caller's
+ * graph with any dt (each replay sets it). */
 zj_status zj_step(zj_solver* s, double dt, int nsteps);
 /* Step graphs (no reference counterpart): zj_step replays blocks of six steps
- * from CUDA graphs captured on the handle's stream at first use (one graph per
- * phase of the rotating stage and trace buffers, at most six per handle), so a
- * long zj_step costs one launch per six steps instead of six to twelve; the
- * handle's first step, remainders, the legacy default stream and a stream the
+ * from CUDA graphs (one graph per phase of the rotating stage and trace
+ * buffers, six per handle), so a long zj_step costs one launch per six steps
+ * instead of six to twelve.  The handle's first zj_step runs its steps with
+ * plain launches and then captures and uploads all six graphs, so later calls
+ * only launch them; remainders, the legacy default stream and a stream the
  * caller is capturing launch kernels directly, with identical results.
  * enable = 0 turns the graphs off for this handle. */
 zj_status zj_set_step_graphs(zj_solver* s, int enable);
@@ -203,18 +206,26 @@ void* zj_get_stream(const zj_solver* s);
  * that may not allocate device memory when they need it (a host application
  * whose device memory is reserved up front by its own allocator, a
  * time-critical loop that must not hit cudaMalloc's implicit synchronisation).
- * Its per-call scratch -- the trace buffer, E*4*(P+1)*4 doubles, plus one
- * double per CTA -- lives in one file-scope device array of
+ * Its per-call scratch lives in one file-scope device array of
  * ZJ_NOALLOC_SCRATCH_BYTES inside the library, which every GPU that loads the
  * library holds until the process exits; the call makes no cudaMalloc,
- * cudaFree or other allocating call.  A mesh whose scratch exceeds the limit
- * is rejected with ZJ_ERR_ARG (P3: up to 65 000 elements).
- * The first call on a device looks up the array's device address (once per
- * device, with that device current); make that first call before any stream
- * capture.  All calls share the one array: calls that overlap on the GPU
- * (other streams, other handles, other host threads) race on it.  Inputs and
- * outputs are the caller's device buffers, 16-byte aligned, on the handle's
- * stream. */
+ * cudaFree or other allocating call.  Scratch bytes of a handle, with
+ * n_t = (4 E + B) (P+1) 4 trace values (E elements, B boundary edges in
+ * physics mode, 0 in compat mode), w = 8 (FP64) or 4 (precision mixed) and
+ * G = the residual's CTA count (E/16 at P3, quads):
+ *     k n_t w + 8 G,   k = 3 for Navier-Stokes (traces and the two gradient
+ *                      trace components), 1 otherwise.
+ * At P3 that admits about 65 000 elements in FP64 Euler or compat, 21 000 in
+ * FP64 Navier-Stokes and 43 000 in the mixed form's Navier-Stokes; a larger
+ * mesh is rejected with ZJ_ERR_ARG and a message giving the bytes it needs.
+ * Call it with the device current on which the handle was created
+ * (ZJ_ERR_ARG otherwise).  The first call on a device looks up the array's
+ * device address (once per device, with that device current) and keeps it for
+ * the life of the process: make that first call before any stream capture, and
+ * do not use the library across a cudaDeviceReset of the device.  All calls
+ * share the one array: calls that overlap on the GPU (other streams, other
+ * handles, other host threads) race on it.  Inputs and outputs are the
+ * caller's device buffers, 16-byte aligned, on the handle's stream. */
 #define ZJ_NOALLOC_SCRATCH_BYTES (32u * 1024u * 1024u)
 zj_status zj_rhs_noalloc(zj_solver* s, const double* U_dev, double* R_dev);
 

@@ -1047,11 +1047,19 @@ void orc_get_vcjh(const orc_ctx* c, double* gL, double* gR) {
     for (int j = 0; j < c->n1; ++j) { gL[j] = c->gLp[j]; gR[j] = c->gRp[j]; }
 }
 
-/* Viscous flux of computeViscousFluxSPKernel (kernels.cu:742-786): velocity
- * and temperature gradients from the conservative gradients, mu = T^0.7/Re,
- * k = mu gamma/((gamma-1) Pr), Stokes hypothesis. */
-void orc_viscous_flux(const double* s, const double* dx, const double* dy, double g, double Re,
-                      double Pr, double* Fv, double* Gv) {
+/* Viscous flux at one state with conservative gradients dx, dy: velocity
+ * and temperature gradients from the conservative ones
+ * (ViscousFlux::velocityGradients / temperatureGradient, navierstokes.hpp:
+ * 115-158, the same formulas as computeViscousFluxSPKernel,
+ * kernels.cu:742-760), Stokes stresses (navierstokes.hpp:36-46), and one of
+ * the reference's two viscosity laws:
+ *   law 0: the kernel's mu = T^0.7/Re, k = mu gamma/((gamma-1) Pr)
+ *          (kernels.cu:762-764) -- the law of every residual here;
+ *   law 1: the header's Sutherland law mu = (T^1.5 (1+S)/(T+S))/Re,
+ *          S = 110.4, and k = (mu cp/Pr)/Re (ViscousFlux::fluxX,
+ *          navierstokes.hpp:17-33, 52-96), kept for its pointwise pin. */
+void orc_viscous_flux_law(int law, const double* s, const double* dx, const double* dy, double g,
+                          double Re, double Pr, double* Fv, double* Gv) {
     double rho = s[0], u = s[1] / rho, v = s[2] / rho;
     double dudx = (dx[1] - u * dx[0]) / rho, dudy = (dy[1] - u * dy[0]) / rho;
     double dvdx = (dx[2] - v * dx[0]) / rho, dvdy = (dy[2] - v * dy[0]) / rho;
@@ -1059,13 +1067,43 @@ void orc_viscous_flux(const double* s, const double* dx, const double* dy, doubl
     double dpdx = (g - 1.0) * (dx[3] - 0.5 * dx[0] * (u * u + v * v) - rho * (u * dudx + v * dvdx));
     double dpdy = (g - 1.0) * (dy[3] - 0.5 * dy[0] * (u * u + v * v) - rho * (u * dudy + v * dvdy));
     double dTdx = (dpdx - T * dx[0]) / rho, dTdy = (dpdy - T * dy[0]) / rho;
-    double mu = pow(T, 0.7) / Re;
-    double k = mu * g / ((g - 1.0) * Pr);
+    double mu, k;
+    if (law == 1) {
+        const double S = 110.4 / 1.0, Tn = T / 1.0;
+        mu = 1.0 * pow(Tn, 1.5) * (1.0 + S) / (Tn + S) / Re;
+        const double cp = g / (g - 1.0);
+        k = mu * cp / Pr / Re;
+    } else {
+        mu = pow(T, 0.7) / Re;
+        k = mu * g / ((g - 1.0) * Pr);
+    }
     double div = dudx + dvdy, lam = -2.0 / 3.0 * mu;
     double txx = 2.0 * mu * dudx + lam * div, tyy = 2.0 * mu * dvdy + lam * div;
     double txy = mu * (dudy + dvdx);
     Fv[0] = 0.0; Fv[1] = txx; Fv[2] = txy; Fv[3] = u * txx + v * txy + k * dTdx;
     Gv[0] = 0.0; Gv[1] = txy; Gv[2] = tyy; Gv[3] = u * txy + v * tyy + k * dTdy;
+}
+
+/* The kernel law (law 0), the viscous flux of every residual here. */
+void orc_viscous_flux(const double* s, const double* dx, const double* dy, double g, double Re,
+                      double Pr, double* Fv, double* Gv) {
+    orc_viscous_flux_law(0, s, dx, dy, g, Re, Pr, Fv, Gv);
+}
+
+/* Common normal viscous flux of a face point (BR2Scheme::commonFlux,
+ * navierstokes.hpp:166-201): average state and average gradients, the
+ * viscous flux there, dotted with the normal. */
+void orc_common_viscous_law(int law, const double* UL, const double* UR, const double* dxL,
+                            const double* dyL, const double* dxR, const double* dyR, double nx,
+                            double ny, double g, double Re, double Pr, double* Fvn) {
+    double Ua[4], dxa[4], dya[4], Fv[4], Gv[4];
+    for (int v = 0; v < 4; ++v) {
+        Ua[v] = 0.5 * (UL[v] + UR[v]);
+        dxa[v] = 0.5 * (dxL[v] + dxR[v]);
+        dya[v] = 0.5 * (dyL[v] + dyR[v]);
+    }
+    orc_viscous_flux_law(law, Ua, dxa, dya, g, Re, Pr, Fv, Gv);
+    for (int v = 0; v < 4; ++v) Fvn[v] = Fv[v] * nx + Gv[v] * ny;
 }
 
 /* Neumann data of the walls on the common normal viscous flux Fvn of a
@@ -1223,15 +1261,8 @@ void orc_rhs_phys(orc_ctx* c, const double* U, double* R) {
                  * Neumann data */
                 const double* QL = Qfp + (lo / 4) * 8;
                 const double* QR = (ro >= 0) ? Qfp + (ro / 4) * 8 : QL;
-                double Ua[4], dxa[4], dya[4], Fv[4], Gv[4];
-                for (int v = 0; v < 4; ++v) {
-                    Ua[v] = 0.5 * (UL[v] + UR[v]);
-                    dxa[v] = 0.5 * (QL[v] + QR[v]);
-                    dya[v] = 0.5 * (QL[4 + v] + QR[4 + v]);
-                }
-                orc_viscous_flux(Ua, dxa, dya, g, c->Re, c->Pr, Fv, Gv);
                 double Fvn[4];
-                for (int v = 0; v < 4; ++v) Fvn[v] = Fv[v] * nx + Gv[v] * ny;
+                orc_common_viscous_law(0, UL, UR, QL, QL + 4, QR, QR + 4, nx, ny, g, c->Re, c->Pr, Fvn);
                 if (re < 0) orc_wall_viscous_closure(c, c->fbct[f], c->ftag[f], nx, ny, Fvn);
                 for (int v = 0; v < 4; ++v) Fc[v] -= Fvn[v];
             }

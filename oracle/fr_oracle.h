@@ -74,9 +74,19 @@ void orc_set_bc_extra(orc_ctx* c, int n, const int* tag_ids, const double* p_tot
 void orc_get_vcjh(const orc_ctx* c, double* gL, double* gR);
 void orc_vcjh(int P, int flux_type, const double* x, double* gL, double* gR);
 void orc_rhs_phys(orc_ctx* c, const double* U, double* R);
-/* viscous flux at one state with gradients dx = dU/dx, dy = dU/dy */
+/* viscous flux at one state with gradients dx = dU/dx, dy = dU/dy (the
+ * kernel's viscosity law, kernels.cu:742-786) */
 void orc_viscous_flux(const double* U, const double* dx, const double* dy, double g, double Re,
                       double Pr, double* Fv, double* Gv);
+/* the same with law 0 (kernel law) or 1 (the header's Sutherland law,
+ * navierstokes.hpp:17-96) */
+void orc_viscous_flux_law(int law, const double* U, const double* dx, const double* dy, double g,
+                          double Re, double Pr, double* Fv, double* Gv);
+/* common normal viscous flux of a face point (BR2Scheme::commonFlux,
+ * navierstokes.hpp:166-201) under law 0 or 1 */
+void orc_common_viscous_law(int law, const double* UL, const double* UR, const double* dxL,
+                            const double* dyL, const double* dxR, const double* dyR, double nx,
+                            double ny, double g, double Re, double Pr, double* Fvn);
 void orc_step_phys(orc_ctx* c, double* U, double dt, int nsteps, double* R_last);
 /* pointwise pins: which = 0 Rusanov, 1 Roe, 2 HLLC */
 void orc_riemann_point(int which, const double* UL, const double* UR, double nx, double ny,

@@ -18,7 +18,9 @@ LIB = os.path.join(HERE, "libfr_oracle.so")
 REF_DIR = os.path.join(HERE, "_ref")
 REF_CPU = os.path.join(REF_DIR, "ref_cpu")
 REF_GPU = os.path.join(REF_DIR, "ref_gpu")
-REFERENCE_ROOT = "/root/reference"
+# The reference sources the harness is compiled from; REF as in
+# `make -C oracle/ref REF=...`.
+REFERENCE_ROOT = os.environ.get("REF", "/root/reference")
 
 
 def build(force: bool = False) -> str:
@@ -84,6 +86,9 @@ def lib():
         h.orc_riemann_point.argtypes = [C.c_int, dp, dp, C.c_double, C.c_double, C.c_double, dp]
         h.orc_ghost_point.argtypes = [C.c_void_p, C.c_int, C.c_int, dp, C.c_double, C.c_double, dp]
         h.orc_wall_viscous_closure.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_double, C.c_double, dp]
+        h.orc_viscous_flux_law.argtypes = [C.c_int, dp, dp, dp, C.c_double, C.c_double, C.c_double, dp, dp]
+        h.orc_common_viscous_law.argtypes = [C.c_int, dp, dp, dp, dp, dp, dp, C.c_double, C.c_double,
+                                             C.c_double, C.c_double, C.c_double, dp]
         _lib = h
     return _lib
 
@@ -294,4 +299,25 @@ def riemann_point(which, UL, UR, nx, ny, g):
     UR = np.ascontiguousarray(UR, dtype=np.float64)
     out = np.empty(4)
     lib().orc_riemann_point(which, _d(UL), _d(UR), nx, ny, g, _d(out))
+    return out
+
+
+def _c(a):
+    return np.ascontiguousarray(a, dtype=np.float64)
+
+
+def viscous_point(law, U, dx, dy, g, Re, Pr):
+    """(Fv, Gv) at one state with conservative gradients: law 0 the kernel's
+    mu = T^0.7/Re (the residual's), law 1 the header's Sutherland law."""
+    U, dx, dy = _c(U), _c(dx), _c(dy)
+    F, G = np.empty(4), np.empty(4)
+    lib().orc_viscous_flux_law(law, _d(U), _d(dx), _d(dy), g, Re, Pr, _d(F), _d(G))
+    return F, G
+
+
+def common_viscous_point(law, UL, UR, dxL, dyL, dxR, dyR, nx, ny, g, Re, Pr):
+    """Common normal viscous flux of one face point (BR2Scheme::commonFlux)."""
+    a = [_c(x) for x in (UL, UR, dxL, dyL, dxR, dyR)]
+    out = np.empty(4)
+    lib().orc_common_viscous_law(law, *[_d(x) for x in a], nx, ny, g, Re, Pr, _d(out))
     return out

@@ -8,10 +8,18 @@
 //             "mesh mesh.bin P out"  -> faces, normals (mesh.cpp:18-194) and
 //                                       J/Jinv exactly as fr_solver.cpp:85-129
 //             "gmsh file.msh out"    -> GmshReader::read (gmsh_reader.cpp:161)
+//             "visc in out gamma Re Pr" -> ViscousFlux::fluxX/fluxY and
+//                                       BR2Scheme::commonFlux (navierstokes.hpp)
 //   ref_gpu : + kernels.cu + fr_solver.cpp, needs a GPU.
 //             "rhs mesh.bin params state out"           -> computeResidual_GPU
 //             "step mesh.bin params state dt n out"     -> n x advance(dt)
 //             "time mesh.bin params state dt nw n out"  -> wall ms of n advance(dt)
+//             "traj mesh.bin params state n out"        -> dt = computeTimeStep(),
+//                                                          then the state and the
+//                                                          residual norm after each
+//                                                          of n advance(dt)
+//             "viscsp in out gamma Re Pr" -> gpu::computeViscousFluxSP
+//                                            (kernels.cu:719-807) on the records
 // Files are raw little-endian arrays; layouts are written by
 // oracle/oracle.py (write_mesh_bin) and read back by it.
 #include <chrono>
@@ -36,6 +44,7 @@
 
 #ifdef ZJ_REF_GPU
 #include <cuda_runtime.h>
+#include "gpu/kernels.hpp"
 #define private public
 #define protected public
 #include "solver/fr_solver.hpp"
@@ -270,6 +279,45 @@ int cmd_phys(char** a) {
     return 0;
 }
 
+// Viscous pin records: in = int64 N, then N x (U[4], dUdx[4], dUdy[4],
+// UR[4], dUdxR[4], dUdyR[4], nx, ny) f64.
+int read_visc(const char* path, std::vector<double>& in) {
+    Reader r(path);
+    const int64_t n = r.get<int64_t>();
+    r.arr(in, static_cast<size_t>(n) * 26);
+    return static_cast<int>(n);
+}
+
+// "visc in out gamma Re Pr": per record the header's ViscousFlux::fluxX and
+// fluxY at (U, dUdx, dUdy) with the header's own velocity and temperature
+// gradients (navierstokes.hpp:52-96, 115-158), then
+// BR2Scheme::commonFlux(UL=U, UR, ...) (navierstokes.hpp:166-201); 12 values.
+int cmd_visc(char** a) {
+    std::vector<double> in;
+    const int n = read_visc(a[0], in);
+    const double g = std::atof(a[2]), Re = std::atof(a[3]), Pr = std::atof(a[4]);
+    ViscousFlux vf(g, Re, Pr);
+    Writer w(a[1]);
+    for (int k = 0; k < n; ++k) {
+        const double* q = &in[static_cast<size_t>(k) * 26];
+        State U, dx, dy, UR, dxR, dyR;
+        for (int v = 0; v < 4; ++v) {
+            U[v] = q[v]; dx[v] = q[4 + v]; dy[v] = q[8 + v];
+            UR[v] = q[12 + v]; dxR[v] = q[16 + v]; dyR[v] = q[20 + v];
+        }
+        Real dudx, dudy, dvdx, dvdy, dTdx, dTdy;
+        ViscousFlux::velocityGradients(U, dx, dy, dudx, dudy, dvdx, dvdy);
+        vf.temperatureGradient(U, dx, dy, dTdx, dTdy);
+        const State F = vf.fluxX(U, dudx, dudy, dvdx, dvdy, dTdx, dTdy);
+        const State G = vf.fluxY(U, dudx, dudy, dvdx, dvdy, dTdx, dTdy);
+        const State C = BR2Scheme::commonFlux(U, UR, dx, dy, dxR, dyR, q[24], q[25], g, Re, Pr);
+        for (int v = 0; v < 4; ++v) w.put(F[v]);
+        for (int v = 0; v < 4; ++v) w.put(G[v]);
+        for (int v = 0; v < 4; ++v) w.put(C[v]);
+    }
+    return 0;
+}
+
 #ifdef ZJ_REF_GPU
 // params: "P gamma rho_inf p_inf Mach AoA"
 SimParams make_params(char** a) {
@@ -306,6 +354,19 @@ int cmd_gpu(int argc, char** argv) {
         cudaDeviceSynchronize();
         s.gpu_data_->dUdt.copyToHost(out.data(), n);
         Writer(argv[10]).arr(out);
+    } else if (cmd == "traj") {
+        // the reference's CFL step from the state just set (computeTimeStep
+        // reads the host copy), then n steps, each one recorded
+        const int ns = std::atoi(argv[10]);
+        const double dt = s.computeTimeStep();
+        Writer w(argv[11]);
+        w.put(dt);
+        for (int k = 0; k < ns; ++k) {
+            s.advance(dt);
+            s.gpu_data_->U.copyToHost(out.data(), n);
+            w.arr(out);
+            w.put(s.computeResidual());
+        }
     } else if (cmd == "time") {
         // wall clock of nsteps advance() calls after nwarm, device idle at both
         // ends: the reference's step includes host work and copies
@@ -336,6 +397,40 @@ int cmd_gpu(int argc, char** argv) {
     }
     return 0;
 }
+
+// "viscsp in out gamma Re Pr": the reference's computeViscousFluxSP kernel
+// (kernels.cu:719-807) over the records' (U, dUdx, dUdy) as one element of N
+// solution points; out = Fv_x[N][4], then Fv_y[N][4].
+int cmd_viscsp(char** a) {
+    std::vector<double> in;
+    const int n = read_visc(a[0], in);
+    const double g = std::atof(a[2]), Re = std::atof(a[3]), Pr = std::atof(a[4]);
+    std::vector<double> U(4 * n), dx(4 * n), dy(4 * n);
+    for (int k = 0; k < n; ++k)
+        for (int v = 0; v < 4; ++v) {
+            U[4 * k + v] = in[26 * k + v];
+            dx[4 * k + v] = in[26 * k + 4 + v];
+            dy[4 * k + v] = in[26 * k + 8 + v];
+        }
+    const size_t bytes = sizeof(double) * 4 * n;
+    double *dU = nullptr, *ddx = nullptr, *ddy = nullptr, *fx = nullptr, *fy = nullptr;
+    if (cudaMalloc(&dU, bytes) || cudaMalloc(&ddx, bytes) || cudaMalloc(&ddy, bytes) ||
+        cudaMalloc(&fx, bytes) || cudaMalloc(&fy, bytes))
+        return 4;
+    cudaMemcpy(dU, U.data(), bytes, cudaMemcpyHostToDevice);
+    cudaMemcpy(ddx, dx.data(), bytes, cudaMemcpyHostToDevice);
+    cudaMemcpy(ddy, dy.data(), bytes, cudaMemcpyHostToDevice);
+    gpu::computeViscousFluxSP(dU, ddx, ddy, fx, fy, g, Re, Pr, 1, n, 0);
+    if (cudaDeviceSynchronize() != cudaSuccess) return 5;
+    std::vector<double> ox(4 * n), oy(4 * n);
+    cudaMemcpy(ox.data(), fx, bytes, cudaMemcpyDeviceToHost);
+    cudaMemcpy(oy.data(), fy, bytes, cudaMemcpyDeviceToHost);
+    Writer w(a[1]);
+    w.arr(ox);
+    w.arr(oy);
+    cudaFree(dU); cudaFree(ddx); cudaFree(ddy); cudaFree(fx); cudaFree(fy);
+    return 0;
+}
 #endif
 
 }  // namespace
@@ -348,9 +443,12 @@ int main(int argc, char** argv) {
     if (cmd == "mesh" && argc == 5) return cmd_mesh(argv[2], std::atoi(argv[3]), argv[4]);
     if (cmd == "gmsh" && argc == 4) return cmd_gmsh(argv[2], argv[3]);
     if (cmd == "phys" && argc == 15) return cmd_phys(argv + 2);
+    if (cmd == "visc" && argc == 7) return cmd_visc(argv + 2);
 #ifdef ZJ_REF_GPU
-    if ((cmd == "rhs" && argc == 11) || (cmd == "step" && argc == 13) || (cmd == "time" && argc == 14))
+    if ((cmd == "rhs" && argc == 11) || (cmd == "step" && argc == 13) || (cmd == "time" && argc == 14) ||
+        (cmd == "traj" && argc == 12))
         return cmd_gpu(argc, argv);
+    if (cmd == "viscsp" && argc == 7) return cmd_viscsp(argv + 2);
 #endif
     std::fprintf(stderr, "bad command\n");
     return 1;

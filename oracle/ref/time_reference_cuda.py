@@ -3,7 +3,7 @@ and fr_solver.cpp compiled for sm_100a by oracle/ref/Makefile) against this
 library's compat path, which computes the same residual semantics (Rusanov,
 inviscid, the reference's correction and clamps), on the benchmark mesh:
 
-    python tests/time_reference_cuda.py [n] [steps]
+    python oracle/ref/time_reference_cuda.py [n] [steps]
 
 256x256 jittered (seed 1) Q1 quads on [0,pi]^2, P3, slip walls, the
 Taylor-Green state at M = 0.3, dt = 1e-6 (small enough that the reference
@@ -23,7 +23,7 @@ import tempfile
 import time
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-sys.path.insert(0, os.path.dirname(HERE))
+sys.path.insert(0, os.path.dirname(os.path.dirname(HERE)))
 
 from oracle import oracle as O  # noqa: E402
 from zhijian_b200 import meshgen as M  # noqa: E402

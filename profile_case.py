@@ -1,7 +1,7 @@
 """A few SSP-RK3 steps of the benchmark's cases, for external profilers (ncu)
 that capture a handful of launches:
 
-    python -m zhijian_b200.profile_case {ns|ns32|euler|euler32|compat|shear|shear32} [steps] [n] [P]
+    python profile_case.py {ns|ns32|euler|euler32|compat|shear|shear32} [steps] [n] [P]
 
 ns / ns32: Navier-Stokes (Re 5000, Pr 0.72, Roe, HU), FP64 / precision form;
 euler / euler32: the inviscid physics-mode residual; compat: the reference
@@ -13,10 +13,13 @@ CFL 0.1, FP64 / precision form."""
 from __future__ import annotations
 
 import math
+import os
 import sys
 
-from . import meshgen as M
-from .solver import FRSolver, make_params
+sys.path.insert(0, os.path.dirname(os.path.abspath(__file__)))
+
+from zhijian_b200 import meshgen as M  # noqa: E402
+from zhijian_b200.solver import FRSolver, make_params  # noqa: E402
 
 GAMMA, MACH = 1.4, 0.3
 MODES = {

@@ -5,9 +5,13 @@
 
 "cpu" runs oracle/_ref/ref_cpu (the reference's basis.cpp, mesh.cpp and
 gmsh_reader.cpp compiled from the reference sources by oracle/ref/Makefile) and
-stores its operators, faces, normals and metric terms.  "gpu" runs
-oracle/_ref/ref_gpu (the reference's kernels.cu and fr_solver.cpp) on the cases
-of GPU_CASES and stores the reference's own residuals and stepped states.
+stores its operators, faces, normals, metric terms, pointwise Riemann fluxes,
+ghost states and (ref_viscous.npz) the header's viscous fluxes.  "gpu" runs
+oracle/_ref/ref_gpu (the reference's kernels.cu and fr_solver.cpp) and stores
+the reference's own residuals and stepped states of case_defs()
+(ref_gpu_residuals.npz), the 200-step trajectories of the isentropic-vortex
+configuration (ref_trajectory.npz) and the reference kernel's viscous fluxes
+(ref_viscous_kernel.npz); --only picks some of those three.
 Inputs are seeded (SplitMix64), so every case is regenerated from its recipe.
 """
 from __future__ import annotations
@@ -151,11 +155,128 @@ def gen_cpu(out):
         ("g", "mach", "aoa", "rho_inf", "p_inf", "p_total", "T_total", "dx", "dy", "p_static", "T_wall")])
     res = np.fromfile(fo, dtype=np.float64).reshape(smp.shape[0], 10, 4)
     np.savez_compressed(os.path.join(out, "ref_physics.npz"), samples=smp, out=res)
+    gen_visc_header(out, tmp)
     print("cpu goldens written to", out)
 
 
-def gen_gpu(out):
+# Pointwise viscous pins: a state, its conservative gradients and a right
+# state with its gradients plus a normal (26 values per record), over a
+# non-dimensional (T ~ 8) and a dimensional (T ~ 8e4) regime.
+VISC_PARAMS = dict(g=1.4, Re=5000.0, Pr=0.72)
+
+
+def visc_samples(n=256, seed=31):
+    r = M.uniform01(seed, n * 26).reshape(n, 26)
+    g = VISC_PARAMS["g"]
+    out = np.empty((n, 26))
+    for k in range(n):
+        dim = k % 2 == 1
+        rho0, p0 = (1.2, 1.0e5) if dim else (1.0, 1.0 / (g * 0.09))
+        rows = []
+        for side in range(2):
+            q = r[k, 13 * side:13 * side + 13]
+            rho = rho0 * (0.3 + 1.4 * q[0])
+            p = p0 * (0.3 + 1.4 * q[1])
+            c = np.sqrt(g * p / rho)
+            u, v = c * (2.0 * q[2] - 1.0), c * (2.0 * q[3] - 1.0)
+            U = M.prim_to_cons(rho, u, v, p, g)
+            grad = np.abs(U) * (2.0 * q[4:12] - 1.0).reshape(2, 4) * (10.0 ** (3.0 * q[12] - 1.0))
+            rows.append(np.concatenate([U, grad[0], grad[1]]))
+        th = 2.0 * np.pi * r[k, 25]
+        out[k] = np.concatenate([rows[0], rows[1], [np.cos(th), np.sin(th)]])
+    return out
+
+
+def _write_visc_in(path, smp):
+    with open(path, "wb") as f:
+        f.write(np.int64(smp.shape[0]).tobytes())
+        f.write(smp.tobytes())
+
+
+def gen_visc_header(out, tmp):
+    smp = visc_samples()
+    fin, fo = os.path.join(tmp, "visc_in.bin"), os.path.join(tmp, "visc_out.bin")
+    _write_visc_in(fin, smp)
+    V = VISC_PARAMS
+    run([O.REF_CPU, "visc", fin, fo, repr(V["g"]), repr(V["Re"]), repr(V["Pr"])])
+    res = np.fromfile(fo, dtype=np.float64).reshape(smp.shape[0], 3, 4)
+    np.savez_compressed(os.path.join(out, "ref_viscous.npz"), samples=smp, out=res)
+
+
+def gen_visc_kernel(out, tmp):
+    smp = visc_samples()
+    fin, fo = os.path.join(tmp, "viscsp_in.bin"), os.path.join(tmp, "viscsp_out.bin")
+    _write_visc_in(fin, smp)
+    V = VISC_PARAMS
+    run([O.REF_GPU, "viscsp", fin, fo, repr(V["g"]), repr(V["Re"]), repr(V["Pr"])])
+    n = smp.shape[0]
+    a = np.fromfile(fo, dtype=np.float64)
+    np.savez_compressed(os.path.join(out, "ref_viscous_kernel.npz"), samples=smp,
+                        Fv=a[:4 * n].reshape(n, 4), Gv=a[4 * n:8 * n].reshape(n, 4))
+    print("viscous kernel pins", n, flush=True)
+
+
+# The isentropic-vortex configuration (20x20 on [-10,10]^2, P3, HU, Rusanov,
+# far field) at the reference's own CFL-0.5 step for 200 steps, as the raw
+# non-dimensional case (the reference's clamps fire) and its dimensional twin
+# (clamps inactive at the start).  Per step: the state's per-variable sum,
+# sum of squares, max and min, TRAJ_SAMPLES seeded solution points, and the
+# residual norm; full states at TRAJ_FULL steps (restart points of the
+# per-step comparison once the scheme's instability has amplified rounding).
+TRAJ_CASES = ("vortex_raw_p3", "vortex_dim_p3")
+TRAJ_STEPS = 200
+TRAJ_SAMPLES = 64
+TRAJ_FULL = (50, 100, 150)
+
+
+def traj_sample_index(n_points, n=TRAJ_SAMPLES, seed=41):
+    return np.sort((M.splitmix64(seed, n) % np.uint64(n_points)).astype(np.int64))
+
+
+def traj_stats(U):
+    """[4 sums, 4 sums of squares, 4 maxima, 4 minima] of a [E][n_sp][4] state."""
+    X = U.reshape(-1, 4)
+    return np.concatenate([X.sum(axis=0), (X * X).sum(axis=0), X.max(axis=0), X.min(axis=0)])
+
+
+def gen_traj(out, tmp):
+    res = {}
+    defs = case_defs()
+    for name in TRAJ_CASES:
+        c = defs[name]
+        mesh, P = c["mesh"], c["P"]
+        rho, p, mach, aoa = c["prm"]
+        orc = O.Oracle(mesh, P, GAMMA, rho, p, mach, aoa, tags=c["tags"])
+        U = make_state(c, orc.sp_coords())
+        mb, ub, tb = (os.path.join(tmp, x) for x in ("m.bin", "u.bin", "t.bin"))
+        O.write_mesh_bin(mb, mesh, c["tags"])
+        U.tofile(ub)
+        prm = [str(P), repr(GAMMA), repr(rho), repr(p), repr(mach), repr(aoa)]
+        run([O.REF_GPU, "traj", mb, *prm, ub, str(TRAJ_STEPS), tb])
+        a = np.fromfile(tb, dtype=np.float64)
+        dt, a = a[0], a[1:].reshape(TRAJ_STEPS, U.size + 1)
+        idx = traj_sample_index(U.shape[0] * U.shape[1])
+        states = a[:, :U.size].reshape((TRAJ_STEPS,) + U.shape)
+        res[f"{name}_U0"] = U
+        res[f"{name}_dt"] = np.array([dt])
+        res[f"{name}_norm"] = a[:, U.size]
+        res[f"{name}_stats"] = np.stack([traj_stats(X) for X in states])
+        res[f"{name}_samples"] = states.reshape(TRAJ_STEPS, -1, 4)[:, idx, :]
+        res[f"{name}_finite"] = np.array([bool(np.isfinite(X).all()) for X in states])
+        for k in TRAJ_FULL:
+            res[f"{name}_U{k}"] = states[k - 1]
+        print(name, "dt", dt, "finite steps", int(res[f"{name}_finite"].sum()), flush=True)
+    np.savez_compressed(os.path.join(out, "ref_trajectory.npz"), **res)
+
+
+def gen_gpu(out, only=("residuals", "traj", "visc")):
     tmp = tempfile.mkdtemp()
+    if "traj" in only:
+        gen_traj(out, tmp)
+    if "visc" in only:
+        gen_visc_kernel(out, tmp)
+    if "residuals" not in only:
+        return
     res = {}
     for name, c in case_defs().items():
         mesh, P = c["mesh"], c["P"]
@@ -187,9 +308,14 @@ def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("what", choices=["cpu", "gpu"])
     ap.add_argument("--out", default=HERE)
+    ap.add_argument("--only", default="residuals,traj,visc",
+                    help="gpu: comma-separated subset of residuals, traj, visc")
     a = ap.parse_args()
     os.makedirs(a.out, exist_ok=True)
-    (gen_cpu if a.what == "cpu" else gen_gpu)(a.out)
+    if a.what == "cpu":
+        gen_cpu(a.out)
+    else:
+        gen_gpu(a.out, tuple(a.only.split(",")))
 
 
 if __name__ == "__main__":

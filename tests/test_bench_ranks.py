@@ -31,7 +31,7 @@ def rank_main(rank, world, port, out):
     rate = bench.whole_job_rate(1000.0, r.world, slowest)
 
     class Args:
-        steps, warmup, gpus = 1, 0, world
+        steps, warmup, gpus, run_seconds = 1, 0, world, 0.2
     ref = bench.run_reference(Args)
     r.barrier()
     r.close()

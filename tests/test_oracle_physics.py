@@ -50,6 +50,45 @@ def test_ghost_states_bitwise_vs_reference(oracle_mod, phys, k, bct, tag):
     assert np.array_equal(got, ref[:, 3 + k])
 
 
+@pytest.fixture(scope="module")
+def visc():
+    return np.load(os.path.join(GOLD, "ref_viscous.npz"))
+
+
+def test_viscous_flux_bitwise_vs_reference_header(oracle_mod, visc):
+    """The oracle's viscous arithmetic (velocity and temperature gradients,
+    Stokes stresses, heat flux, the average-state common flux) under the
+    header's Sutherland law against ViscousFlux::fluxX / fluxY and
+    BR2Scheme::commonFlux (navierstokes.hpp:52-96, 166-201) compiled from the
+    reference: bit for bit on 256 states (both temperature regimes)."""
+    smp, ref = visc["samples"], visc["out"]
+    V = G.VISC_PARAMS
+    for q, r in zip(smp, ref):
+        F, Gv = oracle_mod.viscous_point(1, q[0:4], q[4:8], q[8:12], V["g"], V["Re"], V["Pr"])
+        C = oracle_mod.common_viscous_point(1, q[0:4], q[12:16], q[4:8], q[8:12], q[16:20], q[20:24],
+                                            q[24], q[25], V["g"], V["Re"], V["Pr"])
+        assert np.array_equal(F, r[0]) and np.array_equal(Gv, r[1]) and np.array_equal(C, r[2])
+
+
+def test_viscous_flux_vs_reference_kernel(oracle_mod):
+    """The oracle's viscous flux under the kernel's law (mu = T^0.7/Re, the
+    law of every residual here) against the reference's own
+    computeViscousFluxSPKernel (kernels.cu:719-807) run on a B200
+    (tests/golden/make_golden.py gpu): within 1e-13 of each record's flux
+    scale -- the reference kernel is compiled with FMA contraction, the
+    oracle without."""
+    d = np.load(os.path.join(GOLD, "ref_viscous_kernel.npz"))
+    smp = d["samples"]
+    assert np.array_equal(smp, G.visc_samples())
+    V = G.VISC_PARAMS
+    worst = 0.0
+    for q, fr, gr in zip(smp, d["Fv"], d["Gv"]):
+        F, Gv = oracle_mod.viscous_point(0, q[0:4], q[4:8], q[8:12], V["g"], V["Re"], V["Pr"])
+        scale = max(np.abs(fr).max(), np.abs(gr).max())
+        worst = max(worst, np.abs(F - fr).max() / scale, np.abs(Gv - gr).max() / scale)
+    assert worst <= 1e-13
+
+
 def _legendre(n, x):
     return np.polynomial.legendre.legval(x, [0] * n + [1])
 

@@ -57,6 +57,45 @@ def test_noalloc_matches_rhs_on_two_calls_in_a_row(zjlib):
     s.close()
 
 
+def _physics(mesh, precision):
+    """Navier-Stokes in physics mode (Roe, HU, slip walls, Re 5000) at P3."""
+    prm = make_params(poly_order=3, rho_inf=1.0, p_inf=1.0 / (1.4 * 0.09), Mach=0.3, riemann="Roe",
+                      flux_type="HU", compat=False, viscous=True, Re=5000.0, Pr=0.72,
+                      bcs=[(1, "slipwall")], precision=precision)
+    return FRSolver(mesh, prm)
+
+
+def _tgv_states(s):
+    U = M.taylor_green(s.solution_point_coords())
+    r = M.uniform01(123, U.size).reshape(U.shape)
+    return [U, U * (1.0 + 1.0e-3 * (2.0 * r - 1.0))]
+
+
+# The Navier-Stokes branches keep the gradient traces in the same scratch
+# (three trace blocks), the precision form FP32 traces with the FP64 partial
+# sums behind them, and a mesh of quads and triangles the triangles' partial
+# sums after the quads'.  Bars: the FP64 parity bar, and the precision form's
+# 1e-5 of the flux scale.
+NS_CASES = [("quads", "fp64", TOL), ("quads", "mixed", 1e-5),
+            ("quads+triangles", "fp64", TOL), ("quads+triangles", "mixed", 1e-5)]
+
+
+@pytest.mark.parametrize("kind,precision,tol", NS_CASES)
+def test_noalloc_navier_stokes_matches_rhs_on_two_calls_in_a_row(zjlib, kind, precision, tol):
+    mesh = M.tgv_mesh(32, seed=1)
+    if kind != "quads":
+        mesh = M.split_quads(mesh, 0.3, 3)
+    s = _physics(mesh, precision)
+    used = s.slot_mask()   # a triangle fills (P+1)(P+2)/2 of its (P+1)^2 slots
+    for U in _tgv_states(s):
+        ref = _run(zjlib, zjlib.zj_rhs, s, U)[used]
+        got = _run(zjlib, zjlib.zj_rhs_noalloc, s, U)[used]
+        assert np.isfinite(got).all()
+        # flux scale x the metric 2/h of elements of side h = pi/32
+        assert T.rel_err(got, ref, T.euler_flux_scale(U) * 64.0 / np.pi) <= tol
+    s.close()
+
+
 def test_noalloc_rejects_a_mesh_beyond_its_scratch(zjlib):
     # P5 traces take 768 bytes per element: 210 x 210 elements need ~34 MB.
     mesh = M.tgv_mesh(210, seed=2)

@@ -114,6 +114,7 @@ struct zj_solver {
     bool stepped = false;       // a plain step ran (the kernels' one-time attributes are set)
     bool has_norm = false;
     cudaStream_t own = nullptr, stream = nullptr;
+    int device = 0;             // the device current at zj_solver_create
     double time = 0.0;
     int iter = 0;
     double last_dt = -1.0;
@@ -216,6 +217,14 @@ template <> StageArgsT<float> base_args<float>(const zj_solver* s) {
     return a;
 }
 
+// 1/Re and gamma/((gamma-1) Pr), the viscosity law's constants, once per
+// launch instead of two divisions per viscous flux.
+template <typename T>
+void set_viscous_constants(StageArgsT<T>& a) {
+    a.iRe = 1.0 / a.Re;
+    a.kfac = a.gamma / ((a.gamma - 1.0) * a.Pr);
+}
+
 template <typename T>
 StageArgsT<T> stage_args(const zj_solver* s) {
     StageArgsT<T> a = base_args<T>(s);
@@ -225,6 +234,7 @@ StageArgsT<T> stage_args(const zj_solver* s) {
     a.gamma = s->prm.gamma;
     a.Re = s->prm.Re;
     a.Pr = s->prm.Pr;
+    set_viscous_constants(a);
     return a;
 }
 
@@ -305,6 +315,11 @@ zj_status enqueue_step(zj_solver* s) {
 
 constexpr int kGraphSteps = 6;
 
+// dt[0] = v: the step size reaches the device as a kernel argument, so a
+// zj_step inside a graph the caller captures records the value itself (a copy
+// from a host variable would record a pointer to it).
+__global__ void k_set_dt(double* dt, double v) { *dt = v; }
+
 // The 6-step block starting at the handle's (cur, tpar), captured on first
 // use; nullptr where graphs cannot be used: the legacy default stream (not
 // capturable), a stream the caller is capturing (the plain launches join the
@@ -343,12 +358,34 @@ cudaGraphExec_t step_graph(zj_solver* s) {
     return exec;
 }
 
+// After the handle's first plain step: capture the 6-step graphs of all six
+// buffer phases and upload them, so no later zj_step captures or uploads (a
+// caller timing a later call sees only graph launches).
+template <typename T>
+void capture_all_phases(zj_solver* s) {
+    if (!s->graphs_on || s->graphs_failed || !s->stepped || s->stream == nullptr) return;
+    const int cur0 = s->cur, tpar0 = s->tpar;
+    for (int c = 0; c < 3 && !s->graphs_failed; ++c)
+        for (int p = 0; p < 2 && !s->graphs_failed; ++p) {
+            s->cur = c;
+            s->tpar = p;
+            cudaGraphExec_t g = step_graph<T>(s);
+            if (g && cudaGraphUpload(g, s->stream) != cudaSuccess) {
+                (void)cudaGetLastError();
+                s->graphs_failed = true;
+            }
+        }
+    s->cur = cur0;
+    s->tpar = tpar0;
+}
+
 template <typename T>
 zj_status step_impl(zj_solver* s, int nsteps, double dt) {
     if (!s->traces_valid) {
         ZJ_CK(s, launch_trace_any(s, s->dU[s->cur], tbuf<T>(s, s->tpar)), "trace launch");
         s->traces_valid = true;
     }
+    const bool first = !s->stepped;
     // blocks of six steps replay a captured graph (one launch instead of six
     // to twelve); the rest, and the handle's first step, launch directly
     for (int k = 0; k < nsteps;) {
@@ -366,6 +403,7 @@ zj_status step_impl(zj_solver* s, int nsteps, double dt) {
             ++k;
         }
     }
+    if (first) capture_all_phases<T>(s);
     return ZJ_OK;
 }
 
@@ -464,7 +502,7 @@ zj_status zj_solver_create(const zj_mesh_desc* mesh, const zj_params* params, zj
         s->grid = s->grid_q + s->grid_t;
     }
     s->scratch_n = 148 * 8;
-    cudaError_t e = cudaSuccess;
+    cudaError_t e = cudaGetDevice(&s->device);
 #define ZJ_ALLOC(ptr, n)                                                     \
     if (e == cudaSuccess) e = dalloc(&(ptr), (n));
     for (int i = 0; i < 3; ++i) { ZJ_ALLOC(s->dU[i], s->state_n); }
@@ -652,8 +690,17 @@ zj_status zj_step(zj_solver* s, double dt, int nsteps) {
     if (!s) return ZJ_ERR_ARG;
     if (nsteps < 0 || !std::isfinite(dt)) return fail(s, ZJ_ERR_ARG, "bad dt or nsteps");
     if (nsteps == 0) return ZJ_OK;
-    if (dt != s->last_dt) {
-        ZJ_CK(s, cudaMemcpyAsync(s->dScal, &dt, sizeof(double), cudaMemcpyHostToDevice, s->stream), "dt upload");
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    ZJ_CK(s, cudaStreamIsCapturing(s->stream, &cs), "capture query");
+    if (cs != cudaStreamCaptureStatusNone) {
+        // a caller's capture: the graph sets dt on every replay, and the next
+        // direct call sets it again (replays may have changed it)
+        k_set_dt<<<1, 1, 0, s->stream>>>(s->dScal, dt);
+        ZJ_CK(s, cudaGetLastError(), "dt launch");
+        s->last_dt = std::nan("");
+    } else if (dt != s->last_dt) {
+        k_set_dt<<<1, 1, 0, s->stream>>>(s->dScal, dt);
+        ZJ_CK(s, cudaGetLastError(), "dt launch");
         s->last_dt = dt;
     }
     zj_status st = s->mixed ? step_impl<float>(s, nsteps, dt) : step_impl<double>(s, nsteps, dt);
@@ -737,7 +784,10 @@ namespace {
 
 // Device address of g_noalloc_scratch per device.  In host code the array's
 // name only stands in for the symbol; a kernel must be given the address
-// cudaGetSymbolAddress returns with that device current.
+// cudaGetSymbolAddress returns with that device current.  The address is
+// looked up once per device and kept for the life of the process, so the
+// library must not be used across a cudaDeviceReset of that device (which
+// reloads the module).
 constexpr int kMaxDevices = 64;
 double* g_noalloc_ptr[kMaxDevices] = {};
 std::mutex g_noalloc_mutex;
@@ -766,19 +816,27 @@ zj_status zj_rhs_noalloc(zj_solver* s, const double* U_dev, double* R_dev) {
     if (!s || !U_dev || !R_dev) return ZJ_ERR_ARG;
     if ((reinterpret_cast<uintptr_t>(U_dev) | reinterpret_cast<uintptr_t>(R_dev)) & 15u)
         return fail(s, ZJ_ERR_ARG, "U_dev and R_dev must be 16-byte aligned");
+    int dev = -1;
+    ZJ_CK(s, cudaGetDevice(&dev), "current device");
+    if (dev != s->device)
+        return fail(s, ZJ_ERR_ARG,
+                    "zj_rhs_noalloc: device " + std::to_string(dev) + " is current, the handle was created on device " +
+                        std::to_string(s->device) + " (the static scratch is per device)");
     const size_t tsz = s->mixed ? sizeof(float) : sizeof(double);
     const size_t trace_bytes = (is_ns(s) ? 3 : 1) * s->trace_n * tsz;
     const size_t part_bytes = (size_t)s->grid * sizeof(double);
-    if (trace_bytes + part_bytes > ZJ_NOALLOC_SCRATCH_BYTES)
+    const size_t need = trace_bytes + part_bytes;
+    if (need > ZJ_NOALLOC_SCRATCH_BYTES)
         return fail(s, ZJ_ERR_ARG,
-                    "mesh too large for zj_rhs_noalloc: needs " + std::to_string(trace_bytes + part_bytes) +
+                    "mesh too large for zj_rhs_noalloc: needs " + std::to_string(need) +
                         " bytes of scratch, the static limit is " +
                         std::to_string((size_t)ZJ_NOALLOC_SCRATCH_BYTES) + " bytes");
     double* scratch = nullptr;
     ZJ_CK(s, noalloc_scratch(&scratch), "static scratch address");
     // Every scratch value is written before it is read (all traces by the
-    // trace launch, one partial per CTA), so nothing needs clearing.  The
-    // trace block is a multiple of 16 bytes, so the partials stay aligned.
+    // trace launch, the gradient traces by the gradient launch, one partial
+    // per CTA), so nothing needs clearing.  The trace block is a multiple of
+    // 16 bytes, so the partials stay aligned.
     char* base = reinterpret_cast<char*>(scratch);
     double* partials = reinterpret_cast<double*>(base + trace_bytes);
     if (s->mixed) {
@@ -850,6 +908,7 @@ zj_status jvp_core(zj_solver* s, const double* U, const double* V, double dRe, d
     a.Jinv = s->xJinv; a.J = s->xJ; a.enrm = s->xNrm; a.bc = s->xBC; a.ops = s->xOps;
     a.edges = s->dEdges; a.dt = s->dScal; a.n_elem = s->E; a.gamma = s->prm.gamma;
     a.Re = s->prm.Re; a.Pr = s->prm.Pr; a.dRe = dRe;
+    set_viscous_constants(a);
     a.U = U; a.U0 = U; a.dU = V; a.Tout = s->xT;
     ZJ_CK(s, launch_phys_traces(s->P, a, s->stream), "jvp trace launch");
     a.Tin = s->xT; a.TQ = s->xTQ; a.TQout = s->xTQ;

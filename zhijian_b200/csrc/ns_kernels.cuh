@@ -252,7 +252,7 @@ k_ns_stage(const StageArgsT<T> a) {
     bool valid;
     const long long e = block_element(a, EB, el, valid);
     const bool is_sp = valid && k < NSP, is_fp = valid && k < NFT;
-    const T g = T(a.gamma), Re = reynolds(a), Pr = T(a.Pr);
+    const T g = T(a.gamma);
     const int edge = k / N1, fp = k - edge * N1;
     const int i = k % N1, j = k / N1;
 
@@ -303,9 +303,11 @@ k_ns_stage(const StageArgsT<T> a) {
     if (is_sp) {
         T Qx[4], Qy[4], Fv[4], Gv[4];
         corrected_gradient<N1, RS, VS>(sU + el * FS, sD + el * DS, sOps, i, j, ji, Qx, Qy);
-        viscous_flux(u, Qx, Qy, g, Re, Pr, Fv, Gv);
+        // one reciprocal density for the viscous and the Euler flux
+        const T ir = rcp_any(u[0]);
+        viscous_flux_f(u, ir, Qx, Qy, g, inv_reynolds(a), T(a.kfac), Fv, Gv);
         T F[4], G[4];
-        euler_flux(u, g, F, G);
+        euler_flux_ir(u, ir, g, F, G);
         if constexpr (kRef) {
             T Fe[4], Ge[4];
             euler_flux(ue, g, Fe, Ge);
@@ -346,7 +348,7 @@ k_ns_stage(const StageArgsT<T> a) {
                 dxa[v] = T(0.5) * (Qo[v] + Qn[v]);
                 dya[v] = T(0.5) * (Qo[4 + v] + Qn[4 + v]);
             }
-            viscous_flux(Ua, dxa, dya, g, Re, Pr, Fv, Gv);
+            viscous_flux_f(Ua, rcp_any(Ua[0]), dxa, dya, g, inv_reynolds(a), T(a.kfac), Fv, Gv);
             T Fvn[4];
 #pragma unroll
             for (int v = 0; v < 4; ++v) Fvn[v] = Fv[v] * f.nx + Gv[v] * f.ny;

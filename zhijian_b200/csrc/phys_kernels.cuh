@@ -140,6 +140,14 @@ __device__ __forceinline__ T reynolds(const StageArgsT<T>& a) {
     else return T(a.Re);
 }
 
+// 1/Re (with its tangent -dRe/Re^2 for duals) and gamma/((gamma-1) Pr),
+// read from the launch arguments where they are used.
+template <typename T>
+__device__ __forceinline__ T inv_reynolds(const StageArgsT<T>& a) {
+    if constexpr (IsDual<T>::value) return Dual(a.iRe, -a.dRe * a.iRe * a.iRe);
+    else return T(a.iRe);
+}
+
 // SSP-RK3 stage update in FP64 from the stage state us, the base state u0
 // and the residual res of the arithmetic type.
 template <typename T>
@@ -172,6 +180,15 @@ struct UsesRef { static constexpr bool value = sizeof(T) == 4; };
 template <typename T>
 __device__ __forceinline__ void euler_flux(const T* u, T g, T* F, T* G) {
     const T ir = rcp_any(u[0]);
+    const T uu = u[1] * ir, vv = u[2] * ir, E = u[3] * ir;
+    const T p = (g - T(1)) * u[0] * (E - T(0.5) * (uu * uu + vv * vv));
+    F[0] = u[1]; F[1] = u[1] * uu + p; F[2] = u[1] * vv; F[3] = (u[3] + p) * uu;
+    G[0] = u[2]; G[1] = u[2] * uu; G[2] = u[2] * vv + p; G[3] = (u[3] + p) * vv;
+}
+
+// euler_flux with ir = 1/u[0] supplied (identical arithmetic).
+template <typename T>
+__device__ __forceinline__ void euler_flux_ir(const T* u, T ir, T g, T* F, T* G) {
     const T uu = u[1] * ir, vv = u[2] * ir, E = u[3] * ir;
     const T p = (g - T(1)) * u[0] * (E - T(0.5) * (uu * uu + vv * vv));
     F[0] = u[1]; F[1] = u[1] * uu + p; F[2] = u[1] * vv; F[3] = (u[3] + p) * uu;

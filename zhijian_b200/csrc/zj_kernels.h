@@ -41,6 +41,7 @@ struct StageArgsT {
     const T* TQ;            // gradient traces of U, [E][4 edges][n1][8] = (dU/dx, dU/dy)
     T* TQout;               // gradient traces written by the gradient launch
     double Re, Pr;
+    double iRe, kfac;       // 1/Re and gamma/((gamma-1) Pr) of the viscosity law
     // Element list of a mesh with several element kinds: the launch visits
     // elist[0..n_list) (NULL: every element 0..n_elem)
     const int32_t* elist;

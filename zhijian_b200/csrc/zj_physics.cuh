@@ -26,6 +26,13 @@ __device__ __forceinline__ T pressure(const T* U, T g) {
     return (g - T(1)) * U[0] * (E - T(0.5) * (u * u + v * v));
 }
 
+// The same with ir = 1/U[0] already computed (identical arithmetic).
+template <typename T>
+__device__ __forceinline__ T pressure_ir(const T* U, T ir, T g) {
+    const T u = U[1] * ir, v = U[2] * ir, E = U[3] * ir;
+    return (g - T(1)) * U[0] * (E - T(0.5) * (u * u + v * v));
+}
+
 // IdealGas::soundSpeed (euler.hpp:34-41)
 template <typename T>
 __device__ __forceinline__ T sound_speed(T p_raw, T rho_raw, T g) {
@@ -47,6 +54,29 @@ __device__ __forceinline__ void flux_normal(const T* U, T praw, T nx, T ny, T* F
     Fn[1] = rho * u * vn + p * nx;
     Fn[2] = rho * v * vn + p * ny;
     Fn[3] = H * vn;
+}
+
+// flux_normal with the floored density rho = max(U[0], 1e-10) and its
+// reciprocal ir already computed (identical arithmetic).
+template <typename T>
+__device__ __forceinline__ void flux_normal_ir(const T* U, T rho, T ir, T praw, T nx, T ny, T* Fn) {
+    const T u = U[1] * ir, v = U[2] * ir;
+    const T p = max_any(praw, T(1e-10));
+    const T H = U[3] + praw;
+    const T vn = u * nx + v * ny;
+    Fn[0] = rho * vn;
+    Fn[1] = rho * u * vn + p * nx;
+    Fn[2] = rho * v * vn + p * ny;
+    Fn[3] = H * vn;
+}
+
+// 1/U[0] given ir = 1/max(U[0], 1e-10): the same value unless the floor
+// applied (then computed).
+template <typename T>
+__device__ __forceinline__ T raw_rcp(const T* U, T ir) {
+    T r = ir;
+    if (!(U[0] >= T(1e-10))) r = rcp_any(U[0]);
+    return r;
 }
 
 // RiemannSolvers::rusanov (euler.hpp:184-200): s = |u| + c of each side.
@@ -71,7 +101,9 @@ __device__ __forceinline__ void riemann_roe(const T* UL, const T* UR, T nx, T ny
     const T rhoL = max_any(UL[0], T(1e-10)), rhoR = max_any(UR[0], T(1e-10));
     const T irL = rcp_any(rhoL), irR = rcp_any(rhoR);
     const T uL = UL[1] * irL, vL = UL[2] * irL, uR = UR[1] * irR, vR = UR[2] * irR;
-    const T pL = pressure(UL, g), pR = pressure(UR, g);
+    // pressure() and flux_normal() take 1/U[0] and 1/max(U[0], 1e-10): the
+    // reciprocals above, reused (the same values, each computed once)
+    const T pL = pressure_ir(UL, raw_rcp(UL, irL), g), pR = pressure_ir(UR, raw_rcp(UR, irR), g);
     const T HL = (UL[3] + pL) * irL, HR = (UR[3] + pR) * irR;
     const T sL = sqrt_any(rhoL), sR = sqrt_any(rhoR);
     const T iden = rcp_any(max_any(sL + sR, T(1e-10)));
@@ -95,8 +127,8 @@ __device__ __forceinline__ void riemann_roe(const T* UL, const T* UR, T nx, T ny
     const T a3 = rhoRoe * (dv * nx - du * ny);
     const T a4 = (dp + rhoRoe * c * dvn) * (T(0.5) * ics);
     T FL[4], FR[4];
-    flux_normal(UL, pL, nx, ny, FL);
-    flux_normal(UR, pR, nx, ny, FR);
+    flux_normal_ir(UL, rhoL, irL, pL, nx, ny, FL);
+    flux_normal_ir(UR, rhoR, irR, pR, nx, ny, FR);
     const T tx = -ny, ty = nx;
     const T w1 = l1 * a1, w2 = l2 * a2, w3 = l2 * a3, w4 = l4 * a4;
     const T dF0 = w1 + w2 + w4;
@@ -244,6 +276,29 @@ __device__ __forceinline__ void viscous_flux(const T* s, const T* dx, const T* d
     const T dTdx = (dpdx - Tm * dx[0]) * ir, dTdy = (dpdy - Tm * dy[0]) * ir;
     const T mu = div_any(visc_pow(Tm), Re);
     const T k = div_any(mu * g, (g - T(1)) * Pr);
+    const T div = dudx + dvdy, lam = T(-2.0 / 3.0) * mu;
+    const T txx = T(2) * mu * dudx + lam * div, tyy = T(2) * mu * dvdy + lam * div;
+    const T txy = mu * (dudy + dvdx);
+    Fv[0] = T(0); Fv[1] = txx; Fv[2] = txy; Fv[3] = u * txx + v * txy + k * dTdx;
+    Gv[0] = T(0); Gv[1] = txy; Gv[2] = tyy; Gv[3] = u * txy + v * tyy + k * dTdy;
+}
+
+// viscous_flux with ir = 1/s[0] supplied and the law's two divisions taken
+// as products with iRe = 1/Re and kfac = gamma/((gamma-1) Pr), computed once
+// per thread (each within 2 ulp of the divided form).
+template <typename T>
+__device__ __forceinline__ void viscous_flux_f(const T* s, T ir, const T* dx, const T* dy, T g, T iRe,
+                                               T kfac, T* Fv, T* Gv) {
+    const T u = s[1] * ir, v = s[2] * ir;
+    const T dudx = (dx[1] - u * dx[0]) * ir, dudy = (dy[1] - u * dy[0]) * ir;
+    const T dvdx = (dx[2] - v * dx[0]) * ir, dvdy = (dy[2] - v * dy[0]) * ir;
+    const T p = (g - T(1)) * s[0] * (s[3] * ir - T(0.5) * (u * u + v * v));
+    const T Tm = p * ir;
+    const T dpdx = (g - T(1)) * (dx[3] - T(0.5) * dx[0] * (u * u + v * v) - s[0] * (u * dudx + v * dvdx));
+    const T dpdy = (g - T(1)) * (dy[3] - T(0.5) * dy[0] * (u * u + v * v) - s[0] * (u * dudy + v * dvdy));
+    const T dTdx = (dpdx - Tm * dx[0]) * ir, dTdy = (dpdy - Tm * dy[0]) * ir;
+    const T mu = visc_pow(Tm) * iRe;
+    const T k = mu * kfac;
     const T div = dudx + dvdy, lam = T(-2.0 / 3.0) * mu;
     const T txx = T(2) * mu * dudx + lam * div, tyy = T(2) * mu * dvdy + lam * div;
     const T txy = mu * (dudy + dvdx);
