@@ -478,8 +478,11 @@ def run_ours(args):
         if p5:
             out["p5_value"] = p5["mixed"]["value"]
             out["p5_speedup_vs_fp64"] = p5["speedup_vs_fp64"]
+            out["p5_split_bf16_value"] = p5["split_bf16"]["value"]
+            out["p5_split_bf16_speedup_vs_fp64"] = p5["split_bf16"]["speedup_vs_fp64"]
             if "errors" in p5:
                 out["p5_l2_err_1000"] = p5["errors"]["l2"]
+                out["p5_split_bf16_l2_err_1000"] = p5["errors"]["split_bf16_l2"]
         if shear:
             out["mixed_mesh_speedups"] = [round(c["speedup_vs_fp64"], 3) for c in shear["cases"]]
         if world == 1 and not args.no_cpu_baseline:
@@ -494,7 +497,8 @@ def run_ours(args):
 def p5_precision_case(stream, args, n=512, steps_err=1000):
     """The precision form of the Taylor-Green case on 512x512 jittered quads
     (seed 2) at P5 (36 solution points, 9.4 M DOF per variable), Navier-Stokes
-    Re 5000, Roe, HU: DOF-RHS/s of the precision form and of the FP64 path
+    Re 5000, Roe, HU: DOF-RHS/s of the precision form, of its split-BF16
+    variant (tensor-core operator products) and of the FP64 path
     (CUDA events over min(args.steps, 100) steps after args.warmup), and the
     L2 / Linf error of the precision form against the FP64 path after 1000
     steps, with the FP64 conditioning floor (FP64 from the initial state
@@ -518,7 +522,7 @@ def p5_precision_case(stream, args, n=512, steps_err=1000):
     out = {"workload": f"TGV {n}x{n} jittered (seed 2) Q1 quads, P5, Navier-Stokes Re 5000, Roe, HU, SSP-RK3"}
     U0 = dt = None
     steps = min(args.steps, 100)
-    for prec in ("fp64", "mixed"):
+    for prec in ("fp64", "mixed", "split_bf16"):
         sv = solver(prec)
         if U0 is None:
             U0 = M.taylor_green(sv.solution_point_coords())
@@ -536,17 +540,19 @@ def p5_precision_case(stream, args, n=512, steps_err=1000):
         out[prec] = {"ms_per_step": ms, "value": sv.n_elem * sv.n_sp * 3 / (ms * 1e-3), "steps": steps}
         sv.close()
     out["speedup_vs_fp64"] = out["mixed"]["value"] / out["fp64"]["value"]
+    out["split_bf16"]["speedup_vs_fp64"] = out["split_bf16"]["value"] / out["fp64"]["value"]
     if not args.no_error_run:
-        s64, s32, sfl = solver("fp64"), solver("mixed"), solver("fp64")
-        for sv, U in ((s64, U0), (s32, U0), (sfl, U0.astype(np.float32).astype(np.float64))):
+        s64, s32, sbf, sfl = solver("fp64"), solver("mixed"), solver("split_bf16"), solver("fp64")
+        for sv, U in ((s64, U0), (s32, U0), (sbf, U0), (sfl, U0.astype(np.float32).astype(np.float64))):
             sv.copyToDevice(U)
             sv.advance(dt, steps_err)
-        U64, U32, Ufl = s64.copyToHost(), s32.copyToHost(), sfl.copyToHost()
-        for sv in (s64, s32, sfl):
+        U64, U32, Ubf, Ufl = s64.copyToHost(), s32.copyToHost(), sbf.copyToHost(), sfl.copyToHost()
+        for sv in (s64, s32, sbf, sfl):
             sv.close()
-        e, fl = state_errors(U32, U64), state_errors(Ufl, U64)
+        e, eb, fl = state_errors(U32, U64), state_errors(Ubf, U64), state_errors(Ufl, U64)
         out["errors"] = {"steps": steps_err, "dt": dt, "cfl": 0.3, "vars": ["rho", "rhou", "rhov", "rhoE"],
-                         "l2": e["l2"], "linf": e["linf"], "fp64_floor_l2": fl["l2"]}
+                         "l2": e["l2"], "linf": e["linf"], "fp64_floor_l2": fl["l2"],
+                         "split_bf16_l2": eb["l2"], "split_bf16_linf": eb["linf"]}
     return out
 
 

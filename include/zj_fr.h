@@ -47,8 +47,12 @@ typedef enum zj_flux_type { ZJ_FLUX_DG = 0, ZJ_FLUX_SD = 1, ZJ_FLUX_HU = 2, ZJ_F
 typedef enum zj_riemann { ZJ_RIEMANN_RUSANOV = 0, ZJ_RIEMANN_ROE = 1, ZJ_RIEMANN_HLLC = 2 } zj_riemann;
 
 /* Arithmetic of the residual.  ZJ_FP64: FP64 end to end.  ZJ_MIXED: FP32
- * volume and face work, FP64 stage accumulation, reductions and metrics. */
-typedef enum zj_precision { ZJ_FP64 = 0, ZJ_MIXED = 1 } zj_precision;
+ * volume and face work, FP64 stage accumulation, reductions and metrics.
+ * ZJ_SPLIT_BF16: the mixed form whose Navier-Stokes stage at P4/P5 on quad
+ * meshes takes its dense operator product (divergence and edge flux traces)
+ * on the tensor cores as three BF16 products accumulated in FP32; elsewhere
+ * (P1-P3, Euler, meshes with triangles) it is the mixed form. */
+typedef enum zj_precision { ZJ_FP64 = 0, ZJ_MIXED = 1, ZJ_SPLIT_BF16 = 2 } zj_precision;
 
 /* Element kinds of the mesh descriptor (types.hpp:41-44). */
 typedef enum zj_elem_type { ZJ_ELEM_TRI = 0, ZJ_ELEM_QUAD = 1 } zj_elem_type;
@@ -113,7 +117,7 @@ typedef struct zj_solver zj_solver;
 void zj_params_default(zj_params* p);
 /* Parse a config file with the reference grammar: "key value" lines, '#'
  * comments, unknown keys ignored; adds keys "compat on|off" and
- * "precision fp64|mixed". */
+ * "precision fp64|mixed|split_bf16". */
 zj_status zj_params_parse_file(const char* path, zj_params* p);
 zj_status zj_params_parse_string(const char* text, zj_params* p);
 

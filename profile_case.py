@@ -1,9 +1,10 @@
 """A few SSP-RK3 steps of the benchmark's cases, for external profilers (ncu)
 that capture a handful of launches:
 
-    python profile_case.py {ns|ns32|euler|euler32|compat|shear|shear32} [steps] [n] [P]
+    python profile_case.py {ns|ns32|ns_split|euler|euler32|compat|shear|shear32} [steps] [n] [P]
 
-ns / ns32: Navier-Stokes (Re 5000, Pr 0.72, Roe, HU), FP64 / precision form;
+ns / ns32 / ns_split: Navier-Stokes (Re 5000, Pr 0.72, Roe, HU), FP64 / precision
+form / split-BF16 form (tensor-core operator products at P4, P5);
 euler / euler32: the inviscid physics-mode residual; compat: the reference
 residual semantics.  256x256 jittered Q1 quads on [0,pi]^2 (seed 1), P3,
 slip walls, dt = 2e-4 (n overrides the mesh size, P the order; above P3 dt = 3e-5).
@@ -26,6 +27,8 @@ MODES = {
     "ns": dict(compat=False, viscous=True, riemann="Roe", flux_type="HU", Re=5000.0, Pr=0.72),
     "ns32": dict(compat=False, viscous=True, riemann="Roe", flux_type="HU", Re=5000.0, Pr=0.72,
                  precision="mixed"),
+    "ns_split": dict(compat=False, viscous=True, riemann="Roe", flux_type="HU", Re=5000.0, Pr=0.72,
+                     precision="split_bf16"),
     "euler": dict(compat=False, viscous=False, riemann="Roe", flux_type="HU"),
     "euler32": dict(compat=False, viscous=False, riemann="Roe", flux_type="HU", precision="mixed"),
     "compat": dict(compat=True, viscous=False, riemann="Rusanov", flux_type="HU"),

@@ -185,3 +185,19 @@ def test_mixed_precision_needs_physics_mode(zjlib):
     with pytest.raises(L.ZJError) as e:
         FRSolver(M.vortex_mesh(4), make_params(compat=True, precision="mixed"))
     assert e.value.code == L.ERR_UNSUPPORTED
+
+
+def test_precision_keys(zjlib):
+    """precision fp64 | mixed (alias fp32) | split_bf16; split_bf16 is a
+    physics-mode form like mixed and is refused in compat mode before any
+    device work."""
+    from zhijian_b200 import meshgen as M
+    from zhijian_b200.solver import FRSolver, make_params
+    for text, want in (("fp64", L.FP64), ("mixed", L.MIXED), ("fp32", L.MIXED), ("split_bf16", L.SPLIT_BF16)):
+        p = L.Params()
+        zjlib.zj_params_default(C.byref(p))
+        assert zjlib.zj_params_parse_string(f"precision {text}\n".encode(), C.byref(p)) == L.OK
+        assert p.precision == want
+    with pytest.raises(L.ZJError) as e:
+        FRSolver(M.vortex_mesh(4), make_params(compat=True, precision="split_bf16"))
+    assert e.value.code == L.ERR_UNSUPPORTED

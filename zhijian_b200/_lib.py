@@ -18,7 +18,7 @@ BC_TYPES = {"interior": 0, "wall": 1, "slipwall": 2, "symmetry": 3, "farfield": 
             "inflow": 5, "outflow": 6, "periodic": 7}
 FLUX_TYPES = {"DG": 0, "SD": 1, "HU": 2, "GA": 3}
 RIEMANN = {"Rusanov": 0, "Roe": 1, "HLLC": 2}
-FP64, MIXED = 0, 1
+FP64, MIXED, SPLIT_BF16 = 0, 1, 2
 MAX_BC = 32
 
 

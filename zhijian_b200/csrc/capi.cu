@@ -12,6 +12,7 @@
 // form (whose state and reductions stay FP64).
 // An SSP-RK3 step is three fused stage launches; the first step after a state
 // upload is preceded by one trace launch.
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include <cmath>
@@ -65,6 +66,12 @@ struct zj_solver {
     float* fOps = nullptr;
     float* fBC = nullptr;
     float4* fNrm = nullptr;
+    // split-BF16 Navier-Stokes stage (P4/P5, quads): BF16 operator image,
+    // its TMA tensor map and the kernel's wait-timeout flag
+    bool tc = false;
+    uint16_t* dTcImg = nullptr;
+    int* dTcErr = nullptr;
+    alignas(64) CUtensorMap tc_map;
     // meshes with triangles: element lists per kind, triangle operators
     int64_t n_tri = 0, n_quad = 0;
     int nt = 0;                     // triangle solution points
@@ -159,6 +166,9 @@ void free_all(zj_solver* s) {
     for (auto pp : fs) { if (*pp) cudaFree(*pp); *pp = nullptr; }
     if (s->fNrm) cudaFree(s->fNrm);
     s->fNrm = nullptr;
+    void* tcs[] = {s->dTcImg, s->dTcErr};
+    for (void* p : tcs) if (p) cudaFree(p);
+    s->dTcImg = nullptr; s->dTcErr = nullptr;
     void* ts[] = {s->dElistQ, s->dElistT, s->dTriOps, s->fTriOps, s->dEtype};
     for (void* p : ts) if (p) cudaFree(p);
     s->dElistQ = s->dElistT = nullptr; s->dTriOps = nullptr; s->fTriOps = nullptr; s->dEtype = nullptr;
@@ -184,8 +194,11 @@ zj_status validate_params(const zj_params* p, std::string& msg) {
     if (p->riemann < 0 || p->riemann > 2) { msg = "riemann must be Rusanov, Roe or HLLC"; return ZJ_ERR_ARG; }
     if (p->n_bc < 0 || p->n_bc > ZJ_MAX_BC) { msg = "n_bc out of range"; return ZJ_ERR_ARG; }
     if (!p->compat && p->viscous && !(p->Re > 0.0 && p->Pr > 0.0)) { msg = "Re and Pr must be > 0"; return ZJ_ERR_ARG; }
-    if (p->precision != ZJ_FP64 && p->precision != ZJ_MIXED) { msg = "precision must be fp64 or mixed"; return ZJ_ERR_ARG; }
-    if (p->precision == ZJ_MIXED && p->compat) {
+    if (p->precision != ZJ_FP64 && p->precision != ZJ_MIXED && p->precision != ZJ_SPLIT_BF16) {
+        msg = "precision must be fp64, mixed or split_bf16";
+        return ZJ_ERR_ARG;
+    }
+    if (p->precision != ZJ_FP64 && p->compat) {
         msg = "the mixed-precision form needs physics mode (compat off): compat mode is the reference's FP64 residual";
         return ZJ_ERR_UNSUPPORTED;
     }
@@ -249,6 +262,13 @@ cudaError_t launch_stage(const zj_solver* s, const StageArgsT<T>& a) {
         if (!is_ns(s)) return launch_phys_stage(s->P, s->prm.riemann, a, s->stream);
         cudaError_t e = launch_ns_grad(s->P, a, s->stream);
         if (e != cudaSuccess) return e;
+        if constexpr (sizeof(T) == 4) {
+            if (s->tc) {
+                StageArgsT<T> t = a;
+                t.tc_err = s->dTcErr;
+                return launch_ns_stage_tc(s->P, s->prm.riemann, t, &s->tc_map, s->stream);
+            }
+        }
         return launch_ns_stage(s->P, s->prm.riemann, a, s->stream);
     }
     // quads and triangles: every gradient trace before any stage (a face's
@@ -506,7 +526,15 @@ zj_status zj_solver_create(const zj_mesh_desc* mesh, const zj_params* params, zj
 #define ZJ_ALLOC(ptr, n)                                                     \
     if (e == cudaSuccess) e = dalloc(&(ptr), (n));
     for (int i = 0; i < 3; ++i) { ZJ_ALLOC(s->dU[i], s->state_n); }
-    s->mixed = params->precision == ZJ_MIXED;
+    s->mixed = params->precision != ZJ_FP64;
+    s->tc = params->precision == ZJ_SPLIT_BF16 && tc_order_supported(s->P) && is_ns(s) && s->n_tri == 0;
+    std::vector<uint16_t> tc_img;
+    if (s->tc) {
+        build_tc_image(s->P, s->ops, tc_img);
+        s->grid = tc_grid(s->P, s->E);
+        ZJ_ALLOC(s->dTcImg, tc_img.size());
+        ZJ_ALLOC(s->dTcErr, 1);
+    }
     if (!s->mixed) {
         for (int i = 0; i < 3; ++i) { ZJ_ALLOC(s->dT[i], s->trace_n); }
         if (is_ns(s)) { ZJ_ALLOC(s->dTQ, 2 * s->trace_n); }
@@ -549,6 +577,11 @@ zj_status zj_solver_create(const zj_mesh_desc* mesh, const zj_params* params, zj
     if (e == cudaSuccess) e = cudaMemcpy(s->dH, area.data(), area.size() * 8, cudaMemcpyHostToDevice);
     if (e == cudaSuccess) e = cudaMemcpy(s->dEdges, rec.data(), rec.size() * sizeof(EdgeRec), cudaMemcpyHostToDevice);
     if (e == cudaSuccess) e = cudaMemcpy(s->dNrm, nrm.data(), nrm.size() * 8, cudaMemcpyHostToDevice);
+    if (s->tc) {
+        if (e == cudaSuccess) e = cudaMemcpy(s->dTcImg, tc_img.data(), tc_img.size() * 2, cudaMemcpyHostToDevice);
+        if (e == cudaSuccess) e = cudaMemset(s->dTcErr, 0, sizeof(int));
+        if (e == cudaSuccess) e = make_tc_tensor_map(s->P, s->dTcImg, &s->tc_map);
+    }
     if (s->mixed) {
         // The geometry is computed once in FP64 on the host and rounded to
         // FP32 for the mixed-precision kernels.
@@ -763,6 +796,12 @@ zj_status zj_check_state(zj_solver* s) {
     ZJ_CK(s, cudaMemcpyAsync(&flag, s->dFlag, sizeof(int), cudaMemcpyDeviceToHost, s->stream), "check copy");
     ZJ_CK(s, cudaStreamSynchronize(s->stream), "check sync");
     if (flag) return fail(s, ZJ_ERR_NAN, "state holds NaN or Inf");
+    if (s->tc) {
+        int tflag = 0;
+        ZJ_CK(s, cudaMemcpy(&tflag, s->dTcErr, sizeof(int), cudaMemcpyDeviceToHost), "tensor-core flag copy");
+        if (tflag)
+            return fail(s, ZJ_ERR_TIMEOUT, "a split-BF16 stage gave up waiting for its operator copy or its tensor-core product");
+    }
     return ZJ_OK;
 }
 

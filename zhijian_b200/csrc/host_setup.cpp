@@ -644,7 +644,8 @@ void parse_stream(std::istream& in, zj_params* p) {
         } else if (key == "precision") {
             std::string t; iss >> t; t = lower(t);
             if (t == "fp64") p->precision = ZJ_FP64;
-            else if (t == "mixed" || t == "fp32" || t == "split_bf16") p->precision = ZJ_MIXED;
+            else if (t == "mixed" || t == "fp32") p->precision = ZJ_MIXED;
+            else if (t == "split_bf16") p->precision = ZJ_SPLIT_BF16;
         } else if (key == "bc") {
             int tag = 0;
             std::string type;

@@ -42,6 +42,7 @@ struct StageArgsT {
     T* TQout;               // gradient traces written by the gradient launch
     double Re, Pr;
     double iRe, kfac;       // 1/Re and gamma/((gamma-1) Pr) of the viscosity law
+    int* tc_err;            // split-BF16 kernel: set to 1 if a bounded wait gave up
     // Element list of a mesh with several element kinds: the launch visits
     // elist[0..n_list) (NULL: every element 0..n_elem)
     const int32_t* elist;
@@ -89,6 +90,15 @@ cudaError_t launch_tri(int what, int P, int riemann, bool viscous, const StageAr
 cudaError_t launch_tri(int what, int P, int riemann, bool viscous, const StageArgs32& a,
                        const int32_t* elist, long long n, cudaStream_t s);
 int tri_grid(int P, long long n);
+// Split-BF16 Navier-Stokes stage (ns_tc.cu), precision form at P4/P5 on
+// quad meshes: the operator image (BF16 hi/lo terms, build_tc_image) is
+// staged by TMA through the tensor map make_tc_tensor_map writes (128 bytes,
+// a CUtensorMap); grid tc_grid(P, E) CTAs (partials sized for it).
+bool tc_order_supported(int P);
+int tc_grid(int P, long long n);
+bool build_tc_image(int P, const Operators1D& o, std::vector<uint16_t>& img);
+cudaError_t make_tc_tensor_map(int P, const void* dev_img, void* map_out);
+cudaError_t launch_ns_stage_tc(int P, int riemann, const StageArgs32& a, const void* map, cudaStream_t s);
 // Quad CTA count of a launch over n elements.
 int quad_grid(int P, long long n);
 // Elementwise helpers of the differentiation entry points (jvp.cu).

@@ -37,7 +37,7 @@ def make_params(poly_order=3, gamma=1.4, rho_inf=1.0, p_inf=1.0 / 1.4, Mach=0.5,
     p.Pr = Pr
     p.T_inf = T_inf
     p.compat = int(bool(compat))
-    p.precision = L.FP64 if precision == "fp64" else L.MIXED
+    p.precision = {"fp64": L.FP64, "mixed": L.MIXED, "split_bf16": L.SPLIT_BF16}[precision]
     p.n_bc = 0
     for b in bcs:
         # (tag, type[, p_static]) or a dict with keys tag, type, p_static,
