@@ -224,7 +224,7 @@ k_adj_euler(const AdjArgs a) {
 
 // ---------------------------------------------------- pass B, Navier-Stokes --
 template <int P, int RIEM>
-__global__ void __launch_bounds__(Shape<P, 2>::THREADS, ZJ_ADJ_MIN_BLOCKS)
+__global__ void __launch_bounds__(Shape<P, 2>::THREADS, ZJ_ADJ_MIN_BLOCKS * kCtaScale)
 k_adj_ns(const AdjArgs a) {
     using S = Shape<P, 2>;
     constexpr int N1 = S::N1, NSP = S::NSP, NFT = S::NFT, TPE = S::TPE, EB = S::EB;

@@ -184,11 +184,12 @@ __device__ __forceinline__ void positivity(double* U) {
 
 // -------------------------------------------------------------- kernels --
 
-// Minimum resident CTAs per SM requested from the register allocator.
+// Minimum resident CTAs per SM requested from the register allocator (per
+// 256 threads, scaled to the CTA size).
 #ifndef ZJ_MIN_BLOCKS
 #define ZJ_MIN_BLOCKS 3
 #endif
-constexpr int kMinBlocks = ZJ_MIN_BLOCKS;
+constexpr int kMinBlocks = ZJ_MIN_BLOCKS * kCtaScale;
 
 template <int P>
 __global__ void __launch_bounds__(Shape<P>::THREADS, kMinBlocks)

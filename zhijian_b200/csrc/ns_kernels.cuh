@@ -32,7 +32,7 @@
 #include "phys_kernels.cuh"
 
 #ifndef ZJ_NS_MIN_BLOCKS
-#define ZJ_NS_MIN_BLOCKS 2        // FP64 stage kernel
+#define ZJ_NS_MIN_BLOCKS 2        // FP64 stage kernel (per 256 threads)
 #endif
 #ifndef ZJ_NSG_MIN_BLOCKS
 #define ZJ_NSG_MIN_BLOCKS 4       // FP64 gradient kernel
@@ -51,11 +51,12 @@ using namespace dev;
 using namespace phys;
 
 template <typename T> struct NSMinBlocks;
+// Minimum resident blocks of 256 threads, scaled to the CTA size.
 template <> struct NSMinBlocks<double> {
-    static constexpr int stage = ZJ_NS_MIN_BLOCKS, grad = ZJ_NSG_MIN_BLOCKS;
+    static constexpr int stage = ZJ_NS_MIN_BLOCKS * kCtaScale, grad = ZJ_NSG_MIN_BLOCKS * kCtaScale;
 };
 template <> struct NSMinBlocks<float> {
-    static constexpr int stage = ZJ_NS32_MIN_BLOCKS, grad = ZJ_NSG32_MIN_BLOCKS;
+    static constexpr int stage = ZJ_NS32_MIN_BLOCKS * kCtaScale, grad = ZJ_NSG32_MIN_BLOCKS * kCtaScale;
 };
 template <> struct NSMinBlocks<Dual> { static constexpr int stage = 1, grad = 1; };
 

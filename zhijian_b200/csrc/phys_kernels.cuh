@@ -212,8 +212,8 @@ __device__ __forceinline__ void state_minus_ref(const double* U, const T* ue, T*
 }
 
 template <typename T> struct PhysMinBlocks;
-template <> struct PhysMinBlocks<double> { static constexpr int value = ZJ_PHYS_MIN_BLOCKS; };
-template <> struct PhysMinBlocks<float> { static constexpr int value = ZJ_PHYS32_MIN_BLOCKS; };
+template <> struct PhysMinBlocks<double> { static constexpr int value = ZJ_PHYS_MIN_BLOCKS * kCtaScale; };
+template <> struct PhysMinBlocks<float> { static constexpr int value = ZJ_PHYS32_MIN_BLOCKS * kCtaScale; };
 template <> struct PhysMinBlocks<Dual> { static constexpr int value = 1; };
 
 template <int P, int RIEM, typename T>

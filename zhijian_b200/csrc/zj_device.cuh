@@ -10,6 +10,18 @@
 namespace zj {
 namespace dev {
 
+// Threads per CTA of the element-block kernels (rounded down to whole
+// elements).  128-thread CTAs interleave the load, shared-memory and
+// arithmetic phases of more blocks per SM than 256-thread ones (measured on
+// the Navier-Stokes residual at P3: 4-6% faster); launch bounds scale their
+// minimum resident blocks with it (kCtaScale), so the register limits per
+// thread stay those of the 256-thread tuning.
+#ifndef ZJ_CTA_THREADS
+#define ZJ_CTA_THREADS 128
+#endif
+constexpr int kCtaThreads = ZJ_CTA_THREADS;
+constexpr int kCtaScale = 256 / ZJ_CTA_THREADS;
+
 // EBDIV > 1 packs fewer elements per CTA: the dual-number instantiation
 // (16-byte values) uses EBDIV = 3 so its shared tiles stay within the 48 KB
 // of static shared memory.
@@ -19,7 +31,7 @@ struct Shape {
     static constexpr int NSP = N1 * N1;
     static constexpr int NFT = 4 * N1;                 // flux points per element
     static constexpr int TPE = NSP > NFT ? NSP : NFT;  // threads per element
-    static constexpr int EB = (256 / TPE / EBDIV) > 0 ? (256 / TPE / EBDIV) : 1;
+    static constexpr int EB = (kCtaThreads / TPE / EBDIV) > 0 ? (kCtaThreads / TPE / EBDIV) : 1;
     static constexpr int THREADS = EB * TPE;
     static constexpr int NOPS = N1 * N1 + 4 * N1;
     // Shared-memory layout of per-element fields (doubles): [var][eta row][xi]
