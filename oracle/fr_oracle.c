@@ -57,6 +57,7 @@ struct orc_ctx {
     int tag_ids[64];
     double tag_pt[64], tag_Tt[64], tag_dx[64], tag_dy[64], tag_Tw[64], tag_ps[64];
     double *flen;
+    double *fpn;      /* curved meshes, physics mode: [nf][nfp][3] (nx, ny, s) per face point */
 };
 
 /* ---------------------------------------------------------------- basis -- */
@@ -499,7 +500,7 @@ void orc_destroy(orc_ctx* c) {
     void* ps[] = {c->xy, c->conn, c->J, c->Jinv, c->area, c->fle, c->fll, c->fre, c->frl,
                   c->fbct, c->ftag, c->fbcmap, c->fn, c->bc_data, c->pts, c->D1, c->dxi,
                   c->deta, c->interp, c->corr, c->Fx, c->Fy, c->Ufp, c->Fcom, c->Fdiff,
-                  c->U0, c->U1, c->flen};
+                  c->U0, c->U1, c->flen, c->fpn};
     for (size_t i = 0; i < sizeof(ps) / sizeof(ps[0]); ++i) free(ps[i]);
     free(c);
 }
@@ -1124,6 +1125,52 @@ void orc_wall_viscous_closure(const orc_ctx* c, int bct, int tag, double nx, dou
     }
 }
 
+/* Curved elements (geometric order 2 or 4) in physics mode: the unit normal
+ * and the edge Jacobian s = |dx/dt| at every point of every face, from the
+ * face's left element's mapping (basis.cpp:717-847 shape functions).  The
+ * left element's edge ll runs counter-clockwise with t the 1-D flux points:
+ * (t,-1), (1,t), (-t,1), (-1,-t) for edges 0..3; the outward normal is the
+ * tangent turned clockwise.  On a straight edge s = length/2 and n is the
+ * face normal. */
+static void build_face_point_normals(orc_ctx* c) {
+    const int nfp = c->nfp;
+    c->fpn = (double*)malloc(sizeof(double) * (size_t)c->n_faces * nfp * 3);
+    for (int64_t f = 0; f < c->n_faces; ++f) {
+        const int le = c->fle[f], ll = c->fll[f];
+        const int64_t* nd = c->conn + (int64_t)le * c->nn;
+        for (int fp = 0; fp < nfp; ++fp) {
+            const double t = c->pts[fp];
+            double xi, eta, dxi, deta;
+            if (ll == 0) { xi = t; eta = -1.0; dxi = 1.0; deta = 0.0; }
+            else if (ll == 1) { xi = 1.0; eta = t; dxi = 0.0; deta = 1.0; }
+            else if (ll == 2) { xi = -t; eta = 1.0; dxi = -1.0; deta = 0.0; }
+            else { xi = -1.0; eta = -t; dxi = 0.0; deta = -1.0; }
+            double N[25], dNx[25], dNe[25];
+            const int n = shape_quad(c->eorder, xi, eta, N, dNx, dNe);
+            double tx = 0.0, ty = 0.0;
+            for (int i = 0; i < n; ++i) {
+                const double w = dNx[i] * dxi + dNe[i] * deta;
+                tx += w * c->xy[2 * nd[i]];
+                ty += w * c->xy[2 * nd[i] + 1];
+            }
+            const double len = sqrt(tx * tx + ty * ty);
+            double* q = c->fpn + ((size_t)f * nfp + fp) * 3;
+            q[0] = ty / len; q[1] = -tx / len; q[2] = len;
+        }
+    }
+}
+
+/* (nx, ny, s) of point fp of face f: per point on curved meshes, else the
+ * face's normal and half its length. */
+static void face_point(const orc_ctx* c, int64_t f, int fp, double* nx, double* ny, double* s) {
+    if (c->fpn) {
+        const double* q = c->fpn + ((size_t)f * c->nfp + fp) * 3;
+        *nx = q[0]; *ny = q[1]; *s = q[2];
+    } else {
+        *nx = c->fn[2 * f]; *ny = c->fn[2 * f + 1]; *s = 0.5 * c->flen[f];
+    }
+}
+
 void orc_rhs_phys(orc_ctx* c, const double* U, double* R) {
     const int nsp = c->nsp, n1 = c->n1, nfp = c->nfp;
     const int64_t ne = c->n_elem, nf = c->n_faces;
@@ -1133,6 +1180,7 @@ void orc_rhs_phys(orc_ctx* c, const double* U, double* R) {
     size_t fpn = (size_t)ne * 4 * nfp * 4;
     double* Ft = c->Fx; double* Gt = c->Fy;          /* transformed fluxes at sp */
     double* FnD = (double*)malloc(sizeof(double) * fpn);
+    if (c->eorder > 1 && !c->fpn) build_face_point_normals(c);
     /* traces of the state (dense interp) */
 #pragma omp parallel for num_threads(nt) schedule(static)
     for (int64_t e = 0; e < ne; ++e)
@@ -1155,8 +1203,10 @@ void orc_rhs_phys(orc_ctx* c, const double* U, double* R) {
 #pragma omp parallel for num_threads(nt) schedule(static)
         for (int64_t f = 0; f < nf; ++f) {
             int le = c->fle[f], ll = c->fll[f], re = c->fre[f], rl = c->frl[f];
-            double nx = c->fn[2 * f], ny = c->fn[2 * f + 1];
             for (int fp = 0; fp < nfp; ++fp) {
+                double nx, ny, s;
+                face_point(c, f, fp, &nx, &ny, &s);
+                (void)s;
                 int64_t lo = (((int64_t)le * 4 + ll) * nfp + fp) * 4;
                 const double* UL = c->Ufp + lo;
                 double UR[4];
@@ -1241,8 +1291,9 @@ void orc_rhs_phys(orc_ctx* c, const double* U, double* R) {
 #pragma omp parallel for num_threads(nt) schedule(static)
     for (int64_t f = 0; f < nf; ++f) {
         int le = c->fle[f], ll = c->fll[f], re = c->fre[f], rl = c->frl[f];
-        double nx = c->fn[2 * f], ny = c->fn[2 * f + 1], s = 0.5 * c->flen[f];
         for (int fp = 0; fp < nfp; ++fp) {
+            double nx, ny, s;
+            face_point(c, f, fp, &nx, &ny, &s);
             int64_t lo = (((int64_t)le * 4 + ll) * nfp + fp) * 4;
             const double* UL = c->Ufp + lo;
             double UR[4], Fc[4];

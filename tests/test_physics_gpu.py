@@ -107,20 +107,27 @@ def test_full_size_tgv_roe(zjlib, oracle_mod):
     assert abs(tot[0]) <= 1e-12 * scale and abs(tot[3]) <= 1e-12 * scale
 
 
-def test_physics_mode_rejects_curved_elements(zjlib):
-    m = M.vortex_mesh(2)
-    # a Q2 mesh: add edge midpoints and centres by sub-sampling a 4x4 grid
-    fine = M.structured_quads(4, 4, -10.0, 10.0, -10.0, 10.0)
+def test_physics_mode_takes_straight_q2_elements_like_q1(zjlib):
+    """A Q2 mesh whose edge and centre nodes sit at the midpoints (straight
+    edges) gives the Q1 mesh's physics-mode residual to rounding: the
+    per-flux-point normals of the curved-element path reduce to the per-edge
+    ones."""
+    fine = M.structured_quads(4, 4, -10.0, 10.0, -10.0, 10.0, 0.0, 0, (1, 1, 1, 1), {1: "farfield"})
+    q1 = M.structured_quads(2, 2, -10.0, 10.0, -10.0, 10.0, 0.0, 0, (1, 1, 1, 1), {1: "farfield"})
     conn = []
     for ej in range(2):
         for ei in range(2):
             n = lambda i, j: (2 * ej + j) * 5 + (2 * ei + i)
             conn.append([n(0, 0), n(2, 0), n(2, 2), n(0, 2), n(1, 0), n(2, 1), n(1, 2), n(0, 1), n(1, 1)])
-    q2 = M.QuadMesh(fine.xy, np.array(conn, dtype=np.int64), m.bnd * 0 + np.array([0, 2, 1]), {1: "farfield"})
-    q2.bnd = np.array([[0, 2, 1]], dtype=np.int64)
-    with pytest.raises(L.ZJError) as e:
-        FRSolver(q2, make_params(compat=False))
-    assert e.value.code == L.ERR_UNSUPPORTED
+    bnd = np.array([[0, 2, 1], [2, 4, 1], [4, 14, 1], [14, 24, 1], [24, 22, 1], [22, 20, 1], [20, 10, 1],
+                    [10, 0, 1]], dtype=np.int64)
+    q2 = M.QuadMesh(fine.xy, np.array(conn, dtype=np.int64), bnd, {1: "farfield"})
+    kw = dict(poly_order=3, compat=False, riemann="Roe", rho_inf=1.2, p_inf=1.0e5, Mach=0.4, AoA=10.0,
+              bcs=[(1, "farfield")])
+    U = M.random_state(4, 16, 3, 1.4, 1.2, 1.0e5, 0.05)
+    R1 = FRSolver(q1, make_params(**kw)).rhs(U)
+    R2 = FRSolver(q2, make_params(**kw)).rhs(U)
+    assert T.rel_err(R2, R1, T.euler_flux_scale(U) * 0.2) <= 1e-12
 
 
 # ------------------------------------------------------------ Navier-Stokes --

@@ -59,6 +59,7 @@ struct zj_solver {
     double4* dNrm = nullptr;
     // mixed-precision form: FP32 traces, gradient traces and geometry
     bool mixed = false;
+    int nrm_pp = 0;             // curved elements in physics mode: normals per flux point
     float* fT[3] = {nullptr, nullptr, nullptr};
     float* fTQ = nullptr;
     float* fJinv = nullptr;
@@ -220,13 +221,13 @@ template <typename T> StageArgsT<T> base_args(const zj_solver* s);
 template <> StageArgsT<double> base_args<double>(const zj_solver* s) {
     StageArgsT<double> a{};
     a.Jinv = s->dJinv; a.J = s->dJ; a.enrm = s->dNrm; a.bc = s->dBC; a.ops = s->dOps;
-    a.TQ = s->dTQ; a.TQout = s->dTQ;
+    a.TQ = s->dTQ; a.TQout = s->dTQ; a.nrm_pp = s->nrm_pp;
     return a;
 }
 template <> StageArgsT<float> base_args<float>(const zj_solver* s) {
     StageArgsT<float> a{};
     a.Jinv = s->fJinv; a.J = s->fJ; a.enrm = s->fNrm; a.bc = s->fBC; a.ops = s->fOps;
-    a.TQ = s->fTQ; a.TQout = s->fTQ;
+    a.TQ = s->fTQ; a.TQout = s->fTQ; a.nrm_pp = s->nrm_pp;
     return a;
 }
 
@@ -472,10 +473,6 @@ zj_status zj_solver_create(const zj_mesh_desc* mesh, const zj_params* params, zj
     if (!build_mesh(mesh, params, s->mesh, msg)) { delete s; return fail(nullptr, ZJ_ERR_ARG, msg); }
     s->E = s->mesh.n_elem;
     if (s->E > (1LL << 31) / (4LL * s->nsp)) { delete s; return fail(nullptr, ZJ_ERR_ARG, "mesh too large"); }
-    if (!params->compat && s->mesh.order != 1) {
-        delete s;
-        return fail(nullptr, ZJ_ERR_UNSUPPORTED, "physics mode needs straight-edged (Q1) elements");
-    }
     if (params->compat) build_operators_compat(s->P, s->ops);
     else build_operators_vcjh(s->P, params->flux_type, s->ops);
     s->n_tri = s->mesh.n_tri;
@@ -503,12 +500,19 @@ zj_status zj_solver_create(const zj_mesh_desc* mesh, const zj_params* params, zj
     }
     build_bc_data(s->mesh, params, bc);
     build_edge_records(s->mesh, rec, nrm);
+    if (!params->compat && s->mesh.order > 1) {
+        // curved elements: the conservative face term takes the normal and
+        // the edge Jacobian of every flux point (compat mode keeps the
+        // reference's one normal per face)
+        build_point_normals(s->mesh, s->ops, nrm);
+        s->nrm_pp = 1;
+    }
     element_areas(s->mesh, area);
     for (auto& a : area) a = std::sqrt(a);
     pack_ops(s->ops, packed);
 
     s->n_jinv = Jinv.size(); s->n_j = J.size(); s->n_ops = packed.size();
-    s->n_bcd = bc.size(); s->n_nrm = rec.size();
+    s->n_bcd = bc.size(); s->n_nrm = nrm.size() / 4;
     s->state_n = (size_t)s->E * s->nsp * 4;
     // element traces, then one ghost row per boundary slot (physics mode)
     s->trace_n = ((size_t)s->E * 4 + (size_t)s->mesh.n_bnd_faces) * s->n1 * 4;
@@ -545,7 +549,7 @@ zj_status zj_solver_create(const zj_mesh_desc* mesh, const zj_params* params, zj
         ZJ_ALLOC(s->fJ, J.size());
         ZJ_ALLOC(s->fOps, packed.size());
         ZJ_ALLOC(s->fBC, bc.size());
-        ZJ_ALLOC(s->fNrm, rec.size());
+        ZJ_ALLOC(s->fNrm, nrm.size() / 4);
     }
     ZJ_ALLOC(s->dUs, s->state_n);
     ZJ_ALLOC(s->dRs, s->state_n);
@@ -560,7 +564,7 @@ zj_status zj_solver_create(const zj_mesh_desc* mesh, const zj_params* params, zj
     ZJ_ALLOC(s->dScratch, (size_t)s->scratch_n);
     ZJ_ALLOC(s->dFlag, 1);
     ZJ_ALLOC(s->dEdges, rec.size());
-    ZJ_ALLOC(s->dNrm, rec.size());
+    ZJ_ALLOC(s->dNrm, nrm.size() / 4);
     if (s->n_tri > 0) {
         ZJ_ALLOC(s->dElistQ, listq.size());
         ZJ_ALLOC(s->dElistT, listt.size());
@@ -899,6 +903,7 @@ zj_status diff_supported(zj_solver* s) {
     if (s->prm.compat) return fail(s, ZJ_ERR_UNSUPPORTED, "differentiation needs physics mode (compat off)");
     if (s->mixed) return fail(s, ZJ_ERR_UNSUPPORTED, "differentiation runs on the FP64 path (precision fp64)");
     if (s->n_tri > 0) return fail(s, ZJ_ERR_UNSUPPORTED, "differentiation runs on quadrilateral meshes");
+    if (s->nrm_pp) return fail(s, ZJ_ERR_UNSUPPORTED, "differentiation runs on straight-edged (Q1) meshes");
     return ZJ_OK;
 }
 

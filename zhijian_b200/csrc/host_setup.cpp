@@ -414,6 +414,51 @@ int shape(int order, double xi, double eta, double* N, double* dNx, double* dNe)
 }
 }  // namespace
 
+// Normals of a curved mesh at every flux point: [E][4][n1][4] = (nx, ny,
+// 2 s, 0) with s = |dx/dt| the edge Jacobian at the point and n the face's
+// unit normal there, both from the left element's mapping (shape functions of
+// basis.cpp:717-847).  Edge k of the reference square runs counter-clockwise
+// with t = the 1-D flux points: edge 0 (t, -1), edge 1 (1, t), edge 2
+// (-t, 1), edge 3 (-1, -t); the outward normal of a positively oriented
+// element is the tangent dx/dt turned clockwise.  The face's right element
+// gets the same (face) normal at its coinciding point n1-1-fp, as the
+// per-edge records of straight meshes do.  The 2 s slot keeps the kernels'
+// s = 0.5 * length of a straight edge (for which 2 s is the length).
+void build_point_normals(const HostMesh& m, const Operators1D& ops, std::vector<double>& nrm) {
+    const int n1 = ops.n1;
+    nrm.assign((size_t)m.n_elem * 4 * n1 * 4, 0.0);
+    for (int64_t f = 0; f < m.n_faces; ++f) {
+        const int64_t le = m.fle[(size_t)f];
+        const int ll = m.fll[(size_t)f];
+        const int64_t* nd = &m.conn[(size_t)le * m.nn];
+        for (int fp = 0; fp < n1; ++fp) {
+            const double t = ops.pts[(size_t)fp];
+            double xi, eta, sx, se;
+            switch (ll) {
+                case 0: xi = t; eta = -1.0; sx = 1.0; se = 0.0; break;
+                case 1: xi = 1.0; eta = t; sx = 0.0; se = 1.0; break;
+                case 2: xi = -t; eta = 1.0; sx = -1.0; se = 0.0; break;
+                default: xi = -1.0; eta = -t; sx = 0.0; se = -1.0; break;
+            }
+            double N[25], dNx[25], dNe[25];
+            const int n = shape(m.order, xi, eta, N, dNx, dNe);
+            double tx = 0.0, ty = 0.0;
+            for (int i = 0; i < n; ++i) {
+                const double dn = dNx[i] * sx + dNe[i] * se;
+                tx += dn * m.xy[2 * nd[i]];
+                ty += dn * m.xy[2 * nd[i] + 1];
+            }
+            const double len = std::sqrt(tx * tx + ty * ty);
+            const double rec[4] = {ty / len, -tx / len, 2.0 * len, 0.0};
+            std::memcpy(&nrm[(((size_t)le * 4 + ll) * n1 + fp) * 4], rec, sizeof(rec));
+            if (m.fre[(size_t)f] >= 0) {
+                const size_t r = ((size_t)m.fre[(size_t)f] * 4 + m.frl[(size_t)f]) * n1 + (n1 - 1 - fp);
+                std::memcpy(&nrm[r * 4], rec, sizeof(rec));
+            }
+        }
+    }
+}
+
 // Affine map of a triangle: x_r = (v1 - v0)/2, x_s = (v2 - v0)/2.
 static void tri_jacobian(const HostMesh& m, int64_t e, double& a, double& b, double& c, double& d) {
     const int64_t* nd = &m.conn[(size_t)e * m.nn];

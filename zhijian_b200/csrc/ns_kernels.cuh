@@ -144,7 +144,7 @@ __device__ __forceinline__ void load_face_point(const StageArgsT<T>& a, long lon
     constexpr int NFT = 4 * N1;
     f.r = a.edges[e * 4 + edge];
     T n[3];
-    load_normal(a.enrm + e * 4 + edge, n);
+    load_normal(normal_rec<N1>(a, e, edge, fp), n);
     f.nx = n[0]; f.ny = n[1]; f.len = n[2];
     load4_nc(a.Tin + (e * NFT + edge * N1 + fp) * 4, f.qo);
     f.qn[0] = f.qo[0]; f.qn[1] = f.qo[1]; f.qn[2] = f.qo[2]; f.qn[3] = f.qo[3];

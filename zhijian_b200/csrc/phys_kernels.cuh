@@ -74,6 +74,15 @@ __device__ __forceinline__ long long block_element(const StageArgsT<T>& a, int E
     return g;
 }
 
+// Normal record of flux point fp on edge `edge` of element e: one per edge on
+// straight-sided meshes, one per flux point on curved ones (a.nrm_pp).
+template <int N1, typename T>
+__device__ __forceinline__ const typename Vec4Of<T>::type* normal_rec(const StageArgsT<T>& a, long long e,
+                                                                     int edge, int fp) {
+    const long long r = e * 4 + edge;
+    return a.enrm + (a.nrm_pp ? r * N1 + fp : r);
+}
+
 // Boundary ghost states live in extra rows of every trace buffer, after the
 // E*4 element edges: row E*4 + slot of boundary slot `slot`, stored at the
 // mirrored point n1-1-fp, so a boundary edge loads its ghost exactly like an
@@ -252,7 +261,7 @@ k_phys_stage(const StageArgsT<T> a) {
     if (kRef && valid) load_state(a.U + e * NSP * 4, ue);
     if (is_fp) {
         r = a.edges[e * 4 + edge];
-        load_normal(a.enrm + e * 4 + edge, nr);
+        load_normal(normal_rec<N1>(a, e, edge, fp), nr);
         load4_nc(a.Tin + (e * NFT + k) * 4, qo);
     }
     if (is_sp) {
@@ -442,7 +451,7 @@ k_phys_traces(const StageArgsT<T> a) {
         const EdgeRec r = a.edges[e * 4 + edge];
         if (r.flags & kEdgeBoundary) {
             T n[3];
-            load_normal(a.enrm + e * 4 + edge, n);
+            load_normal(normal_rec<N1>(a, e, edge, fp), n);
             store_ghost<N1>(a, r, n[0], n[1], fp, t);
         }
     }

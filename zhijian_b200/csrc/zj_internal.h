@@ -101,6 +101,9 @@ void element_areas(const HostMesh& m, std::vector<double>& area);
 // Boundary data, 8 doubles per boundary slot (fr_solver.cpp:432-482).
 void build_bc_data(const HostMesh& m, const zj_params* p, std::vector<double>& bc);
 void build_edge_records(const HostMesh& m, std::vector<EdgeRec>& rec, std::vector<double>& nrm);
+// Curved meshes in physics mode: the face normal and edge Jacobian at every
+// flux point, [E][4][n1][4] = (nx, ny, 2 |dx/dt|, 0).
+void build_point_normals(const HostMesh& m, const Operators1D& ops, std::vector<double>& nrm);
 
 // Gmsh reader (gmsh.cpp).
 struct GmshGroup {

@@ -29,7 +29,9 @@ struct StageArgsT {
     const T* Jinv;          // [E][n_sp][4] = (xi_x, xi_y, eta_x, eta_y)
     const T* J;             // [E][n_sp]
     const EdgeRec* edges;   // [E][4]
-    const typename Vec4Of<T>::type* enrm;  // [E][4] = (face nx, face ny, edge length, 0)
+    const typename Vec4Of<T>::type* enrm;  // [E][4] = (face nx, face ny, edge length, 0), or
+                                           // [E][4][n1] per flux point (nrm_pp) on curved meshes
+                                           // with 2 |dx/dt| in the length slot
     const T* bc;            // [slots][8]
     const T* ops;           // packed 1D operators, see OpsLayout
     const double* dt;       // device scalar: step size
@@ -43,6 +45,7 @@ struct StageArgsT {
     double Re, Pr;
     double iRe, kfac;       // 1/Re and gamma/((gamma-1) Pr) of the viscosity law
     int* tc_err;            // split-BF16 kernel: set to 1 if a bounded wait gave up
+    int nrm_pp;             // 1: enrm holds one record per flux point (curved elements)
     // Element list of a mesh with several element kinds: the launch visits
     // elist[0..n_list) (NULL: every element 0..n_elem)
     const int32_t* elist;

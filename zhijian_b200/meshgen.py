@@ -132,6 +132,56 @@ def structured_quads(nx: int, ny: int, x0: float, x1: float, y0: float, y1: floa
     return QuadMesh(xy, conn, bnd, dict(tag_names))
 
 
+# Node positions of the Q2 (9-node) and Q4 (25-node) quads on the element's
+# (order+1)^2 lattice, in the shape-function order of basis.cpp:717-847
+# (corners counter-clockwise from (-1,-1), then edge nodes, then interior).
+_Q2_LATTICE = [(0, 0), (2, 0), (2, 2), (0, 2), (1, 0), (2, 1), (1, 2), (0, 1), (1, 1)]
+_Q4_XI = [0, 4, 4, 0, 1, 2, 3, 4, 4, 4, 3, 2, 1, 0, 0, 0, 1, 2, 3, 1, 2, 3, 1, 2, 3]
+_Q4_ETA = [0, 0, 4, 4, 0, 0, 0, 1, 2, 3, 4, 4, 4, 3, 2, 1, 1, 1, 1, 2, 2, 2, 3, 3, 3]
+
+
+def curved_quads(nx: int, ny: int, order: int, x0: float, x1: float, y0: float, y1: float,
+                 amp: float = 0.03, side_tags=(1, 1, 1, 1), tag_names=None) -> QuadMesh:
+    """nx*ny curved quads of geometric order 2 or 4 on [x0,x1]x[y0,y1]: every
+    node of the (order*nx+1) x (order*ny+1) lattice, element corners, edge
+    and interior nodes alike, is moved by the smooth map
+      x += amp (x1-x0) sin(pi s) sin(2 pi t),  y += amp (y1-y0) sin(2 pi s) sin(pi t)
+    (s, t the lattice coordinates scaled to [0, 1]), which vanishes on the
+    boundary: the outer edges stay straight, every interior edge is curved.
+    Boundary edges are listed by their corner nodes (the reference's face
+    tags), side_tags = (bottom, right, top, left)."""
+    if order not in (2, 4):
+        raise ValueError("order must be 2 or 4")
+    mx, my = order * nx, order * ny
+    ii, jj = np.meshgrid(np.arange(mx + 1), np.arange(my + 1))
+    ii = ii.ravel(); jj = jj.ravel()
+    s_, t_ = ii / mx, jj / my
+    x = x0 + s_ * (x1 - x0) + amp * (x1 - x0) * np.sin(np.pi * s_) * np.sin(2.0 * np.pi * t_)
+    y = y0 + t_ * (y1 - y0) + amp * (y1 - y0) * np.sin(2.0 * np.pi * s_) * np.sin(np.pi * t_)
+    x[ii == 0] = x0; x[ii == mx] = x1
+    y[jj == 0] = y0; y[jj == my] = y1
+    xy = np.stack([x, y], axis=1).astype(np.float64)
+    node = lambda a, b: b * (mx + 1) + a
+    lat = _Q2_LATTICE if order == 2 else list(zip(_Q4_XI, _Q4_ETA))
+    conn = []
+    for ej in range(ny):
+        for ei in range(nx):
+            conn.append([node(order * ei + a, order * ej + b) for a, b in lat])
+    conn = np.asarray(conn, dtype=np.int64)
+    b = []
+    for i in range(nx):
+        b.append((node(order * i, 0), node(order * (i + 1), 0), side_tags[0]))
+    for j in range(ny):
+        b.append((node(mx, order * j), node(mx, order * (j + 1)), side_tags[1]))
+    for i in range(nx):
+        b.append((node(order * (i + 1), my), node(order * i, my), side_tags[2]))
+    for j in range(ny):
+        b.append((node(0, order * (j + 1)), node(0, order * j), side_tags[3]))
+    if tag_names is None:
+        tag_names = {t: "farfield" for t in set(side_tags)}
+    return QuadMesh(xy, conn, np.asarray(b, dtype=np.int64), dict(tag_names))
+
+
 # ------------------------------------------------------------- the configs --
 
 def vortex_mesh(n: int = 20) -> QuadMesh:
