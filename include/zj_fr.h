@@ -233,6 +233,49 @@ void* zj_get_stream(const zj_solver* s);
 #define ZJ_NOALLOC_SCRATCH_BYTES (32u * 1024u * 1024u)
 zj_status zj_rhs_noalloc(zj_solver* s, const double* U_dev, double* R_dev);
 
+/* ---- mesh partitions (several GPUs) -----------------------------
+ * Replace MeshPartitioner::partition (src/mesh/partitioner.cpp:10-93, METIS
+ * k-way on the element dual graph) and MPICommunicator::exchangeHalo
+ * (src/parallel/mpi_comm.cpp:68-171).  A partitioned mesh runs as one handle
+ * per part; the parts couple only through the traces and gradient traces at
+ * the faces the partition cuts, which cross after every launch that writes
+ * them: the sender gathers its side's trace rows, the receiver copies them
+ * into its own memory (a peer copy between devices) and scatters them into
+ * the ghost rows its interface faces read.  Physics mode, quadrilateral
+ * meshes (straight or curved), FP64, mixed or split_bf16; the result equals
+ * the whole mesh's residual.
+ *
+ * zj_partition: recursive coordinate bisection of the element centroids into
+ * nparts parts whose sizes differ by at most one element (deterministic);
+ * part[E].  Host only. */
+zj_status zj_partition(const zj_mesh_desc* mesh, int nparts, int32_t* part);
+/* The halo plan of part `rank` (host only): n_nbr neighbouring parts nbr[]
+ * (ascending) with their interfaces [nbr_off[i], nbr_off[i+1]) in the global
+ * face order (the order both sides of a cut agree on); per interface the
+ * global face id, this part's side and the other side as global
+ * element*4 + local edge; elems (may be NULL) the part's global element ids,
+ * ascending.  Sizes from zj_halo_plan_size (n_elem may be NULL). */
+zj_status zj_halo_plan_size(const zj_mesh_desc* mesh, const int32_t* part, int nparts, int rank, int* n_nbr,
+                            int64_t* n_iface, int64_t* n_elem);
+zj_status zj_halo_plan(const zj_mesh_desc* mesh, const int32_t* part, int nparts, int rank, int32_t* nbr,
+                       int64_t* nbr_off, int64_t* face, int64_t* mine, int64_t* remote, int64_t* elems);
+/* The handle of part `rank`, on the device current at the call: its state is
+ * [E_part][n_sp][4] over its elements in ascending global order
+ * (zj_part_elements), set and read with zj_set_state / zj_get_state as
+ * usual.  zj_step and zj_rhs refuse a part (ZJ_ERR_UNSUPPORTED): the parts
+ * of a partition step together. */
+zj_status zj_solver_create_part(const zj_mesh_desc* mesh, const zj_params* params, const int32_t* part,
+                                int nparts, int rank, zj_solver** out);
+zj_status zj_part_elements(const zj_solver* s, int64_t* global_ids);
+/* All n parts of one partition from one process (any order; each on its own
+ * device and stream, ordered by events): nsteps SSP-RK3 steps, one residual
+ * of the device states U_dev[rank] into R_dev[rank], synchronisation, and the
+ * L2 norm of the last stage's residual over all parts. */
+zj_status zj_parts_step(zj_solver* const* parts, int n, double dt, int nsteps);
+zj_status zj_parts_rhs(zj_solver* const* parts, int n, const double* const* U_dev, double* const* R_dev);
+zj_status zj_parts_synchronize(zj_solver* const* parts, int n);
+zj_status zj_parts_residual_norm(zj_solver* const* parts, int n, double* out);
+
 /* ---- differentiation (physics mode, FP64) ----------------------------------
  * No reference counterpart: the reference has no adjoint.  All pointers are
  * device pointers to [E][n_sp][4] FP64 arrays, 16-byte aligned; the calls are

@@ -1,0 +1,75 @@
+"""Partitioned meshes on the GPU: the parts of a mesh as handles driven
+together by zj_parts_rhs / zj_parts_step (their cut faces' traces and
+gradient traces copied into each other's ghost rows after every launch that
+writes them), on one device here -- the same driver moves the rows with peer
+copies when the parts sit on different GPUs.  Every part evaluates each face
+from the same inputs with the same orientation as the whole-mesh handle, so
+residuals and steps equal the whole mesh's bit for bit; the residual norm sums
+the parts' partial sums in another order (within 1e-13)."""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+from zhijian_b200 import _lib as L
+from zhijian_b200 import meshgen as M
+from zhijian_b200 import partition as PT
+from zhijian_b200.solver import FRSolver, make_params
+from tests.test_physics_gpu import BCS_A, BCS_B
+
+pytestmark = pytest.mark.gpu
+KW = dict(rho_inf=1.2, p_inf=1.0e5, Mach=0.4, AoA=10.0, T_inf=8.5e4)
+
+
+def mesh_of(kind, bcs):
+    names = {b["tag"]: b["type"] for b in bcs}
+    if kind == "curved":
+        return M.curved_quads(7, 6, 2, 0.0, 1.0, 0.0, 1.0, 0.04, (1, 2, 3, 4), names)
+    return M.structured_quads(9, 7, 0.0, 1.0, 0.0, 1.0, 0.15, 5, (1, 2, 3, 4), names)
+
+
+@pytest.mark.parametrize("nparts", [2, 3])
+@pytest.mark.parametrize("kind", ["jittered", "curved"])
+@pytest.mark.parametrize("viscous,precision", [(False, "fp64"), (True, "fp64"), (True, "mixed")])
+def test_parts_rhs_equals_whole_mesh(zjlib, nparts, kind, viscous, precision):
+    bcs = BCS_A if nparts == 2 else BCS_B
+    mesh = mesh_of(kind, bcs)
+    P = 3 if kind == "jittered" else 4
+    prm = make_params(poly_order=P, riemann="Roe", flux_type="HU", compat=False, viscous=viscous, Re=50.0,
+                      Pr=0.72, bcs=bcs, precision=precision, **KW)
+    whole = FRSolver(mesh, prm)
+    parts = PT.PartitionedSolver(mesh, prm, nparts)
+    assert np.array_equal(parts.solution_point_coords(), whole.solution_point_coords())
+    U = M.random_state(mesh.n_elem, (P + 1) ** 2, 71, 1.4, 1.2, 1.0e5, 0.05)
+    assert np.array_equal(parts.rhs(U), whole.rhs(U))
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_parts_steps_equal_whole_mesh(zjlib, precision):
+    mesh = M.tgv_mesh(24, seed=1)
+    prm = make_params(poly_order=3, rho_inf=1.0, p_inf=1.0 / (1.4 * 0.09), Mach=0.3, riemann="Roe",
+                      compat=False, viscous=True, Re=5000.0, Pr=0.72, bcs=[(1, "slipwall")], precision=precision)
+    whole = FRSolver(mesh, prm)
+    parts = PT.PartitionedSolver(mesh, prm, 4)
+    U0 = M.taylor_green(whole.solution_point_coords())
+    whole.copyToDevice(U0)
+    parts.copyToDevice(U0)
+    dt = whole.computeTimeStep()
+    assert parts.computeTimeStep() == dt
+    whole.advance(dt, 7)
+    parts.advance(dt, 7)
+    assert np.array_equal(parts.copyToHost(), whole.copyToHost())
+    nw, npart = whole.computeResidual(), parts.computeResidual()
+    assert abs(nw - npart) <= 1e-13 * nw
+
+
+def test_a_part_refuses_single_handle_stepping(zjlib):
+    mesh = M.tgv_mesh(8, seed=1)
+    prm = make_params(poly_order=2, compat=False, bcs=[(1, "slipwall")], **KW)
+    parts = PT.PartitionedSolver(mesh, prm, 2)
+    assert zjlib.zj_step(parts.parts[0].h, 1e-6, 1) == L.ERR_UNSUPPORTED
+    one = (C.c_void_p * 1)(parts.parts[0].h)
+    assert zjlib.zj_parts_step(one, 1, 1e-6, 1) == L.ERR_ARG       # a 2-part partition needs both parts
+    with pytest.raises(L.ZJError) as e:
+        PT.PartitionedSolver(mesh, make_params(poly_order=2, compat=True, bcs=[(1, "slipwall")], **KW), 2)
+    assert e.value.code == L.ERR_UNSUPPORTED

@@ -108,6 +108,19 @@ def lib():
         "zj_rhs_vjp": (ip, [vp, vp, vp, vp, dp]),
         "zj_step_vjp": (ip, [vp, vp, C.c_double, vp, vp, dp]),
         "zj_adjoint_run": (ip, [vp, C.c_double, ip, ip, vp, dp, C.POINTER(C.c_int64), dp, dp]),
+        "zj_partition": (ip, [C.POINTER(MeshDesc), ip, C.POINTER(C.c_int32)]),
+        "zj_halo_plan_size": (ip, [C.POINTER(MeshDesc), C.POINTER(C.c_int32), ip, ip, C.POINTER(ip),
+                                   C.POINTER(C.c_int64), C.POINTER(C.c_int64)]),
+        "zj_halo_plan": (ip, [C.POINTER(MeshDesc), C.POINTER(C.c_int32), ip, ip, C.POINTER(C.c_int32),
+                              C.POINTER(C.c_int64), C.POINTER(C.c_int64), C.POINTER(C.c_int64),
+                              C.POINTER(C.c_int64), C.POINTER(C.c_int64)]),
+        "zj_solver_create_part": (ip, [C.POINTER(MeshDesc), C.POINTER(Params), C.POINTER(C.c_int32), ip, ip,
+                                       C.POINTER(vp)]),
+        "zj_part_elements": (ip, [vp, C.POINTER(C.c_int64)]),
+        "zj_parts_step": (ip, [C.POINTER(vp), ip, C.c_double, ip]),
+        "zj_parts_rhs": (ip, [C.POINTER(vp), ip, C.POINTER(vp), C.POINTER(vp)]),
+        "zj_parts_synchronize": (ip, [C.POINTER(vp), ip]),
+        "zj_parts_residual_norm": (ip, [C.POINTER(vp), ip, dp]),
     }
     for name, (res, args) in sig.items():
         f = getattr(h, name)

@@ -16,7 +16,7 @@ CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libzj_fr.so")
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 
-SOURCES = ["host_setup.cpp", "tri_setup.cpp", "gmsh.cpp", "compat_fp64.cu", "phys_fp64.cu", "phys_fp32.cu", "ns_fp64.cu",
+SOURCES = ["host_setup.cpp", "tri_setup.cpp", "gmsh.cpp", "partition.cpp", "compat_fp64.cu", "phys_fp64.cu", "phys_fp32.cu", "ns_fp64.cu",
            "ns_fp32.cu", "ns_tc.cu", "tri_fp64.cu", "tri_fp32.cu", "jvp.cu", "adjoint.cu", "capi.cu"]
 OBJDIR = os.path.join(HERE, "_build")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]

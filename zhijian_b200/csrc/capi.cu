@@ -123,6 +123,18 @@ struct zj_solver {
     bool has_norm = false;
     cudaStream_t own = nullptr, stream = nullptr;
     int device = 0;             // the device current at zj_solver_create
+    // one part of a partitioned mesh (zj_solver_create_part): the part's
+    // view, its halo rows (sent: its side of each interface; received: the
+    // interfaces' ghost rows) and exchange buffers of n_iface rows of n1*8
+    // values in the handle's arithmetic type
+    bool is_part = false;
+    PartSlice part;
+    int64_t n_ghost = 0;        // ghost rows after the element rows: boundary slots + interfaces
+    int32_t* dSendRows = nullptr;
+    int32_t* dRecvRows = nullptr;
+    void* dSendBuf = nullptr;
+    void* dRecvBuf = nullptr;
+    cudaEvent_t ev_pack = nullptr, ev_done = nullptr;
     double time = 0.0;
     int iter = 0;
     double last_dt = -1.0;
@@ -183,6 +195,12 @@ void free_all(zj_solver* s) {
     if (s->dNrm) cudaFree(s->dNrm);
     s->dFlag = nullptr; s->dEdges = nullptr; s->dNrm = nullptr;
     for (auto& g : s->gexec) { if (g) cudaGraphExecDestroy(g); g = nullptr; }
+    void* hs[] = {s->dSendRows, s->dRecvRows, s->dSendBuf, s->dRecvBuf};
+    for (void* p : hs) if (p) cudaFree(p);
+    s->dSendRows = s->dRecvRows = nullptr; s->dSendBuf = s->dRecvBuf = nullptr;
+    if (s->ev_pack) cudaEventDestroy(s->ev_pack);
+    if (s->ev_done) cudaEventDestroy(s->ev_done);
+    s->ev_pack = s->ev_done = nullptr;
     if (s->own) cudaStreamDestroy(s->own);
     s->own = nullptr;
 }
@@ -457,7 +475,15 @@ const char* zj_last_error(const zj_solver* s) {
     return s ? s->err.c_str() : g_create_err.c_str();
 }
 
-zj_status zj_solver_create(const zj_mesh_desc* mesh, const zj_params* params, zj_solver** out) {
+}  // extern "C"
+
+namespace {
+
+// The one creation path: the whole mesh (part == NULL), or part `rank` of a
+// partition (the global per-element arrays are built, then restricted to the
+// part's elements, with the cut faces as interface ghost rows).
+zj_status create_impl(const zj_mesh_desc* mesh, const zj_params* params, const int32_t* part, int nparts,
+                      int rank, zj_solver** out) {
     if (!out) return fail(nullptr, ZJ_ERR_ARG, "out is NULL");
     *out = nullptr;
     if (!mesh || !params) return fail(nullptr, ZJ_ERR_ARG, "mesh or params is NULL");
@@ -472,6 +498,18 @@ zj_status zj_solver_create(const zj_mesh_desc* mesh, const zj_params* params, zj
     s->nsp = s->n1 * s->n1;
     if (!build_mesh(mesh, params, s->mesh, msg)) { delete s; return fail(nullptr, ZJ_ERR_ARG, msg); }
     s->E = s->mesh.n_elem;
+    if (part) {
+        if (params->compat) {
+            delete s;
+            return fail(nullptr, ZJ_ERR_UNSUPPORTED, "partitioned meshes run in physics mode (compat off)");
+        }
+        if (s->mesh.n_tri > 0) {
+            delete s;
+            return fail(nullptr, ZJ_ERR_UNSUPPORTED, "partitioned meshes are quadrilateral meshes");
+        }
+        if (!make_part_slice(s->mesh, part, nparts, rank, s->part, msg)) { delete s; return fail(nullptr, ZJ_ERR_ARG, msg); }
+        s->is_part = true;
+    }
     if (s->E > (1LL << 31) / (4LL * s->nsp)) { delete s; return fail(nullptr, ZJ_ERR_ARG, "mesh too large"); }
     if (params->compat) build_operators_compat(s->P, s->ops);
     else build_operators_vcjh(s->P, params->flux_type, s->ops);
@@ -510,12 +548,32 @@ zj_status zj_solver_create(const zj_mesh_desc* mesh, const zj_params* params, zj
     element_areas(s->mesh, area);
     for (auto& a : area) a = std::sqrt(a);
     pack_ops(s->ops, packed);
+    s->n_ghost = s->mesh.n_bnd_faces;
+    if (s->is_part) {
+        // this part's rows of every per-element array
+        const PartSlice& ps = s->part;
+        J = slice_rows(ps, J, (size_t)s->nsp);
+        Jinv = slice_rows(ps, Jinv, (size_t)s->nsp * 4);
+        nrm = slice_rows(ps, nrm, (size_t)(s->nrm_pp ? 4 * s->n1 * 4 : 4 * 4));
+        area = slice_rows(ps, area, 1);
+        std::vector<EdgeRec> lrec;
+        slice_edge_records(ps, rec, lrec);
+        rec.swap(lrec);
+        bc = slice_bc_data(ps, bc);
+        std::vector<int8_t> et;
+        for (int64_t g : ps.elems) et.push_back(s->etype[(size_t)g]);
+        s->etype.swap(et);
+        s->E = (int64_t)ps.elems.size();
+        s->n_quad = s->E;
+        s->n_ghost = (int64_t)(ps.bnd_slots.size() + ps.mine.size());
+    }
 
     s->n_jinv = Jinv.size(); s->n_j = J.size(); s->n_ops = packed.size();
     s->n_bcd = bc.size(); s->n_nrm = nrm.size() / 4;
     s->state_n = (size_t)s->E * s->nsp * 4;
-    // element traces, then one ghost row per boundary slot (physics mode)
-    s->trace_n = ((size_t)s->E * 4 + (size_t)s->mesh.n_bnd_faces) * s->n1 * 4;
+    // element traces, then one ghost row per boundary slot and, for a part,
+    // per interface (physics mode)
+    s->trace_n = ((size_t)s->E * 4 + (size_t)s->n_ghost) * s->n1 * 4;
     s->grid = stage_grid(s->P, s->E);
     std::vector<int32_t> listq, listt;
     if (s->n_tri > 0) {
@@ -610,6 +668,31 @@ zj_status zj_solver_create(const zj_mesh_desc* mesh, const zj_params* params, zj
             e = cudaMemcpy(s->fTriOps, f.data(), f.size() * 4, cudaMemcpyHostToDevice);
         }
     }
+    if (s->is_part && e == cudaSuccess) {
+        // halo rows: this part's side of every interface (sent), and the
+        // interfaces' ghost rows E*4 + n_bnd + k (received), in the plan's
+        // order (neighbours ascending, global face order within each)
+        const PartSlice& ps = s->part;
+        const size_t ni = ps.mine.size();
+        std::vector<int32_t> send(ni), recv(ni);
+        const int64_t nb = (int64_t)ps.bnd_slots.size();
+        for (size_t k = 0; k < ni; ++k) {
+            send[k] = (int32_t)(ps.g2l[(size_t)(ps.mine[k] / 4)] * 4 + ps.mine[k] % 4);
+            recv[k] = (int32_t)(s->E * 4 + nb + (int64_t)k);
+        }
+        const size_t tsz = s->mixed ? sizeof(float) : sizeof(double);
+        e = dalloc(&s->dSendRows, ni);
+        if (e == cudaSuccess) e = dalloc(&s->dRecvRows, ni);
+        if (e == cudaSuccess) e = cudaMalloc(&s->dSendBuf, std::max<size_t>(ni, 1) * s->n1 * 8 * tsz);
+        if (e == cudaSuccess) e = cudaMalloc(&s->dRecvBuf, std::max<size_t>(ni, 1) * s->n1 * 8 * tsz);
+        if (e == cudaSuccess && ni)
+            e = cudaMemcpy(s->dSendRows, send.data(), ni * 4, cudaMemcpyHostToDevice);
+        if (e == cudaSuccess && ni)
+            e = cudaMemcpy(s->dRecvRows, recv.data(), ni * 4, cudaMemcpyHostToDevice);
+        if (e == cudaSuccess) e = cudaEventCreateWithFlags(&s->ev_pack, cudaEventDisableTiming);
+        if (e == cudaSuccess) e = cudaEventCreateWithFlags(&s->ev_done, cudaEventDisableTiming);
+        s->graphs_on = false;   // parts step through the multi-part driver
+    }
     // every state buffer starts at zero: slots no kernel writes (a
     // triangle's unused ones) stay finite through the buffer rotation
     for (int i = 0; i < 3 && e == cudaSuccess; ++i) e = cudaMemset(s->dU[i], 0, s->state_n * 8);
@@ -624,6 +707,14 @@ zj_status zj_solver_create(const zj_mesh_desc* mesh, const zj_params* params, zj
     s->stream = s->own;
     *out = s;
     return ZJ_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+zj_status zj_solver_create(const zj_mesh_desc* mesh, const zj_params* params, zj_solver** out) {
+    return create_impl(mesh, params, nullptr, 1, 0, out);
 }
 
 void zj_solver_destroy(zj_solver* s) {
@@ -647,6 +738,7 @@ zj_status zj_solution_point_coords(const zj_solver* s, double* xy) {
     std::string msg;
     if (s->n_tri > 0 && !build_operators_tri(s->P, s->prm.flux_type, tri, msg)) return fail(const_cast<zj_solver*>(s), ZJ_ERR_ARG, msg);
     sp_coords(s->mesh, s->ops, c, s->n_tri ? &tri : nullptr);
+    if (s->is_part) c = slice_rows(s->part, c, (size_t)s->nsp * 2);
     std::memcpy(xy, c.data(), c.size() * sizeof(double));
     return ZJ_OK;
 }
@@ -723,8 +815,14 @@ zj_status zj_get_state_device(zj_solver* s, double* U) {
     return ZJ_OK;
 }
 
+// A part's interfaces are filled by the multi-part driver (zj_parts_*).
+static zj_status refuse_part(zj_solver* s) {
+    return fail(s, ZJ_ERR_UNSUPPORTED, "a part of a partitioned mesh steps and evaluates through zj_parts_step / zj_parts_rhs");
+}
+
 zj_status zj_step(zj_solver* s, double dt, int nsteps) {
     if (!s) return ZJ_ERR_ARG;
+    if (s->is_part) return refuse_part(s);
     if (nsteps < 0 || !std::isfinite(dt)) return fail(s, ZJ_ERR_ARG, "bad dt or nsteps");
     if (nsteps == 0) return ZJ_OK;
     cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
@@ -754,6 +852,7 @@ zj_status zj_synchronize(zj_solver* s) {
 
 zj_status zj_rhs(zj_solver* s, const double* U_dev, double* R_dev) {
     if (!s || !U_dev || !R_dev) return ZJ_ERR_ARG;
+    if (s->is_part) return refuse_part(s);
     if ((reinterpret_cast<uintptr_t>(U_dev) | reinterpret_cast<uintptr_t>(R_dev)) & 15u)
         return fail(s, ZJ_ERR_ARG, "U_dev and R_dev must be 16-byte aligned");
     if (s->mixed) return rhs_impl<float>(s, U_dev, R_dev, s->fT[2], nullptr, s->dPartR);
@@ -857,6 +956,7 @@ extern "C" {
 
 zj_status zj_rhs_noalloc(zj_solver* s, const double* U_dev, double* R_dev) {
     if (!s || !U_dev || !R_dev) return ZJ_ERR_ARG;
+    if (s->is_part) return refuse_part(s);
     if ((reinterpret_cast<uintptr_t>(U_dev) | reinterpret_cast<uintptr_t>(R_dev)) & 15u)
         return fail(s, ZJ_ERR_ARG, "U_dev and R_dev must be 16-byte aligned");
     int dev = -1;
@@ -904,6 +1004,7 @@ zj_status diff_supported(zj_solver* s) {
     if (s->mixed) return fail(s, ZJ_ERR_UNSUPPORTED, "differentiation runs on the FP64 path (precision fp64)");
     if (s->n_tri > 0) return fail(s, ZJ_ERR_UNSUPPORTED, "differentiation runs on quadrilateral meshes");
     if (s->nrm_pp) return fail(s, ZJ_ERR_UNSUPPORTED, "differentiation runs on straight-edged (Q1) meshes");
+    if (s->is_part) return fail(s, ZJ_ERR_UNSUPPORTED, "differentiation runs on a whole mesh, not a part");
     return ZJ_OK;
 }
 
@@ -1418,6 +1519,354 @@ zj_status zj_solver_create_from_gmsh(const char* msh_path, const zj_params* para
     st = zj_solver_create(&m->desc, &p, out);
     zj_gmsh_free(m);
     return st;
+}
+
+}  // extern "C"
+
+// ------------------------------------------------------- mesh partitions --
+// A partitioned mesh runs as one handle per part (zj_solver_create_part);
+// the parts couple only through the traces and gradient traces at the faces
+// their partition cuts.  Each part's interface faces read the other side's
+// trace rows from ghost rows, which an exchange fills after every launch that
+// writes traces: the sender gathers its side's rows into a send buffer in the
+// plan's order (neighbours ascending, global face order within each), the
+// receiver copies the matching slice of it into its own memory (a peer copy
+// across devices, an ordinary copy on one device) and scatters it into its
+// ghost rows.  zj_parts_* drive all parts of a partition from one process,
+// the parts' streams ordered by events.
+namespace {
+
+template <typename T>
+__global__ void k_rows_gather(const T* __restrict__ src, const int32_t* __restrict__ rows, long long n, int w,
+                              T* __restrict__ dst) {
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n * w) return;
+    const long long k = i / w, j = i - k * w;
+    dst[i] = src[(long long)rows[k] * w + j];
+}
+
+template <typename T>
+__global__ void k_rows_scatter(const T* __restrict__ src, const int32_t* __restrict__ rows, long long n, int w,
+                               T* __restrict__ dst) {
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n * w) return;
+    const long long k = i / w, j = i - k * w;
+    dst[(long long)rows[k] * w + j] = src[i];
+}
+
+struct DeviceGuard {
+    int prev = -1;
+    DeviceGuard() { cudaGetDevice(&prev); }
+    ~DeviceGuard() { if (prev >= 0) cudaSetDevice(prev); }
+};
+
+// The parts of one partition, indexed by rank, checked for consistency.
+zj_status parts_check(zj_solver* const* parts, int n, std::vector<zj_solver*>& by_rank) {
+    if (!parts || n < 1) return fail(nullptr, ZJ_ERR_ARG, "parts is NULL or empty");
+    by_rank.assign((size_t)n, nullptr);
+    for (int i = 0; i < n; ++i) {
+        zj_solver* s = parts[i];
+        if (!s) return fail(nullptr, ZJ_ERR_ARG, "a part handle is NULL");
+        if (!s->is_part || s->part.nparts != n)
+            return fail(s, ZJ_ERR_ARG, "every handle must be a part of the same n-part partition");
+        if (by_rank[(size_t)s->part.rank]) return fail(s, ZJ_ERR_ARG, "two handles hold the same part");
+        if (s->mixed != parts[0]->mixed || s->P != parts[0]->P || s->tc != parts[0]->tc)
+            return fail(s, ZJ_ERR_ARG, "the parts differ in order or precision");
+        by_rank[(size_t)s->part.rank] = s;
+    }
+    return ZJ_OK;
+}
+
+// Rows of width w of every part's buffer bufs[rank] (trace rows: n1*4 values,
+// gradient trace rows: n1*8) across the cuts.
+template <typename T>
+zj_status parts_exchange(const std::vector<zj_solver*>& P, const std::vector<T*>& bufs, int w) {
+    const int threads = 256;
+    for (zj_solver* s : P) {
+        const long long ni = (long long)s->part.mine.size();
+        ZJ_CK(s, cudaSetDevice(s->device), "set device");
+        if (ni > 0) {
+            k_rows_gather<T><<<(unsigned)((ni * w + threads - 1) / threads), threads, 0, s->stream>>>(
+                bufs[(size_t)s->part.rank], s->dSendRows, ni, w, static_cast<T*>(s->dSendBuf));
+            ZJ_CK(s, cudaGetLastError(), "halo gather");
+        }
+        ZJ_CK(s, cudaEventRecord(s->ev_pack, s->stream), "halo event");
+    }
+    for (zj_solver* q : P) {
+        const PartSlice& pq = q->part;
+        ZJ_CK(q, cudaSetDevice(q->device), "set device");
+        for (size_t i = 0; i < pq.nbr.size(); ++i) {
+            zj_solver* p = P[(size_t)pq.nbr[i]];
+            const PartSlice& pp = p->part;
+            size_t j = 0;
+            while (j < pp.nbr.size() && pp.nbr[j] != pq.rank) ++j;
+            const int64_t cnt = pq.nbr_off[i + 1] - pq.nbr_off[i];
+            if (j == pp.nbr.size() || pp.nbr_off[j + 1] - pp.nbr_off[j] != cnt)
+                return fail(q, ZJ_ERR_ARG, "the parts' halo plans do not match");
+            ZJ_CK(q, cudaStreamWaitEvent(q->stream, p->ev_pack, 0), "halo wait");
+            const size_t bytes = (size_t)cnt * w * sizeof(T);
+            const T* src = static_cast<const T*>(p->dSendBuf) + (size_t)pp.nbr_off[j] * w;
+            T* dst = static_cast<T*>(q->dRecvBuf) + (size_t)pq.nbr_off[i] * w;
+            if (p->device == q->device) {
+                ZJ_CK(q, cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToDevice, q->stream), "halo copy");
+            } else {
+                ZJ_CK(q, cudaMemcpyPeerAsync(dst, q->device, src, p->device, bytes, q->stream), "halo peer copy");
+            }
+        }
+        const long long ni = (long long)pq.mine.size();
+        if (ni > 0) {
+            k_rows_scatter<T><<<(unsigned)((ni * w + threads - 1) / threads), threads, 0, q->stream>>>(
+                static_cast<const T*>(q->dRecvBuf), q->dRecvRows, ni, w, bufs[(size_t)pq.rank]);
+            ZJ_CK(q, cudaGetLastError(), "halo scatter");
+        }
+        ZJ_CK(q, cudaEventRecord(q->ev_done, q->stream), "halo event");
+    }
+    // a part's send buffer is reused by its next exchange once its
+    // neighbours have copied it
+    for (zj_solver* p : P) {
+        ZJ_CK(p, cudaSetDevice(p->device), "set device");
+        for (int32_t r : p->part.nbr) ZJ_CK(p, cudaStreamWaitEvent(p->stream, P[(size_t)r]->ev_done, 0), "halo wait");
+    }
+    return ZJ_OK;
+}
+
+template <typename T>
+T* grad_buf(const zj_solver* s);
+template <> double* grad_buf<double>(const zj_solver* s) { return s->dTQ; }
+template <> float* grad_buf<float>(const zj_solver* s) { return s->fTQ; }
+
+// One residual (stage 0) or SSP-RK3 stage of every part: for Navier-Stokes
+// the gradient launches, their gradient traces across the cuts, then the
+// stage launches; a stage's new traces cross after it.
+template <typename T>
+zj_status parts_stage(const std::vector<zj_solver*>& P, const std::vector<StageArgsT<T>>& A) {
+    const bool ns = is_ns(P[0]);
+    if (ns) {
+        std::vector<T*> tq;
+        for (size_t i = 0; i < P.size(); ++i) {
+            ZJ_CK(P[i], cudaSetDevice(P[i]->device), "set device");
+            ZJ_CK(P[i], launch_ns_grad(P[i]->P, A[i], P[i]->stream), "gradient launch");
+            tq.push_back(grad_buf<T>(P[i]));
+        }
+        zj_status st = parts_exchange<T>(P, tq, P[0]->n1 * 8);
+        if (st != ZJ_OK) return st;
+    }
+    std::vector<T*> out;
+    for (size_t i = 0; i < P.size(); ++i) {
+        zj_solver* s = P[i];
+        ZJ_CK(s, cudaSetDevice(s->device), "set device");
+        cudaError_t e;
+        if (!ns) {
+            e = launch_phys_stage(s->P, s->prm.riemann, A[i], s->stream);
+        } else if constexpr (sizeof(T) == 4) {
+            if (s->tc) {
+                StageArgsT<T> t = A[i];
+                t.tc_err = s->dTcErr;
+                e = launch_ns_stage_tc(s->P, s->prm.riemann, t, &s->tc_map, s->stream);
+            } else {
+                e = launch_ns_stage(s->P, s->prm.riemann, A[i], s->stream);
+            }
+        } else {
+            e = launch_ns_stage(s->P, s->prm.riemann, A[i], s->stream);
+        }
+        ZJ_CK(s, e, "stage launch");
+        out.push_back(const_cast<T*>(A[i].Tout));
+    }
+    if (A[0].stage == 0) return ZJ_OK;
+    return parts_exchange<T>(P, out, P[0]->n1 * 4);
+}
+
+template <typename T>
+zj_status parts_traces(const std::vector<zj_solver*>& P, const std::vector<const double*>& U, const std::vector<T*>& Tb) {
+    for (size_t i = 0; i < P.size(); ++i) {
+        ZJ_CK(P[i], cudaSetDevice(P[i]->device), "set device");
+        ZJ_CK(P[i], launch_trace_any(P[i], U[i], Tb[i]), "trace launch");
+    }
+    return parts_exchange<T>(P, Tb, P[0]->n1 * 4);
+}
+
+template <typename T>
+zj_status parts_step_t(const std::vector<zj_solver*>& P, double dt, int nsteps) {
+    const size_t n = P.size();
+    std::vector<const double*> U(n);
+    std::vector<T*> Tb(n);
+    if (!P[0]->traces_valid) {
+        for (size_t i = 0; i < n; ++i) { U[i] = P[i]->dU[P[i]->cur]; Tb[i] = tbuf<T>(P[i], P[i]->tpar); }
+        zj_status st = parts_traces<T>(P, U, Tb);
+        if (st != ZJ_OK) return st;
+        for (zj_solver* s : P) s->traces_valid = true;
+    }
+    std::vector<StageArgsT<T>> A(n);
+    for (int step = 0; step < nsteps; ++step) {
+        for (int stage = 1; stage <= 3; ++stage) {
+            for (size_t i = 0; i < n; ++i) {
+                zj_solver* s = P[i];
+                const int c = s->cur, a1 = (c + 1) % 3, b1 = (c + 2) % 3, p = s->tpar;
+                StageArgsT<T> a = stage_args<T>(s);
+                a.partials = s->dPart;
+                a.U0 = s->dU[c];
+                a.stage = stage;
+                if (stage == 1) { a.U = s->dU[c]; a.Uout = s->dU[a1]; a.Tin = tbuf<T>(s, p); a.Tout = tbuf<T>(s, 1 - p); }
+                if (stage == 2) { a.U = s->dU[a1]; a.Uout = s->dU[b1]; a.Tin = tbuf<T>(s, 1 - p); a.Tout = tbuf<T>(s, p); }
+                if (stage == 3) { a.U = s->dU[b1]; a.Uout = s->dU[a1]; a.Tin = tbuf<T>(s, p); a.Tout = tbuf<T>(s, 1 - p); }
+                A[i] = a;
+            }
+            zj_status st = parts_stage<T>(P, A);
+            if (st != ZJ_OK) return st;
+        }
+        for (zj_solver* s : P) {
+            s->cur = (s->cur + 1) % 3;
+            s->tpar = 1 - s->tpar;
+            s->time += dt;
+            s->iter += 1;
+        }
+    }
+    for (zj_solver* s : P) s->has_norm = true;
+    return ZJ_OK;
+}
+
+template <typename T>
+zj_status parts_rhs_t(const std::vector<zj_solver*>& P, const double* const* Ud, double* const* Rd) {
+    const size_t n = P.size();
+    std::vector<const double*> U(n);
+    std::vector<T*> Tb(n);
+    for (size_t i = 0; i < n; ++i) {
+        const size_t r = (size_t)P[i]->part.rank;
+        U[i] = Ud[r];
+        Tb[i] = tbuf<T>(P[i], 2);
+    }
+    zj_status st = parts_traces<T>(P, U, Tb);
+    if (st != ZJ_OK) return st;
+    std::vector<StageArgsT<T>> A(n);
+    for (size_t i = 0; i < n; ++i) {
+        StageArgsT<T> a = stage_args<T>(P[i]);
+        a.U = U[i]; a.U0 = U[i]; a.Uout = nullptr; a.Tin = Tb[i]; a.Tout = nullptr;
+        a.R = Rd[(size_t)P[i]->part.rank]; a.partials = P[i]->dPartR; a.stage = 0;
+        A[i] = a;
+    }
+    return parts_stage<T>(P, A);
+}
+
+}  // namespace
+
+extern "C" {
+
+zj_status zj_partition(const zj_mesh_desc* mesh, int nparts, int32_t* part) {
+    if (!mesh || !part || nparts < 1) return fail(nullptr, ZJ_ERR_ARG, "mesh or part is NULL, or nparts < 1");
+    HostMesh m;
+    std::string msg;
+    if (!build_mesh(mesh, nullptr, m, msg)) return fail(nullptr, ZJ_ERR_ARG, msg);
+    if (m.n_elem < nparts) return fail(nullptr, ZJ_ERR_ARG, "fewer elements than parts");
+    std::vector<int32_t> p;
+    partition_rcb(m, nparts, p);
+    std::memcpy(part, p.data(), p.size() * sizeof(int32_t));
+    return ZJ_OK;
+}
+
+zj_status zj_halo_plan_size(const zj_mesh_desc* mesh, const int32_t* part, int nparts, int rank, int* n_nbr,
+                            int64_t* n_iface, int64_t* n_elem) {
+    if (!mesh || !part || !n_nbr || !n_iface) return fail(nullptr, ZJ_ERR_ARG, "NULL argument");
+    HostMesh m;
+    PartSlice ps;
+    std::string msg;
+    if (!build_mesh(mesh, nullptr, m, msg) || !make_part_slice(m, part, nparts, rank, ps, msg))
+        return fail(nullptr, ZJ_ERR_ARG, msg);
+    *n_nbr = (int)ps.nbr.size();
+    *n_iface = (int64_t)ps.mine.size();
+    if (n_elem) *n_elem = (int64_t)ps.elems.size();
+    return ZJ_OK;
+}
+
+zj_status zj_halo_plan(const zj_mesh_desc* mesh, const int32_t* part, int nparts, int rank, int32_t* nbr,
+                       int64_t* nbr_off, int64_t* face, int64_t* mine, int64_t* remote, int64_t* elems) {
+    if (!mesh || !part || !nbr || !nbr_off || !face || !mine || !remote) return fail(nullptr, ZJ_ERR_ARG, "NULL argument");
+    HostMesh m;
+    PartSlice ps;
+    std::string msg;
+    if (!build_mesh(mesh, nullptr, m, msg) || !make_part_slice(m, part, nparts, rank, ps, msg))
+        return fail(nullptr, ZJ_ERR_ARG, msg);
+    std::copy(ps.nbr.begin(), ps.nbr.end(), nbr);
+    std::copy(ps.nbr_off.begin(), ps.nbr_off.end(), nbr_off);
+    std::copy(ps.face.begin(), ps.face.end(), face);
+    std::copy(ps.mine.begin(), ps.mine.end(), mine);
+    std::copy(ps.remote.begin(), ps.remote.end(), remote);
+    if (elems) std::copy(ps.elems.begin(), ps.elems.end(), elems);
+    return ZJ_OK;
+}
+
+zj_status zj_solver_create_part(const zj_mesh_desc* mesh, const zj_params* params, const int32_t* part,
+                                int nparts, int rank, zj_solver** out) {
+    if (!part) return fail(nullptr, ZJ_ERR_ARG, "part is NULL");
+    return create_impl(mesh, params, part, nparts, rank, out);
+}
+
+zj_status zj_part_elements(const zj_solver* s, int64_t* global_ids) {
+    if (!s || !global_ids) return ZJ_ERR_ARG;
+    if (!s->is_part) {
+        for (int64_t e = 0; e < s->E; ++e) global_ids[e] = e;
+        return ZJ_OK;
+    }
+    std::copy(s->part.elems.begin(), s->part.elems.end(), global_ids);
+    return ZJ_OK;
+}
+
+zj_status zj_parts_step(zj_solver* const* parts, int n, double dt, int nsteps) {
+    std::vector<zj_solver*> P;
+    zj_status st = parts_check(parts, n, P);
+    if (st != ZJ_OK) return st;
+    if (nsteps < 0 || !std::isfinite(dt)) return fail(P[0], ZJ_ERR_ARG, "bad dt or nsteps");
+    if (nsteps == 0) return ZJ_OK;
+    DeviceGuard guard;
+    for (zj_solver* s : P) {
+        ZJ_CK(s, cudaSetDevice(s->device), "set device");
+        if (dt != s->last_dt) {
+            k_set_dt<<<1, 1, 0, s->stream>>>(s->dScal, dt);
+            ZJ_CK(s, cudaGetLastError(), "dt launch");
+            s->last_dt = dt;
+        }
+    }
+    return P[0]->mixed ? parts_step_t<float>(P, dt, nsteps) : parts_step_t<double>(P, dt, nsteps);
+}
+
+zj_status zj_parts_rhs(zj_solver* const* parts, int n, const double* const* U_dev, double* const* R_dev) {
+    std::vector<zj_solver*> P;
+    zj_status st = parts_check(parts, n, P);
+    if (st != ZJ_OK) return st;
+    if (!U_dev || !R_dev) return fail(P[0], ZJ_ERR_ARG, "U_dev or R_dev is NULL");
+    DeviceGuard guard;
+    return P[0]->mixed ? parts_rhs_t<float>(P, U_dev, R_dev) : parts_rhs_t<double>(P, U_dev, R_dev);
+}
+
+zj_status zj_parts_synchronize(zj_solver* const* parts, int n) {
+    std::vector<zj_solver*> P;
+    zj_status st = parts_check(parts, n, P);
+    if (st != ZJ_OK) return st;
+    DeviceGuard guard;
+    for (zj_solver* s : P) {
+        ZJ_CK(s, cudaSetDevice(s->device), "set device");
+        ZJ_CK(s, cudaStreamSynchronize(s->stream), "synchronize");
+    }
+    return ZJ_OK;
+}
+
+zj_status zj_parts_residual_norm(zj_solver* const* parts, int n, double* out) {
+    std::vector<zj_solver*> P;
+    zj_status st = parts_check(parts, n, P);
+    if (st != ZJ_OK) return st;
+    if (!out) return fail(P[0], ZJ_ERR_ARG, "out is NULL");
+    DeviceGuard guard;
+    double sum = 0.0;
+    for (zj_solver* s : P) {
+        ZJ_CK(s, cudaSetDevice(s->device), "set device");
+        if (!s->has_norm) continue;
+        ZJ_CK(s, launch_reduce_sum(s->dPart, s->grid, s->dScal + 1, s->stream), "norm reduce");
+        double v = 0.0;
+        ZJ_CK(s, cudaMemcpyAsync(&v, s->dScal + 1, sizeof(double), cudaMemcpyDeviceToHost, s->stream), "norm copy");
+        ZJ_CK(s, cudaStreamSynchronize(s->stream), "norm sync");
+        sum += v;
+    }
+    *out = std::sqrt(sum);
+    return ZJ_OK;
 }
 
 }  // extern "C"

@@ -153,8 +153,8 @@ k_ns_stage_tc(const StageArgsT<float> a, const __grid_constant__ CUtensorMap ama
         load4_nc(qt + 4, Qo + 4);
 #pragma unroll
         for (int v = 0; v < 8; ++v) Qn[v] = Qo[v];
-        if (!(f.r.flags & (kEdgeOrphan | kEdgeBoundary))) {
-            const float* qn = a.TQ + (((long long)f.r.nbr * 4 + f.r.nbr_edge) * N1 + (N1 - 1 - fp)) * 8;
+        if (has_neighbour_gradient(f.r)) {
+            const float* qn = a.TQ + (neighbour_row(f.r, a.n_elem) * N1 + (N1 - 1 - fp)) * 8;
             load4_nc(qn, Qn);
             load4_nc(qn + 4, Qn + 4);
         }
@@ -353,7 +353,7 @@ k_ns_stage_tc(const StageArgsT<float> a, const __grid_constant__ CUtensorMap ama
 #pragma unroll
         for (int v = 0; v < 4; ++v) t[v] += ue[v];
         store4(a.Tout + (e * NFT + k) * 4, t);
-        if (f.r.flags & kEdgeBoundary) store_ghost<N1>(a, f.r, f.nx, f.ny, fp, t);
+        if (boundary_condition_edge(f.r)) store_ghost<N1>(a, f.r, f.nx, f.ny, fp, t);
     }
 
     // ---- teardown: every copy and product has completed (or the waits gave

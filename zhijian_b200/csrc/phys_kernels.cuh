@@ -93,6 +93,17 @@ __device__ __forceinline__ long long neighbour_row(const EdgeRec& r, long long n
     return (r.flags & kEdgeBoundary) ? n_elem * 4 + r.nbr_edge : (long long)r.nbr * 4 + r.nbr_edge;
 }
 
+// A boundary edge whose ghost row the traces' kernel writes from its
+// boundary condition (a partition's interface rows come from the exchange).
+__device__ __forceinline__ bool boundary_condition_edge(const EdgeRec& r) {
+    return (r.flags & (kEdgeBoundary | kEdgeInterface)) == kEdgeBoundary;
+}
+// An edge whose neighbour's gradient trace is read (interior edges and
+// partition interfaces; a boundary copies the interior gradient).
+__device__ __forceinline__ bool has_neighbour_gradient(const EdgeRec& r) {
+    return !(r.flags & kEdgeOrphan) && (!(r.flags & kEdgeBoundary) || (r.flags & kEdgeInterface));
+}
+
 template <int N1, typename T>
 __device__ __forceinline__ void store_ghost(const StageArgsT<T>& a, const EdgeRec& r, T nx, T ny,
                                             int fp, const T* t) {
@@ -407,7 +418,7 @@ k_phys_stage(const StageArgsT<T> a) {
             for (int v = 0; v < 4; ++v) t[v] += ue[v];
         }
         store4(a.Tout + (e * NFT + k) * 4, t);
-        if (r.flags & kEdgeBoundary) store_ghost<N1>(a, r, nr[0], nr[1], fp, t);
+        if (boundary_condition_edge(r)) store_ghost<N1>(a, r, nr[0], nr[1], fp, t);
     }
 }
 
@@ -449,7 +460,7 @@ k_phys_traces(const StageArgsT<T> a) {
         }
         store4(a.Tout + (e * NFT + k) * 4, t);
         const EdgeRec r = a.edges[e * 4 + edge];
-        if (r.flags & kEdgeBoundary) {
+        if (boundary_condition_edge(r)) {
             T n[3];
             load_normal(normal_rec<N1>(a, e, edge, fp), n);
             store_ghost<N1>(a, r, n[0], n[1], fp, t);

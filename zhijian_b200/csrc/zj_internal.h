@@ -31,6 +31,10 @@ struct EdgeRec {
 constexpr int32_t kEdgeRight = 1;    // this element is the face's right side
 constexpr int32_t kEdgeBoundary = 2; // boundary face (ghost state)
 constexpr int32_t kEdgeOrphan = 4;   // edge on no face (non-manifold): no correction
+// A face cut by a mesh partition (with kEdgeBoundary: its neighbour's trace
+// and gradient trace sit in a ghost row, filled by the halo exchange instead
+// of a boundary condition; kEdgeRight as on an interior face).
+constexpr int32_t kEdgeInterface = 8;
 ZJ_HD inline int32_t edge_bc_type(int32_t flags) { return (flags >> 8) & 0xF; }
 
 // 1D operators of one polynomial order.  The 2D tensor-product operators of
@@ -104,6 +108,41 @@ void build_edge_records(const HostMesh& m, std::vector<EdgeRec>& rec, std::vecto
 // Curved meshes in physics mode: the face normal and edge Jacobian at every
 // flux point, [E][4][n1][4] = (nx, ny, 2 |dx/dt|, 0).
 void build_point_normals(const HostMesh& m, const Operators1D& ops, std::vector<double>& nrm);
+
+// Mesh partitions (partition.cpp).  Recursive coordinate bisection of the
+// element centroids into nparts balanced parts (deterministic).
+void partition_rcb(const HostMesh& m, int nparts, std::vector<int32_t>& part);
+// One part of a partitioned mesh: its elements (ascending global ids), its
+// boundary slots, and its interface faces grouped by neighbouring part
+// (ascending) and, within a group, in the global face order -- the order
+// both sides of a cut agree on.  Interface k's ghost row is local boundary
+// slot n_bnd + k.
+struct PartSlice {
+    int rank = 0, nparts = 1;
+    std::vector<int64_t> elems;          // local -> global element
+    std::vector<int64_t> g2l;            // global -> local element, -1 elsewhere
+    std::vector<int32_t> bnd_slots;      // local boundary slot -> global slot
+    std::vector<int32_t> nbr;            // neighbouring parts
+    std::vector<int64_t> nbr_off;        // interfaces of nbr[i]: [nbr_off[i], nbr_off[i+1])
+    std::vector<int64_t> face;           // global face id of interface k
+    std::vector<int64_t> mine;           // global element*4 + edge of this part's side
+    std::vector<int64_t> remote;         // global element*4 + edge of the other side
+};
+bool make_part_slice(const HostMesh& m, const int32_t* part, int nparts, int rank, PartSlice& ps,
+                     std::string& msg);
+// The global per-element arrays restricted to the part: edge records with
+// local neighbours, local boundary slots and interface ghost slots; rows of
+// width w of any [E][...] array; boundary data of the local slots followed by
+// zero rows for the interfaces.
+void slice_edge_records(const PartSlice& ps, const std::vector<EdgeRec>& rec, std::vector<EdgeRec>& out);
+template <class T>
+std::vector<T> slice_rows(const PartSlice& ps, const std::vector<T>& a, size_t w) {
+    std::vector<T> out(ps.elems.size() * w);
+    for (size_t l = 0; l < ps.elems.size(); ++l)
+        for (size_t k = 0; k < w; ++k) out[l * w + k] = a[(size_t)ps.elems[l] * w + k];
+    return out;
+}
+std::vector<double> slice_bc_data(const PartSlice& ps, const std::vector<double>& bc);
 
 // Gmsh reader (gmsh.cpp).
 struct GmshGroup {

@@ -329,10 +329,11 @@ __device__ __forceinline__ void wall_viscous_closure(int bc_type, bool adiabatic
     }
 }
 
-// The closure of boundary face r (no-op elsewhere); bc is the face data table.
+// The closure of boundary face r (no-op elsewhere, partition interfaces
+// included); bc is the face data table.
 template <typename T, typename B>
 __device__ __forceinline__ void boundary_viscous_closure(const EdgeRec& r, const B* bc, T nx, T ny, T* Fvn) {
-    if (!(r.flags & kEdgeBoundary)) return;
+    if ((r.flags & (kEdgeBoundary | kEdgeInterface)) != kEdgeBoundary) return;
     const int bt = edge_bc_type(r.flags);
     const bool adiabatic = bt == ZJ_BC_WALL && !(bc[(long long)r.nbr_edge * 8] > B(0));
     wall_viscous_closure(bt, adiabatic, nx, ny, Fvn);

@@ -62,39 +62,53 @@ def _dptr(a: np.ndarray):
     return a.ctypes.data_as(C.POINTER(C.c_double))
 
 
+def mesh_desc(mesh):
+    """The zj_mesh_desc of a QuadMesh or MixedMesh, with the arrays it points
+    into (keep them alive while the descriptor is used)."""
+    xy = np.ascontiguousarray(mesh.xy, dtype=np.float64)
+    if hasattr(mesh, "offsets"):          # MixedMesh: quads and triangles
+        conn = np.ascontiguousarray(mesh.conn, dtype=np.int64)
+        et = np.ascontiguousarray(mesh.etype, dtype=np.int32)
+        ne = et.shape[0]
+        eo = np.ones(ne, dtype=np.int32)
+        off = np.ascontiguousarray(mesh.offsets, dtype=np.int64)
+    else:
+        conn = np.ascontiguousarray(mesh.conn, dtype=np.int64)
+        ne, nn = conn.shape
+        et = np.ones(ne, dtype=np.int32)
+        eo = np.full(ne, {4: 1, 9: 2, 25: 4}[nn], dtype=np.int32)
+        off = (np.arange(ne + 1, dtype=np.int64) * nn)
+    bnd = np.ascontiguousarray(mesh.bnd, dtype=np.int64)
+    d = L.MeshDesc()
+    d.n_nodes = xy.shape[0]
+    d.xy = _dptr(xy)
+    d.n_elem = ne
+    d.elem_type = et.ctypes.data_as(C.POINTER(C.c_int32))
+    d.elem_order = eo.ctypes.data_as(C.POINTER(C.c_int32))
+    d.conn_offsets = off.ctypes.data_as(C.POINTER(C.c_int64))
+    d.conn = conn.ctypes.data_as(C.POINTER(C.c_int64))
+    d.n_bnd_edges = bnd.shape[0]
+    d.bnd_edges = bnd.ctypes.data_as(C.POINTER(C.c_int64))
+    return d, [xy, conn, et, eo, off, bnd]
+
+
 class FRSolver:
     """One zj_solver handle."""
 
     def __init__(self, mesh: QuadMesh, params: L.Params):
         lib = L.lib()
-        self._keep = []
-        xy = np.ascontiguousarray(mesh.xy, dtype=np.float64)
-        if hasattr(mesh, "offsets"):          # MixedMesh: quads and triangles
-            conn = np.ascontiguousarray(mesh.conn, dtype=np.int64)
-            et = np.ascontiguousarray(mesh.etype, dtype=np.int32)
-            ne = et.shape[0]
-            eo = np.ones(ne, dtype=np.int32)
-            off = np.ascontiguousarray(mesh.offsets, dtype=np.int64)
-        else:
-            conn = np.ascontiguousarray(mesh.conn, dtype=np.int64)
-            ne, nn = conn.shape
-            et = np.ones(ne, dtype=np.int32)
-            eo = np.full(ne, {4: 1, 9: 2, 25: 4}[nn], dtype=np.int32)
-            off = (np.arange(ne + 1, dtype=np.int64) * nn)
-        bnd = np.ascontiguousarray(mesh.bnd, dtype=np.int64)
-        d = L.MeshDesc()
-        d.n_nodes = xy.shape[0]
-        d.xy = _dptr(xy)
-        d.n_elem = ne
-        d.elem_type = et.ctypes.data_as(C.POINTER(C.c_int32))
-        d.elem_order = eo.ctypes.data_as(C.POINTER(C.c_int32))
-        d.conn_offsets = off.ctypes.data_as(C.POINTER(C.c_int64))
-        d.conn = conn.ctypes.data_as(C.POINTER(C.c_int64))
-        d.n_bnd_edges = bnd.shape[0]
-        d.bnd_edges = bnd.ctypes.data_as(C.POINTER(C.c_int64))
+        d, self._keep = mesh_desc(mesh)
         h = C.c_void_p()
         L.check(lib.zj_solver_create(C.byref(d), C.byref(params), C.byref(h)))
         self._attach(h, params)
+
+    @classmethod
+    def from_handle(cls, h, params: L.Params, keep=()) -> "FRSolver":
+        """Wrap a handle the library created (a part of a partition)."""
+        s = cls.__new__(cls)
+        s._keep = list(keep)
+        s._attach(h, params)
+        return s
 
     @classmethod
     def from_gmsh(cls, path: str, params: L.Params) -> "FRSolver":
