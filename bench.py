@@ -166,11 +166,15 @@ def build_case():
     return mesh
 
 
+def make_params_for(mode="ns"):
+    from zhijian_b200.solver import make_params
+    return make_params(poly_order=P, gamma=GAMMA, rho_inf=1.0, p_inf=1.0 / (GAMMA * MACH * MACH),
+                       Mach=MACH, bcs=[(1, "slipwall")], **MODES[mode])
+
+
 def make_solver(mesh, mode="ns"):
-    from zhijian_b200.solver import FRSolver, make_params
-    prm = make_params(poly_order=P, gamma=GAMMA, rho_inf=1.0, p_inf=1.0 / (GAMMA * MACH * MACH),
-                      Mach=MACH, bcs=[(1, "slipwall")], **MODES[mode])
-    return FRSolver(mesh, prm)
+    from zhijian_b200.solver import FRSolver
+    return FRSolver(mesh, make_params_for(mode))
 
 
 def make_oracle(mesh, mode, threads):
@@ -447,11 +451,13 @@ def run_ours(args):
     adjoint = adjoint_run(stream) if not args.no_adjoint else None
     p5 = p5_precision_case(stream, args) if not args.no_p5 else None
     shear = shear_layer_sweep(stream, args) if not args.no_mixed else None
+    parts = partition_case(mesh, args) if (world == 1 and not args.no_parts) else None
 
     out = None
     if rank == 0:
         detail = {"fp64": fp64, "compat": compat, "precision_errors": precision, "adjoint": adjoint,
-                  "p5_precision": p5, "mixed_elements": shear, "e2e": e2e, "roofline": roofline}
+                  "p5_precision": p5, "mixed_elements": shear, "partitioned": parts, "e2e": e2e,
+                  "roofline": roofline}
         out = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
                "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
                "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
@@ -483,6 +489,9 @@ def run_ours(args):
             if "errors" in p5:
                 out["p5_l2_err_1000"] = p5["errors"]["l2"]
                 out["p5_split_bf16_l2_err_1000"] = p5["errors"]["split_bf16_l2"]
+        if parts:
+            parts["vs_whole"] = parts["value"] / value
+            out["parts4_vs_whole"] = parts["vs_whole"]
         if shear:
             out["mixed_mesh_speedups"] = [round(c["speedup_vs_fp64"], 3) for c in shear["cases"]]
         if world == 1 and not args.no_cpu_baseline:
@@ -697,6 +706,44 @@ def adjoint_run(stream, steps=200, k_ckpt=20, n_fd=4):
             "fd_check": {"h": 1e-6, "directions": n_fd, "max_rel_err": max(errs)}}
 
 
+def partition_case(mesh, args, nparts=4, mode="ns32"):
+    """The headline workload split into `nparts` RCB parts on this one GPU and
+    stepped by the multi-part driver (each part on its own stream; after each
+    launch that writes traces the cut-face rows are gathered, copied into the
+    neighbours' buffers and scattered into their ghost rows): DOF-RHS/s and
+    its ratio to the whole-mesh handle on the same GPU.  It measures the cost
+    of the exchange machinery, not a link: every copy stays on one device."""
+    import torch
+    from zhijian_b200 import meshgen as M
+    from zhijian_b200.partition import PartitionedSolver
+    parts = PartitionedSolver(mesh, make_params_for(mode), nparts)
+    streams = [torch.cuda.Stream() for _ in range(nparts)]
+    for p, st in zip(parts.parts, streams):
+        p.set_stream(st.cuda_stream)
+    parts.copyToDevice(M.taylor_green(parts.solution_point_coords()))
+    parts.advance(DT, max(args.warmup, 3))
+    torch.cuda.synchronize()
+    steps = max(args.steps, 20)
+    e0 = torch.cuda.Event(enable_timing=True)
+    e0.record(streams[0])
+    for st in streams[1:]:
+        st.wait_event(e0)
+    parts.advance(DT, steps, sync=False)
+    ends = []
+    for st in streams:
+        ev = torch.cuda.Event(enable_timing=True)
+        ev.record(st)
+        ends.append(ev)
+    torch.cuda.synchronize()
+    ms = max(e0.elapsed_time(ev) for ev in ends)
+    for p in parts.parts:
+        p.check_state()
+    parts.close()
+    dof = mesh.n_elem * (P + 1) ** 2
+    return {"workload": workload_name(mode) + f", precision form, {nparts} RCB parts on one GPU",
+            "value": dof * 3 * steps / (ms * 1e-3), "ms_per_step": ms / steps, "steps": steps}
+
+
 def precision_errors(mesh, stream, steps=1000):
     """L2 / Linf error of the precision form against the FP64 path after
     `steps` SSP-RK3 steps at CFL 0.5 from the Taylor-Green state (the FP64 GPU
@@ -736,6 +783,7 @@ def main():
     ap.add_argument("--no-adjoint", action="store_true")
     ap.add_argument("--no-p5", action="store_true")
     ap.add_argument("--no-mixed", action="store_true")
+    ap.add_argument("--no-parts", action="store_true")
     ap.add_argument("--detail", default=None, help="also write every sub-result to this JSON file")
     args = ap.parse_args()
     if args.warmup < 3:

@@ -850,11 +850,22 @@ zj_status zj_synchronize(zj_solver* s) {
     return ZJ_OK;
 }
 
+}  // extern "C"
+
+namespace {
+// The kernels read and write state rows as single 32-byte accesses, so a
+// caller's device arrays must start on a 32-byte boundary (cudaMalloc and
+// torch allocations do).
+bool misaligned(const void* p) { return (reinterpret_cast<uintptr_t>(p) & 31u) != 0; }
+constexpr const char* kAlignMsg = "device arrays must be 32-byte aligned";
+}  // namespace
+
+extern "C" {
+
 zj_status zj_rhs(zj_solver* s, const double* U_dev, double* R_dev) {
     if (!s || !U_dev || !R_dev) return ZJ_ERR_ARG;
     if (s->is_part) return refuse_part(s);
-    if ((reinterpret_cast<uintptr_t>(U_dev) | reinterpret_cast<uintptr_t>(R_dev)) & 15u)
-        return fail(s, ZJ_ERR_ARG, "U_dev and R_dev must be 16-byte aligned");
+    if (misaligned(U_dev) || misaligned(R_dev)) return fail(s, ZJ_ERR_ARG, kAlignMsg);
     if (s->mixed) return rhs_impl<float>(s, U_dev, R_dev, s->fT[2], nullptr, s->dPartR);
     return rhs_impl<double>(s, U_dev, R_dev, s->dT[2], nullptr, s->dPartR);
 }
@@ -957,8 +968,7 @@ extern "C" {
 zj_status zj_rhs_noalloc(zj_solver* s, const double* U_dev, double* R_dev) {
     if (!s || !U_dev || !R_dev) return ZJ_ERR_ARG;
     if (s->is_part) return refuse_part(s);
-    if ((reinterpret_cast<uintptr_t>(U_dev) | reinterpret_cast<uintptr_t>(R_dev)) & 15u)
-        return fail(s, ZJ_ERR_ARG, "U_dev and R_dev must be 16-byte aligned");
+    if (misaligned(U_dev) || misaligned(R_dev)) return fail(s, ZJ_ERR_ARG, kAlignMsg);
     int dev = -1;
     ZJ_CK(s, cudaGetDevice(&dev), "current device");
     if (dev != s->device)
@@ -978,16 +988,19 @@ zj_status zj_rhs_noalloc(zj_solver* s, const double* U_dev, double* R_dev) {
     ZJ_CK(s, noalloc_scratch(&scratch), "static scratch address");
     // Every scratch value is written before it is read (all traces by the
     // trace launch, the gradient traces by the gradient launch, one partial
-    // per CTA), so nothing needs clearing.  The trace block is a multiple of
-    // 16 bytes, so the partials stay aligned.
+    // per CTA), so nothing needs clearing.  The gradient traces (read and
+    // written as 32-byte rows) come first, at the array's 256-byte aligned
+    // start; the traces follow at 2 trace_n values (a multiple of 32 bytes,
+    // trace_n being a multiple of 4), the partials after them at a multiple of
+    // 16 bytes.
     char* base = reinterpret_cast<char*>(scratch);
     double* partials = reinterpret_cast<double*>(base + trace_bytes);
+    const size_t tq_n = is_ns(s) ? 2 * s->trace_n : 0;
     if (s->mixed) {
-        float* traces = reinterpret_cast<float*>(base);
-        return rhs_impl<float>(s, U_dev, R_dev, traces, is_ns(s) ? traces + s->trace_n : nullptr, partials);
+        float* tq = reinterpret_cast<float*>(base);
+        return rhs_impl<float>(s, U_dev, R_dev, tq + tq_n, is_ns(s) ? tq : nullptr, partials);
     }
-    double* traces = scratch;
-    return rhs_impl<double>(s, U_dev, R_dev, traces, is_ns(s) ? traces + s->trace_n : nullptr, partials);
+    return rhs_impl<double>(s, U_dev, R_dev, scratch + tq_n, is_ns(s) ? scratch : nullptr, partials);
 }
 
 }  // extern "C"
@@ -1008,7 +1021,6 @@ zj_status diff_supported(zj_solver* s) {
     return ZJ_OK;
 }
 
-bool misaligned(const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15u) != 0; }
 
 zj_status ensure_diff(zj_solver* s) {
     if (s->diff_ready) return ZJ_OK;
@@ -1200,7 +1212,7 @@ zj_status zj_rhs_jvp(zj_solver* s, const double* U_dev, const double* V_dev, dou
                      double* R_dev, double* JV_dev) {
     if (!s || !U_dev || !V_dev || !JV_dev) return ZJ_ERR_ARG;
     if (misaligned(U_dev) || misaligned(V_dev) || misaligned(JV_dev) || (R_dev && misaligned(R_dev)))
-        return fail(s, ZJ_ERR_ARG, "device arrays must be 16-byte aligned");
+        return fail(s, ZJ_ERR_ARG, kAlignMsg);
     zj_status st = diff_supported(s);
     if (st == ZJ_OK) st = ensure_diff(s);
     if (st == ZJ_OK) st = jvp_core(s, U_dev, V_dev, dRe, R_dev, JV_dev);
@@ -1211,7 +1223,7 @@ zj_status zj_rhs_vjp(zj_solver* s, const double* U_dev, const double* L_dev, dou
                      double* dRe_out) {
     if (!s || !U_dev || !L_dev || !W_dev) return ZJ_ERR_ARG;
     if (misaligned(U_dev) || misaligned(L_dev) || misaligned(W_dev))
-        return fail(s, ZJ_ERR_ARG, "device arrays must be 16-byte aligned");
+        return fail(s, ZJ_ERR_ARG, kAlignMsg);
     zj_status st = diff_supported(s);
     if (st == ZJ_OK) st = ensure_diff(s);
     if (st != ZJ_OK) return st;
@@ -1225,6 +1237,7 @@ zj_status zj_rhs_vjp(zj_solver* s, const double* U_dev, const double* L_dev, dou
 zj_status zj_step_vjp(zj_solver* s, const double* U_dev, double dt, const double* B_dev,
                       double* A_dev, double* dRe_acc) {
     if (!s || !U_dev || !B_dev || !A_dev) return ZJ_ERR_ARG;
+    if (misaligned(U_dev) || misaligned(B_dev) || misaligned(A_dev)) return fail(s, ZJ_ERR_ARG, kAlignMsg);
     if (!std::isfinite(dt)) return fail(s, ZJ_ERR_ARG, "bad dt");
     zj_status st = diff_supported(s);
     if (st == ZJ_OK) st = ensure_diff(s);
@@ -1245,6 +1258,7 @@ zj_status zj_step_vjp(zj_solver* s, const double* U_dev, double dt, const double
 zj_status zj_adjoint_run(zj_solver* s, double dt, int nsteps, int k_ckpt, double* G_dev, double* dRe,
                          int64_t* bytes, double* ms_forward, double* ms_adjoint) {
     if (!s || !G_dev) return ZJ_ERR_ARG;
+    if (misaligned(G_dev)) return fail(s, ZJ_ERR_ARG, kAlignMsg);
     if (nsteps < 1 || k_ckpt < 1 || !std::isfinite(dt)) return fail(s, ZJ_ERR_ARG, "bad dt, nsteps or k_ckpt");
     zj_status st = diff_supported(s);
     if (st == ZJ_OK) st = ensure_diff(s);
@@ -1833,6 +1847,9 @@ zj_status zj_parts_rhs(zj_solver* const* parts, int n, const double* const* U_de
     zj_status st = parts_check(parts, n, P);
     if (st != ZJ_OK) return st;
     if (!U_dev || !R_dev) return fail(P[0], ZJ_ERR_ARG, "U_dev or R_dev is NULL");
+    for (int i = 0; i < n; ++i)
+        if (!U_dev[i] || !R_dev[i] || misaligned(U_dev[i]) || misaligned(R_dev[i]))
+            return fail(P[0], ZJ_ERR_ARG, "U_dev and R_dev must be non-NULL, 32-byte aligned device arrays");
     DeviceGuard guard;
     return P[0]->mixed ? parts_rhs_t<float>(P, U_dev, R_dev) : parts_rhs_t<double>(P, U_dev, R_dev);
 }

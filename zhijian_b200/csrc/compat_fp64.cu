@@ -229,7 +229,7 @@ k_compat_stage(const StageArgs a) {
     }
     if (is_sp) {
         const long long idx = e * NSP + k;
-        load4(a.U + idx * 4, u);
+        gload4(a.U + idx * 4, u);
         if ((k & 3) == 0) {
             prefetch_l2(a.Jinv + idx * 4);
             if (a.stage >= 2) prefetch_l2(a.U0 + idx * 4);
@@ -295,7 +295,7 @@ k_compat_stage(const StageArgs a) {
         const long long idx = e * NSP + k;
         double ji[4], u0[4];
         load4_nc(a.Jinv + idx * 4, ji);
-        if (a.stage >= 2) load4(a.U0 + idx * 4, u0);
+        if (a.stage >= 2) gload4(a.U0 + idx * 4, u0);
         double Di[N1], Dj[N1];
 #pragma unroll
         for (int m = 0; m < N1; ++m) { Di[m] = sOps[i * N1 + m]; Dj[m] = sOps[j * N1 + m]; }
@@ -335,7 +335,7 @@ k_compat_stage(const StageArgs a) {
             res[v] = rr;
         }
         if (a.stage == 0) {
-            store4(a.R + idx * 4, res);
+            gstore4(a.R + idx * 4, res);
 #pragma unroll
             for (int v = 0; v < 4; ++v) rsq += res[v] * res[v];
         } else {
@@ -348,7 +348,7 @@ k_compat_stage(const StageArgs a) {
                 else uo[v] = (1.0 / 3.0) * u0[v] + (2.0 / 3.0) * u[v] + (2.0 / 3.0) * dt * res[v];
             }
             positivity(uo);
-            store4(a.Uout + idx * 4, uo);
+            gstore4(a.Uout + idx * 4, uo);
             double* su = sU + el * FS + j * RS + i;
 #pragma unroll
             for (int v = 0; v < 4; ++v) su[v * VS] = uo[v];
@@ -369,7 +369,7 @@ k_compat_stage(const StageArgs a) {
     if (is_fp) {
         double t[4];
         trace_point<N1, RS, VS>(sU + el * FS, sOps + N1 * N1, sOps + N1 * N1 + N1, edge, fp, t);
-        store4(a.Tout + (e * NFT + k) * 4, t);
+        gstore4(a.Tout + (e * NFT + k) * 4, t);
     }
 }
 
@@ -399,7 +399,7 @@ k_traces(const double* __restrict__ U, double* __restrict__ T, const double* __r
         const int edge = k / N1, fp = k - edge * N1;
         double t[4];
         trace_point<N1, RS, VS>(sU + el * FS, sOps + N1 * N1, sOps + N1 * N1 + N1, edge, fp, t);
-        store4(T + (e * NFT + k) * 4, t);
+        gstore4(T + (e * NFT + k) * 4, t);
     }
 }
 

@@ -188,7 +188,7 @@ k_ns_grad(const StageArgsT<T> a) {
             // D (U - U_e): the reference drops out of the derivative exactly
             double ud[4];
             T ue[4];
-            load4(a.U + idx * 4, ud);
+            gload4(a.U + idx * 4, ud);
             load_state(a.U + e * NSP * 4, ue);
             state_minus_ref(ud, ue, u);
         } else {
@@ -224,8 +224,7 @@ k_ns_grad(const StageArgsT<T> a) {
         trace_point<N1, RS, VS>(sQ + el * QS + 4 * VS, sOps + N1 * N1, sOps + N1 * N1 + N1, edge,
                                 fp, t + 4);
         T* o = a.TQout + (e * NFT + k) * 8;
-        store4(o, t);
-        store4(o + 4, t + 4);
+        gstore8(o, t);
     }
 }
 
@@ -263,14 +262,12 @@ k_ns_stage(const StageArgsT<T> a) {
     if (is_fp) {
         load_face_point<N1>(a, e, edge, fp, f);
         const T* qt = a.TQ + (e * NFT + k) * 8;
-        load4_nc(qt, Qo);
-        load4_nc(qt + 4, Qo + 4);
+        gload8_nc(qt, Qo);
 #pragma unroll
         for (int v = 0; v < 8; ++v) Qn[v] = Qo[v];
         if (has_neighbour_gradient(f.r)) {
             const T* qn = a.TQ + (neighbour_row(f.r, a.n_elem) * N1 + (N1 - 1 - fp)) * 8;
-            load4_nc(qn, Qn);
-            load4_nc(qn + 4, Qn + 4);
+            gload8_nc(qn, Qn);
         }
         T d[4];
 #pragma unroll
@@ -378,7 +375,7 @@ k_ns_stage(const StageArgsT<T> a) {
     if (is_sp) {
         const long long idx = e * NSP + k;
         double u0[4];
-        if (a.stage >= 2) load4(a.U0 + idx * 4, u0);
+        if (a.stage >= 2) gload4(a.U0 + idx * 4, u0);
         T Di[N1], Dj[N1];
 #pragma unroll
         for (int m = 0; m < N1; ++m) { Di[m] = sOps[i * N1 + m]; Dj[m] = sOps[j * N1 + m]; }
@@ -422,11 +419,11 @@ k_ns_stage(const StageArgsT<T> a) {
 #pragma unroll
                 for (int v = 0; v < 4; ++v) us[v] = double(u[v]);
             } else {
-                load4(a.U + idx * 4, us);
+                gload4(a.U + idx * 4, us);
             }
             double uo[4];
             rk_update(a.stage, *a.dt, us, u0, res, uo);
-            store4(a.Uout + idx * 4, uo);
+            gstore4(a.Uout + idx * 4, uo);
             T* su = sU + el * FS + j * RS + i;
             T un[4];
             if constexpr (kRef) state_minus_ref(uo, ue, un);
@@ -457,7 +454,7 @@ k_ns_stage(const StageArgsT<T> a) {
 #pragma unroll
             for (int v = 0; v < 4; ++v) t[v] += ue[v];
         }
-        store4(a.Tout + (e * NFT + k) * 4, t);
+        gstore4(a.Tout + (e * NFT + k) * 4, t);
         if (boundary_condition_edge(f.r)) store_ghost<N1>(a, f.r, f.nx, f.ny, fp, t);
     }
 }

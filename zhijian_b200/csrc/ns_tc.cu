@@ -149,14 +149,12 @@ k_ns_stage_tc(const StageArgsT<float> a, const __grid_constant__ CUtensorMap ama
     if (is_fp) {
         load_face_point<N1>(a, e, edge, fp, f);
         const float* qt = a.TQ + (e * NFT + k) * 8;
-        load4_nc(qt, Qo);
-        load4_nc(qt + 4, Qo + 4);
+        gload8_nc(qt, Qo);
 #pragma unroll
         for (int v = 0; v < 8; ++v) Qn[v] = Qo[v];
         if (has_neighbour_gradient(f.r)) {
             const float* qn = a.TQ + (neighbour_row(f.r, a.n_elem) * N1 + (N1 - 1 - fp)) * 8;
-            load4_nc(qn, Qn);
-            load4_nc(qn + 4, Qn + 4);
+            gload8_nc(qn, Qn);
         }
         float d[4];
 #pragma unroll
@@ -302,7 +300,7 @@ k_ns_stage_tc(const StageArgsT<float> a, const __grid_constant__ CUtensorMap ama
     if (is_sp) {
         const long long idx = e * NSP + k;
         double u0[4];
-        if (a.stage >= 2) load4(a.U0 + idx * 4, u0);
+        if (a.stage >= 2) gload4(a.U0 + idx * 4, u0);
         const float* gL = sOps + N1 * N1 + 2 * N1;
         const float* gR = gL + N1;
         const float gRi = gR[i], gLi = gL[i], gRj = gR[j], gLj = gL[j];
@@ -325,10 +323,10 @@ k_ns_stage_tc(const StageArgsT<float> a, const __grid_constant__ CUtensorMap ama
             store_residual(a, idx, res, rsq);
         } else {
             double us[4];
-            load4(a.U + idx * 4, us);
+            gload4(a.U + idx * 4, us);
             double uo[4];
             rk_update(a.stage, *a.dt, us, u0, res, uo);
-            store4(a.Uout + idx * 4, uo);
+            gstore4(a.Uout + idx * 4, uo);
             float un[4];
             state_minus_ref(uo, ue, un);
             float* su = sU + el * FS + j * RS + i;
@@ -352,7 +350,7 @@ k_ns_stage_tc(const StageArgsT<float> a, const __grid_constant__ CUtensorMap ama
         trace_point<N1, RS, VS>(sU + el * FS, sOps + N1 * N1, sOps + N1 * N1 + N1, edge, fp, t);
 #pragma unroll
         for (int v = 0; v < 4; ++v) t[v] += ue[v];
-        store4(a.Tout + (e * NFT + k) * 4, t);
+        gstore4(a.Tout + (e * NFT + k) * 4, t);
         if (boundary_condition_edge(f.r)) store_ghost<N1>(a, f.r, f.nx, f.ny, fp, t);
     }
 

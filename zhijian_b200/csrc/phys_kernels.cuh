@@ -109,14 +109,14 @@ __device__ __forceinline__ void store_ghost(const StageArgsT<T>& a, const EdgeRe
                                             int fp, const T* t) {
     T q[4];
     ghost_phys(t, nx, ny, edge_bc_type(r.flags), a.bc + (long long)r.nbr_edge * 8, T(a.gamma), q);
-    store4(a.Tout + ((a.n_elem * 4 + r.nbr_edge) * N1 + (N1 - 1 - fp)) * 4, q);
+    gstore4(a.Tout + ((a.n_elem * 4 + r.nbr_edge) * N1 + (N1 - 1 - fp)) * 4, q);
 }
 
 // Conserved state of one solution point in the arithmetic type.
 template <typename T>
 __device__ __forceinline__ void load_state(const double* p, T* u) {
     double d[4];
-    load4(p, d);
+    gload4(p, d);
 #pragma unroll
     for (int v = 0; v < 4; ++v) u[v] = T(d[v]);
 }
@@ -125,10 +125,10 @@ __device__ __forceinline__ void load_state(const double* p, T* u) {
 // (with the input tangent for the dual-number instantiation).
 template <typename T>
 __device__ __forceinline__ void stage_state(const StageArgsT<T>& a, long long idx, double* ud, T* u) {
-    load4(a.U + idx * 4, ud);
+    gload4(a.U + idx * 4, ud);
     if constexpr (IsDual<T>::value) {
         double t[4];
-        load4(a.dU + idx * 4, t);
+        gload4(a.dU + idx * 4, t);
 #pragma unroll
         for (int v = 0; v < 4; ++v) u[v] = Dual(ud[v], t[v]);
     } else {
@@ -145,12 +145,12 @@ __device__ __forceinline__ void store_residual(const StageArgsT<T>& a, long long
     double rd[4];
 #pragma unroll
     for (int v = 0; v < 4; ++v) { rd[v] = double(res[v]); rsq += rd[v] * rd[v]; }
-    store4(a.R + idx * 4, rd);
+    gstore4(a.R + idx * 4, rd);
     if constexpr (IsDual<T>::value) {
         double td[4];
 #pragma unroll
         for (int v = 0; v < 4; ++v) td[v] = res[v].d;
-        store4(a.dR + idx * 4, td);
+        gstore4(a.dR + idx * 4, td);
     }
 }
 
@@ -343,7 +343,7 @@ k_phys_stage(const StageArgsT<T> a) {
     if (is_sp) {
         const long long idx = e * NSP + k;
         double u0[4];
-        if (a.stage >= 2) load4(a.U0 + idx * 4, u0);
+        if (a.stage >= 2) gload4(a.U0 + idx * 4, u0);
         T Di[N1], Dj[N1];
 #pragma unroll
         for (int m = 0; m < N1; ++m) { Di[m] = sOps[i * N1 + m]; Dj[m] = sOps[j * N1 + m]; }
@@ -382,11 +382,11 @@ k_phys_stage(const StageArgsT<T> a) {
 #pragma unroll
                 for (int v = 0; v < 4; ++v) us[v] = double(u[v]);
             } else {
-                load4(a.U + idx * 4, us);
+                gload4(a.U + idx * 4, us);
             }
             double uo[4];
             rk_update(a.stage, *a.dt, us, u0, res, uo);
-            store4(a.Uout + idx * 4, uo);
+            gstore4(a.Uout + idx * 4, uo);
             T* su = sU + el * FS + j * RS + i;
             T un[4];
             if constexpr (kRef) state_minus_ref(uo, ue, un);
@@ -417,7 +417,7 @@ k_phys_stage(const StageArgsT<T> a) {
 #pragma unroll
             for (int v = 0; v < 4; ++v) t[v] += ue[v];
         }
-        store4(a.Tout + (e * NFT + k) * 4, t);
+        gstore4(a.Tout + (e * NFT + k) * 4, t);
         if (boundary_condition_edge(r)) store_ghost<N1>(a, r, nr[0], nr[1], fp, t);
     }
 }
@@ -458,7 +458,7 @@ k_phys_traces(const StageArgsT<T> a) {
 #pragma unroll
             for (int v = 0; v < 4; ++v) t[v] += ue[v];
         }
-        store4(a.Tout + (e * NFT + k) * 4, t);
+        gstore4(a.Tout + (e * NFT + k) * 4, t);
         const EdgeRec r = a.edges[e * 4 + edge];
         if (boundary_condition_edge(r)) {
             T n[3];

@@ -147,7 +147,7 @@ k_tri_traces(const StageArgsT<T> a, const int32_t* __restrict__ elist, long long
 #pragma unroll
             for (int v = 0; v < 4; ++v) t[v] += ue[v];
         }
-        store4(a.Tout + (e * 4 * N1 + k) * 4, t);
+        gstore4(a.Tout + (e * 4 * N1 + k) * 4, t);
         const EdgeRec r = a.edges[e * 4 + edge];
         if (r.flags & kEdgeBoundary) {
             T n[3];
@@ -223,8 +223,7 @@ k_tri_grad(const StageArgsT<T> a, const int32_t* __restrict__ elist, long long n
         tri_interp<NT, FS>(sQ + el * 2 * ES, sOps + Lo::L + k * NT, t);
         tri_interp<NT, FS>(sQ + el * 2 * ES + ES, sOps + Lo::L + k * NT, t + 4);
         T* o = a.TQout + (e * 4 * N1 + k) * 8;
-        store4(o, t);
-        store4(o + 4, t + 4);
+        gstore8(o, t);
     }
 }
 
@@ -269,14 +268,12 @@ k_tri_stage(const StageArgsT<T> a, const int32_t* __restrict__ elist, long long 
         if (!(r.flags & kEdgeOrphan)) load4_nc(a.Tin + (neighbour_row(r, a.n_elem) * N1 + (N1 - 1 - fp)) * 4, qn);
         if constexpr (VISC) {
             const T* qt = a.TQ + (e * 4 * N1 + k) * 8;
-            load4_nc(qt, Qo);
-            load4_nc(qt + 4, Qo + 4);
+            gload8_nc(qt, Qo);
 #pragma unroll
             for (int v = 0; v < 8; ++v) Qn[v] = Qo[v];
             if (!(r.flags & (kEdgeOrphan | kEdgeBoundary))) {
                 const T* q2 = a.TQ + (((long long)r.nbr * 4 + r.nbr_edge) * N1 + (N1 - 1 - fp)) * 8;
-                load4_nc(q2, Qn);
-                load4_nc(q2 + 4, Qn + 4);
+                gload8_nc(q2, Qn);
             }
             T d[4];
 #pragma unroll
@@ -380,7 +377,7 @@ k_tri_stage(const StageArgsT<T> a, const int32_t* __restrict__ elist, long long 
     if (is_sp) {
         const long long idx = e * NSP + k;
         double u0[4];
-        if (a.stage >= 2) load4(a.U0 + idx * 4, u0);
+        if (a.stage >= 2) gload4(a.U0 + idx * 4, u0);
         T div[4] = {T(0), T(0), T(0), T(0)};
         const T* Dr = sOps + Lo::DR + k * NT;
         const T* Dsr = sOps + Lo::DSo + k * NT;
@@ -408,10 +405,10 @@ k_tri_stage(const StageArgsT<T> a, const int32_t* __restrict__ elist, long long 
             store_residual(a, idx, res, rsq);
         } else {
             double us[4];
-            load4(a.U + idx * 4, us);
+            gload4(a.U + idx * 4, us);
             double uo[4];
             rk_update(a.stage, *a.dt, us, u0, res, uo);
-            store4(a.Uout + idx * 4, uo);
+            gstore4(a.Uout + idx * 4, uo);
             T un[4];
             if constexpr (kRef) state_minus_ref(uo, ue, un);
             else {
@@ -441,7 +438,7 @@ k_tri_stage(const StageArgsT<T> a, const int32_t* __restrict__ elist, long long 
 #pragma unroll
             for (int v = 0; v < 4; ++v) t[v] += ue[v];
         }
-        store4(a.Tout + (e * 4 * N1 + k) * 4, t);
+        gstore4(a.Tout + (e * 4 * N1 + k) * 4, t);
         if (r.flags & kEdgeBoundary) store_ghost<N1>(a, r, nr[0], nr[1], fp, t);
     }
 }

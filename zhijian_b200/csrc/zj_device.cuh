@@ -53,10 +53,33 @@ __device__ __forceinline__ void load4(const double* p, double* v) {
     const double2 b = *reinterpret_cast<const double2*>(p + 2);
     v[0] = a.x; v[1] = a.y; v[2] = b.x; v[3] = b.y;
 }
+// Global rows of four doubles: one 32-byte access per thread (sm_100
+// ld/st .v4.f64), so a warp's request covers each 32-byte sector once; two
+// 16-byte accesses fetch the same sectors twice.  The rows are 32-byte
+// aligned: the library's buffers come from cudaMalloc with every row at a
+// multiple of 32 bytes, and the entry points refuse caller arrays that are
+// not 32-byte aligned.
 __device__ __forceinline__ void load4_nc(const double* p, double* v) {
-    const double2 a = __ldg(reinterpret_cast<const double2*>(p));
-    const double2 b = __ldg(reinterpret_cast<const double2*>(p + 2));
-    v[0] = a.x; v[1] = a.y; v[2] = b.x; v[3] = b.y;
+    asm("ld.global.nc.v4.f64 {%0, %1, %2, %3}, [%4];" : "=d"(v[0]), "=d"(v[1]), "=d"(v[2]), "=d"(v[3]) : "l"(p));
+}
+__device__ __forceinline__ void gload4(const double* p, double* v) {
+    asm volatile("ld.global.v4.f64 {%0, %1, %2, %3}, [%4];"
+                 : "=d"(v[0]), "=d"(v[1]), "=d"(v[2]), "=d"(v[3])
+                 : "l"(p)
+                 : "memory");
+}
+__device__ __forceinline__ void gstore4(double* p, const double* v) {
+    asm volatile("st.global.v4.f64 [%0], {%1, %2, %3, %4};" ::"l"(p), "d"(v[0]), "d"(v[1]), "d"(v[2]), "d"(v[3])
+                 : "memory");
+}
+// Eight values (a gradient-trace point): two 32-byte accesses.
+__device__ __forceinline__ void gload8_nc(const double* p, double* v) {
+    load4_nc(p, v);
+    load4_nc(p + 4, v + 4);
+}
+__device__ __forceinline__ void gstore8(double* p, const double* v) {
+    gstore4(p, v);
+    gstore4(p + 4, v + 4);
 }
 __device__ __forceinline__ void store4(double* p, const double* v) {
     *reinterpret_cast<double2*>(p) = make_double2(v[0], v[1]);
@@ -75,15 +98,27 @@ __device__ __forceinline__ void load4_nc(const float* p, float* v) {
 __device__ __forceinline__ void store4(float* p, const float* v) {
     *reinterpret_cast<float4*>(p) = make_float4(v[0], v[1], v[2], v[3]);
 }
+// Global float rows: four values are one 16-byte access; eight (a gradient
+// trace point, 32-byte aligned like the double rows) one 32-byte access.
+__device__ __forceinline__ void gstore4(float* p, const float* v) { store4(p, v); }
+__device__ __forceinline__ void gload8_nc(const float* p, float* v) {
+    asm("ld.global.nc.v8.f32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
+        : "=f"(v[0]), "=f"(v[1]), "=f"(v[2]), "=f"(v[3]), "=f"(v[4]), "=f"(v[5]), "=f"(v[6]), "=f"(v[7])
+        : "l"(p));
+}
+__device__ __forceinline__ void gstore8(float* p, const float* v) {
+    asm volatile("st.global.v8.f32 [%0], {%1, %2, %3, %4, %5, %6, %7, %8};" ::"l"(p), "f"(v[0]), "f"(v[1]),
+                 "f"(v[2]), "f"(v[3]), "f"(v[4]), "f"(v[5]), "f"(v[6]), "f"(v[7])
+                 : "memory");
+}
 
 __device__ __forceinline__ double ldg_any(const double* p) { return __ldg(p); }
 __device__ __forceinline__ float ldg_any(const float* p) { return __ldg(p); }
 
 // (nx, ny, len) of an edge-normal record.
 __device__ __forceinline__ void load_normal(const double4* p, double* n) {
-    const double2 a = __ldg(reinterpret_cast<const double2*>(p));
-    const double2 b = __ldg(reinterpret_cast<const double2*>(p) + 1);
-    n[0] = a.x; n[1] = a.y; n[2] = b.x;
+    double pad;
+    asm("ld.global.nc.v4.f64 {%0, %1, %2, %3}, [%4];" : "=d"(n[0]), "=d"(n[1]), "=d"(n[2]), "=d"(pad) : "l"(p));
 }
 __device__ __forceinline__ void load_normal(const float4* p, float* n) {
     const float4 a = __ldg(p);

@@ -90,6 +90,17 @@ __device__ __forceinline__ void store4(Dual* p, const Dual* v) {
 #pragma unroll
     for (int i = 0; i < 4; ++i) q[i] = make_double2(v[i].v, v[i].d);
 }
+// The global-row helpers of the FP64 and FP32 kernels, on dual numbers.
+__device__ __forceinline__ void gload4(const Dual* p, Dual* v) { load4(p, v); }
+__device__ __forceinline__ void gstore4(Dual* p, const Dual* v) { store4(p, v); }
+__device__ __forceinline__ void gload8_nc(const Dual* p, Dual* v) {
+    load4(p, v);
+    load4(p + 4, v + 4);
+}
+__device__ __forceinline__ void gstore8(Dual* p, const Dual* v) {
+    store4(p, v);
+    store4(p + 4, v + 4);
+}
 __device__ __forceinline__ Dual ldg_any(const Dual* p) { return *p; }
 __device__ __forceinline__ void load_normal(const Dual4* p, Dual* n) {
     n[0] = p->x; n[1] = p->y; n[2] = p->z;
