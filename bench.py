@@ -263,8 +263,8 @@ def run_reference(args):
             "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
 
 
-KERNELS = {"ns": "k_ns_grad<3,double> + k_ns_stage<3,Roe,double> (one residual)",
-           "ns32": "k_ns_grad<3,float> + k_ns_stage<3,Roe,float> (one residual)",
+KERNELS = {"ns": "k_ns_grad_lines<3,double> + k_ns_stage<3,Roe,double> (one residual)",
+           "ns32": "k_ns_grad_lines<3,float> + k_ns_stage<3,Roe,float> (one residual)",
            "compat": "k_compat_stage<3>"}
 LAUNCHES_PER_RHS = {"ns": 2, "ns32": 2, "compat": 1}
 # handles of the streamed end-to-end loop: 2 reach 3.6e9 DOF-RHS/s, 3 and 4

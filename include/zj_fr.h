@@ -181,8 +181,9 @@ zj_status zj_step(zj_solver* s, double dt, int nsteps);
  * enable = 0 turns the graphs off for this handle. */
 zj_status zj_set_step_graphs(zj_solver* s, int enable);
 zj_status zj_synchronize(zj_solver* s);
-/* One residual R = dU/dt on device buffers of E*n_sp*4 doubles, on the
- * handle's stream (computeResidual_GPU, fr_solver.cpp:335-608).  Borrowed. */
+/* One residual R = dU/dt on device buffers of E*n_sp*4 doubles, 32-byte
+ * aligned (ZJ_ERR_ARG otherwise), on the handle's stream
+ * (computeResidual_GPU, fr_solver.cpp:335-608).  Borrowed. */
 zj_status zj_rhs(zj_solver* s, const double* U_dev, double* R_dev);
 /* Same through host buffers: H2D, residual, D2H, synchronised. */
 zj_status zj_rhs_host(zj_solver* s, const double* U_host, double* R_host);
@@ -229,7 +230,7 @@ void* zj_get_stream(const zj_solver* s);
  * do not use the library across a cudaDeviceReset of the device.  All calls
  * share the one array: calls that overlap on the GPU (other streams, other
  * handles, other host threads) race on it.  Inputs and outputs are the
- * caller's device buffers, 16-byte aligned, on the handle's stream. */
+ * caller's device buffers, 32-byte aligned, on the handle's stream. */
 #define ZJ_NOALLOC_SCRATCH_BYTES (32u * 1024u * 1024u)
 zj_status zj_rhs_noalloc(zj_solver* s, const double* U_dev, double* R_dev);
 
@@ -278,7 +279,7 @@ zj_status zj_parts_residual_norm(zj_solver* const* parts, int n, double* out);
 
 /* ---- differentiation (physics mode, FP64) ----------------------------------
  * No reference counterpart: the reference has no adjoint.  All pointers are
- * device pointers to [E][n_sp][4] FP64 arrays, 16-byte aligned; the calls are
+ * device pointers to [E][n_sp][4] FP64 arrays, 32-byte aligned; the calls are
  * asynchronous on the handle's stream.  Compat mode and the mixed-precision
  * form return ZJ_ERR_UNSUPPORTED. */
 

@@ -43,6 +43,12 @@
 #ifndef ZJ_NSG32_MIN_BLOCKS
 #define ZJ_NSG32_MIN_BLOCKS 6     // mixed-precision gradient kernel (40 registers)
 #endif
+#ifndef ZJ_NSL_MIN_BLOCKS
+#define ZJ_NSL_MIN_BLOCKS 4       // FP64 gradient kernel by lines (per 128 threads)
+#endif
+#ifndef ZJ_NSL32_MIN_BLOCKS
+#define ZJ_NSL32_MIN_BLOCKS 6     // mixed-precision gradient kernel by lines
+#endif
 
 namespace zj {
 namespace {
@@ -226,6 +232,220 @@ k_ns_grad(const StageArgsT<T> a) {
         T* o = a.TQout + (e * NFT + k) * 8;
         gstore8(o, t);
     }
+}
+
+// ---- gradient by lines (float and double)
+//
+// 2 N1 threads per element: one per row j (an xi-line of solution points
+// (0..N1-1, j)) and one per column i (an eta-line (i, 0..N1-1)).  The CTA
+// first stages its elements' states and metrics into shared memory with
+// 16-byte cp.async copies (each 16-byte piece fetched once, the metrics before
+// pdl_wait since they never come from a kernel), while every line thread
+// loads the traces at its line's two end points (its own and the
+// neighbour's).  A line thread then takes the corrected derivative along its
+// line in registers (row: dU/dxi with the jumps of edges 1 and 3; column:
+// dU/deta with those of edges 0 and 2) and swaps derivatives with the
+// crossing lines through one shared tile.  It forms Q = (xi_x dU/dxi + eta_x
+// dU/deta, xi_y dU/dxi + eta_y dU/deta) at its N1 points and the traces of Q
+// at its two end points (row j: edge 1 point j with l(+1), edge 3 point
+// N1-1-j with l(-1); column i: edge 0 point i with l(-1), edge 2 point
+// N1-1-i with l(+1)).  Every sum is corrected_gradient_tr's and
+// trace_point's, term for term in the same order, so the traces equal
+// k_ns_grad's.
+//
+// Rows and columns run the same instruction stream (the role only selects
+// strides, edges and weights) and fill separate warps at P3.  The derivative
+// tile holds point (a = xi index, b = eta index) at a*(N1+1) + b; the staged
+// rows are padded by 16 bytes; the element strides spread both access
+// patterns over the banks.
+template <int P, typename T>
+struct LineShape {
+    static constexpr int N1 = P + 1, NSP = N1 * N1, NFT = 4 * N1;
+    static constexpr int EB = kCtaThreads / (2 * N1);   // elements per CTA
+    static constexpr int THREADS = EB * 2 * N1;
+    static constexpr int NOPS = N1 * N1 + 4 * N1;
+    // derivative tile: [el][role][var][a*R + b]
+    static constexpr int R = N1 + 1;
+    static constexpr int VB = N1 * R;
+    static constexpr int MOD = sizeof(T) == 8 ? 16 : 32;
+    static constexpr int ES = 8 * VB + ((4 - (8 * VB) % MOD) + MOD) % MOD;
+    // staged states (doubles): [el][b][a*4 + v], rows padded by 16 bytes, the
+    // element stride 64 bytes past a multiple of 128
+    static constexpr int RU = N1 * 4 + 2;
+    static constexpr int EU = N1 * RU + ((8 - (N1 * RU) % 16) + 16) % 16;
+    // staged metrics (T): [el][b][a*4 + c], same padding rules
+    static constexpr int TW = 16 / sizeof(T);            // values per 16 bytes
+    static constexpr int RJ = N1 * 4 + TW;
+    static constexpr int JM = 128 / sizeof(T), JO = 64 / sizeof(T);
+    static constexpr int EJ = N1 * RJ + ((JO - (N1 * RJ) % JM) + JM) % JM;
+    // dynamic shared memory layout (byte offsets, 16-byte aligned)
+    static constexpr size_t OFF_U = 0;
+    static constexpr size_t OFF_J = OFF_U + sizeof(double) * EB * EU;
+    static constexpr size_t OFF_D = OFF_J + sizeof(T) * EB * EJ;
+    static constexpr size_t OFF_OPS = OFF_D + ((sizeof(T) * EB * ES + 15) & ~size_t(15));
+    static constexpr size_t SMEM = OFF_OPS + ((sizeof(T) * NOPS + 15) & ~size_t(15));
+    static_assert(OFF_J % 16 == 0 && OFF_D % 16 == 0 && OFF_OPS % 16 == 0, "16-byte aligned regions");
+    // A line thread holds a line's states and derivatives: twice the values
+    // of a point thread, at half the threads per element.
+    static constexpr int MIN_BLOCKS = sizeof(T) == 8 ? ZJ_NSL_MIN_BLOCKS : ZJ_NSL32_MIN_BLOCKS;
+};
+
+// 16-byte asynchronous global -> shared copy (cp.async, cached in L2 only),
+// and the wait for all of this thread's copies.
+__device__ __forceinline__ void cp_async16(void* sdst, const void* gsrc) {
+    const unsigned d = static_cast<unsigned>(__cvta_generic_to_shared(sdst));
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(d), "l"(gsrc) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
+
+template <int P, typename T>
+__global__ void __launch_bounds__(LineShape<P, T>::THREADS, LineShape<P, T>::MIN_BLOCKS)
+k_ns_grad_lines(const StageArgsT<T> a) {
+    using L = LineShape<P, T>;
+    constexpr int N1 = L::N1, NSP = L::NSP, NFT = L::NFT, EB = L::EB, R = L::R, VB = L::VB, ES = L::ES;
+    constexpr int RU = L::RU, EU = L::EU, RJ = L::RJ, EJ = L::EJ, TW = L::TW;
+    extern __shared__ __align__(16) unsigned char smem[];
+    double* sU = reinterpret_cast<double*>(smem + L::OFF_U);
+    T* sJ = reinterpret_cast<T*>(smem + L::OFF_J);
+    T* sD = reinterpret_cast<T*>(smem + L::OFF_D);
+    T* sOps = reinterpret_cast<T*>(smem + L::OFF_OPS);
+
+    const int tid = threadIdx.x;
+    // metrics: 16-byte pieces of the CTA's elements (geometry: before pdl_wait)
+    constexpr int KJ = 4 / TW;                 // pieces per point
+    for (int c = tid; c < EB * NSP * KJ; c += L::THREADS) {
+        const int el2 = c / (NSP * KJ), r = c - el2 * NSP * KJ, p = r / KJ, h = r - p * KJ;
+        bool v2;
+        const long long e2 = block_element(a, EB, el2, v2);
+        if (v2) cp_async16(sJ + el2 * EJ + (p / N1) * RJ + (p % N1) * 4 + h * TW, a.Jinv + (e2 * NSP + p) * 4 + h * TW);
+    }
+    cp_async_commit();
+    for (int t = tid; t < L::NOPS; t += L::THREADS) sOps[t] = a.ops[t];
+    pdl_launch_dependents();
+    pdl_wait();   // the state and traces come from the previous stage
+    for (int c = tid; c < EB * NSP * 2; c += L::THREADS) {
+        const int el2 = c / (NSP * 2), r = c - el2 * NSP * 2, p = r >> 1, h = r & 1;
+        bool v2;
+        const long long e2 = block_element(a, EB, el2, v2);
+        if (v2) cp_async16(sU + el2 * EU + (p / N1) * RU + (p % N1) * 4 + h * 2, a.U + (e2 * NSP + p) * 4 + h * 2);
+    }
+    cp_async_commit();
+
+    const int role = tid / (EB * N1);            // 0: row (xi-line), 1: column (eta-line)
+    const int rem = tid - role * EB * N1;
+    const int el = rem / N1, line = rem - el * N1;
+    bool valid;
+    const long long e = block_element(a, EB, el, valid);
+    // staged offset of the line's point m: row j -> (m, j), column i -> (i, m)
+    const int ubase = role ? line * 4 : line * RU, ustride = role ? RU : 4;
+    const int jbase = role ? line * 4 : line * RJ, jstride = role ? RJ : 4;
+    // derivative-tile offset of point m: (a, b) -> a*R + b
+    const int tbase = role ? line * R : line, tstride = role ? 1 : R;
+    const int eA = role ? 0 : 1, eB = role ? 2 : 3;
+    const int fA = line, fB = N1 - 1 - line;
+    constexpr bool kRef = UsesRef<T>::value;
+
+    // jumps U_c - U_own = (U_nbr - U_own)/2 at the line's end points
+    T dA[4], dB[4];
+    if (valid) {
+#pragma unroll
+        for (int s2 = 0; s2 < 2; ++s2) {
+            const int ed = s2 ? eB : eA, fp = s2 ? fB : fA;
+            const EdgeRec r = a.edges[e * 4 + ed];
+            T qo[4], qn[4];
+            load4_nc(a.Tin + (e * NFT + ed * N1 + fp) * 4, qo);
+#pragma unroll
+            for (int v = 0; v < 4; ++v) qn[v] = qo[v];
+            if (!(r.flags & kEdgeOrphan)) load4_nc(a.Tin + (neighbour_row(r, a.n_elem) * N1 + (N1 - 1 - fp)) * 4, qn);
+            T* d = s2 ? dB : dA;
+#pragma unroll
+            for (int v = 0; v < 4; ++v) d[v] = (r.flags & kEdgeOrphan) ? T(0) : T(0.5) * (qn[v] - qo[v]);
+        }
+    }
+    cp_async_wait_all();
+    __syncthreads();   // staged states and metrics, operators
+
+    T mine[N1][4];
+    if (valid) {
+        T u[N1][4];
+        const double* su = sU + el * EU;
+        T ue[4];
+        if constexpr (kRef) {
+            double d0[4];
+            load4(su, d0);   // the element's first solution point
+#pragma unroll
+            for (int v = 0; v < 4; ++v) ue[v] = T(d0[v]);
+        }
+#pragma unroll
+        for (int m = 0; m < N1; ++m) {
+            double ud[4];
+            load4(su + ubase + m * ustride, ud);
+            if constexpr (kRef) {
+                // D (U - U_e): the reference drops out of the derivative exactly
+                state_minus_ref(ud, ue, u[m]);
+            } else {
+#pragma unroll
+                for (int v = 0; v < 4; ++v) u[m][v] = T(ud[v]);
+            }
+        }
+        // corrected derivative along the line: sum_k D[m][k] u_k, then
+        // + g1(m) jump_A + g2(m) jump_B (rows: g_R, g_L; columns: g_L, g_R)
+        const T* gL = sOps + N1 * N1 + 2 * N1;
+        const T* gR = gL + N1;
+        const T* g1 = role ? gL : gR;
+        const T* g2 = role ? gR : gL;
+#pragma unroll
+        for (int m = 0; m < N1; ++m) {
+            T Dm[N1];
+            load_op_row<N1>(sOps, m, Dm);
+            const T g1m = g1[m], g2m = g2[m];
+#pragma unroll
+            for (int v = 0; v < 4; ++v) {
+                T acc = T(0);
+#pragma unroll
+                for (int k = 0; k < N1; ++k) acc = fma_any(Dm[k], u[k][v], acc);
+                acc += g1m * dA[v] + g2m * dB[v];
+                mine[m][v] = acc;
+            }
+        }
+        T* sd = sD + el * ES + role * 4 * VB + tbase;
+#pragma unroll
+        for (int m = 0; m < N1; ++m)
+#pragma unroll
+            for (int v = 0; v < 4; ++v) sd[v * VB + m * tstride] = mine[m][v];
+    }
+    __syncthreads();
+    if (!valid) return;
+
+    // Q at the line's points and its traces at the two end points
+    const T* WA = sOps + N1 * N1 + (role ? 0 : N1);   // row: l(+1) at edge 1; column: l(-1) at edge 0
+    const T* WB = sOps + N1 * N1 + (role ? N1 : 0);   // row: l(-1) at edge 3; column: l(+1) at edge 2
+    const T* so = sD + el * ES + (1 - role) * 4 * VB + tbase;
+    const T* sj = sJ + el * EJ + jbase;
+    T tA[8], tB[8];
+#pragma unroll
+    for (int c = 0; c < 8; ++c) { tA[c] = T(0); tB[c] = T(0); }
+#pragma unroll
+    for (int m = 0; m < N1; ++m) {
+        T ji[4];
+        load4(sj + m * jstride, ji);
+        const T wa = WA[m], wb = WB[m];
+#pragma unroll
+        for (int v = 0; v < 4; ++v) {
+            const T other = so[v * VB + m * tstride];
+            const T dxi = role ? other : mine[m][v];
+            const T deta = role ? mine[m][v] : other;
+            const T Qx = ji[0] * dxi + ji[2] * deta;
+            const T Qy = ji[1] * dxi + ji[3] * deta;
+            tA[v] = fma_any(wa, Qx, tA[v]);
+            tA[4 + v] = fma_any(wa, Qy, tA[4 + v]);
+            tB[v] = fma_any(wb, Qx, tB[v]);
+            tB[4 + v] = fma_any(wb, Qy, tB[4 + v]);
+        }
+    }
+    gstore8(a.TQout + (e * NFT + eA * N1 + fA) * 8, tA);
+    gstore8(a.TQout + (e * NFT + eB * N1 + fB) * 8, tB);
 }
 
 template <int P, int RIEM, typename T>
@@ -461,12 +681,25 @@ k_ns_stage(const StageArgsT<T> a) {
 
 template <int P, typename T>
 cudaError_t ns_grad_t(const StageArgsT<T>& a, cudaStream_t s) {
-    using S = Shape<P, EbDiv<T>::value>;
-    const long long grid = ((a.elist ? a.n_list : a.n_elem) + S::EB - 1) / S::EB;
-    if (grid <= 0) return cudaSuccess;
-    static bool set = false;
-    if (!set) { prefer_shared(k_ns_grad<P, T>); set = true; }
-    return launch_programmatic(k_ns_grad<P, T>, (unsigned)grid, S::THREADS, s, a);
+    if constexpr (!IsDual<T>::value) {
+        using L = LineShape<P, T>;
+        const long long grid = ((a.elist ? a.n_list : a.n_elem) + L::EB - 1) / L::EB;
+        if (grid <= 0) return cudaSuccess;
+        static bool set = false;
+        if (!set) {
+            prefer_shared(k_ns_grad_lines<P, T>);
+            cudaFuncSetAttribute(k_ns_grad_lines<P, T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L::SMEM);
+            set = true;
+        }
+        return launch_programmatic_smem(k_ns_grad_lines<P, T>, (unsigned)grid, L::THREADS, L::SMEM, s, a);
+    } else {
+        using S = Shape<P, EbDiv<T>::value>;
+        const long long grid = ((a.elist ? a.n_list : a.n_elem) + S::EB - 1) / S::EB;
+        if (grid <= 0) return cudaSuccess;
+        static bool set = false;
+        if (!set) { prefer_shared(k_ns_grad<P, T>); set = true; }
+        return launch_programmatic(k_ns_grad<P, T>, (unsigned)grid, S::THREADS, s, a);
+    }
 }
 
 template <int P, int RIEM, typename T>

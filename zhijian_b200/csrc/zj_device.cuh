@@ -4,6 +4,7 @@
 #pragma once
 
 #include <cuda_runtime.h>
+#include <type_traits>
 
 #include "zj_math.h"
 
@@ -191,6 +192,19 @@ __device__ __forceinline__ void load_row(const double* row, double* out) {
     if (N & 1) out[N - 1] = row[N - 1];
 }
 
+// Row r of an N1 x N1 operator in a 16-byte aligned table: vector loads
+// when every row starts on a 16-byte boundary, scalar ones otherwise.
+template <int N1, typename T>
+__device__ __forceinline__ void load_op_row(const T* op, int r, T* out) {
+    if constexpr ((std::is_same<T, float>::value || std::is_same<T, double>::value) &&
+                  (N1 * sizeof(T)) % 16 == 0) {
+        load_row<N1>(op + r * N1, out);
+    } else {
+#pragma unroll
+        for (int m = 0; m < N1; ++m) out[m] = op[r * N1 + m];
+    }
+}
+
 // Trace of one flux point from a state held in shared memory as
 // s[var*VS + j*RS + i] (i: xi index, j: eta index).  Edge parametrisations
 // follow FROperators::initQuad (basis.cpp:540-552): edges 0,1 run with +s,
@@ -235,12 +249,12 @@ __device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;"
 // pdl_wait before reading anything a kernel writes) may start while the
 // previous kernel in the stream drains.
 template <typename... KA, typename... AA>
-cudaError_t launch_programmatic(void (*kernel)(KA...), unsigned grid, unsigned threads, cudaStream_t s,
-                                AA&&... args) {
+cudaError_t launch_programmatic_smem(void (*kernel)(KA...), unsigned grid, unsigned threads, size_t smem,
+                                     cudaStream_t s, AA&&... args) {
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3(grid);
     cfg.blockDim = dim3(threads);
-    cfg.dynamicSmemBytes = 0;
+    cfg.dynamicSmemBytes = smem;
     cfg.stream = s;
     cudaLaunchAttribute attr[1];
     attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
@@ -248,6 +262,11 @@ cudaError_t launch_programmatic(void (*kernel)(KA...), unsigned grid, unsigned t
     cfg.attrs = attr;
     cfg.numAttrs = 1;
     return cudaLaunchKernelEx(&cfg, kernel, static_cast<AA&&>(args)...);
+}
+template <typename... KA, typename... AA>
+cudaError_t launch_programmatic(void (*kernel)(KA...), unsigned grid, unsigned threads, cudaStream_t s,
+                                AA&&... args) {
+    return launch_programmatic_smem(kernel, grid, threads, 0, s, static_cast<AA&&>(args)...);
 }
 
 // Trace of one flux point from row `line` of a [var][row][col] tile (weights W
