@@ -135,6 +135,7 @@ struct zj_solver {
     void* dSendBuf = nullptr;
     void* dRecvBuf = nullptr;
     cudaEvent_t ev_pack = nullptr, ev_done = nullptr;
+    cudaEvent_t ev_join = nullptr;   // step graphs of a partition: fork/join of the parts' streams
     double time = 0.0;
     int iter = 0;
     double last_dt = -1.0;
@@ -200,7 +201,8 @@ void free_all(zj_solver* s) {
     s->dSendRows = s->dRecvRows = nullptr; s->dSendBuf = s->dRecvBuf = nullptr;
     if (s->ev_pack) cudaEventDestroy(s->ev_pack);
     if (s->ev_done) cudaEventDestroy(s->ev_done);
-    s->ev_pack = s->ev_done = nullptr;
+    if (s->ev_join) cudaEventDestroy(s->ev_join);
+    s->ev_pack = s->ev_done = s->ev_join = nullptr;
     if (s->own) cudaStreamDestroy(s->own);
     s->own = nullptr;
 }
@@ -691,7 +693,7 @@ zj_status create_impl(const zj_mesh_desc* mesh, const zj_params* params, const i
             e = cudaMemcpy(s->dRecvRows, recv.data(), ni * 4, cudaMemcpyHostToDevice);
         if (e == cudaSuccess) e = cudaEventCreateWithFlags(&s->ev_pack, cudaEventDisableTiming);
         if (e == cudaSuccess) e = cudaEventCreateWithFlags(&s->ev_done, cudaEventDisableTiming);
-        s->graphs_on = false;   // parts step through the multi-part driver
+        if (e == cudaSuccess) e = cudaEventCreateWithFlags(&s->ev_join, cudaEventDisableTiming);
     }
     // every state buffer starts at zero: slots no kernel writes (a
     // triangle's unused ones) stay finite through the buffer rotation
@@ -1699,40 +1701,142 @@ zj_status parts_traces(const std::vector<zj_solver*>& P, const std::vector<const
     return parts_exchange<T>(P, Tb, P[0]->n1 * 4);
 }
 
+// One SSP-RK3 step of every part at their common buffer phase (cur, tpar):
+// three stages with the exchanges between them; the phase advances.
+template <typename T>
+zj_status parts_enqueue_step(const std::vector<zj_solver*>& P) {
+    const size_t n = P.size();
+    std::vector<StageArgsT<T>> A(n);
+    for (int stage = 1; stage <= 3; ++stage) {
+        for (size_t i = 0; i < n; ++i) {
+            zj_solver* s = P[i];
+            const int c = s->cur, a1 = (c + 1) % 3, b1 = (c + 2) % 3, p = s->tpar;
+            StageArgsT<T> a = stage_args<T>(s);
+            a.partials = s->dPart;
+            a.U0 = s->dU[c];
+            a.stage = stage;
+            if (stage == 1) { a.U = s->dU[c]; a.Uout = s->dU[a1]; a.Tin = tbuf<T>(s, p); a.Tout = tbuf<T>(s, 1 - p); }
+            if (stage == 2) { a.U = s->dU[a1]; a.Uout = s->dU[b1]; a.Tin = tbuf<T>(s, 1 - p); a.Tout = tbuf<T>(s, p); }
+            if (stage == 3) { a.U = s->dU[b1]; a.Uout = s->dU[a1]; a.Tin = tbuf<T>(s, p); a.Tout = tbuf<T>(s, 1 - p); }
+            A[i] = a;
+        }
+        zj_status st = parts_stage<T>(P, A);
+        if (st != ZJ_OK) return st;
+    }
+    for (zj_solver* s : P) {
+        s->cur = (s->cur + 1) % 3;
+        s->tpar = 1 - s->tpar;
+    }
+    return ZJ_OK;
+}
+
+// One step of a partition whose parts share a device, as a graph: captured
+// on the rank-0 part's stream with the other parts' streams forked from it
+// and joined back (their kernels, copies and events keep their order inside
+// the graph), one graph per buffer phase, kept on the rank-0 handle.  Parts on
+// several devices, a disabled or failed capture, or a stream the caller is
+// capturing step with plain launches.
+template <typename T>
+cudaGraphExec_t parts_step_graph(const std::vector<zj_solver*>& P) {
+    zj_solver* s0 = P[0];
+    if (!s0->graphs_on || s0->graphs_failed || !s0->stepped) return nullptr;
+    for (zj_solver* s : P)
+        if (s->device != s0->device || s->stream == nullptr) return nullptr;
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    for (zj_solver* s : P)
+        if (cudaStreamIsCapturing(s->stream, &cs) != cudaSuccess || cs != cudaStreamCaptureStatusNone) return nullptr;
+    const int idx = s0->cur * 2 + s0->tpar;
+    if (s0->gexec[idx]) return s0->gexec[idx];
+    std::vector<std::pair<int, int>> phase0;
+    for (zj_solver* s : P) phase0.push_back({s->cur, s->tpar});
+    const std::string err0 = s0->err;
+    if (cudaStreamBeginCapture(s0->stream, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
+        (void)cudaGetLastError();
+        s0->graphs_failed = true;
+        return nullptr;
+    }
+    cudaError_t e = cudaEventRecord(s0->ev_join, s0->stream);
+    for (size_t i = 1; i < P.size() && e == cudaSuccess; ++i) e = cudaStreamWaitEvent(P[i]->stream, s0->ev_join, 0);
+    zj_status st = e == cudaSuccess ? parts_enqueue_step<T>(P) : ZJ_ERR_CUDA;
+    // join every forked stream, also after a failure, so the capture closes
+    for (size_t i = 1; i < P.size(); ++i) {
+        if (cudaEventRecord(P[i]->ev_join, P[i]->stream) == cudaSuccess)
+            (void)cudaStreamWaitEvent(s0->stream, P[i]->ev_join, 0);
+    }
+    cudaGraph_t graph = nullptr;
+    e = cudaStreamEndCapture(s0->stream, &graph);
+    for (size_t i = 0; i < P.size(); ++i) {   // nothing ran: back to the starting phase
+        P[i]->cur = phase0[i].first;
+        P[i]->tpar = phase0[i].second;
+    }
+    cudaGraphExec_t exec = nullptr;
+    if (st == ZJ_OK && e == cudaSuccess && graph) e = cudaGraphInstantiate(&exec, graph, 0);
+    if (graph) cudaGraphDestroy(graph);
+    if (st == ZJ_OK && e == cudaSuccess && exec) e = cudaGraphUpload(exec, s0->stream);
+    if (st != ZJ_OK || e != cudaSuccess || !exec) {
+        (void)cudaGetLastError();
+        if (exec) cudaGraphExecDestroy(exec);
+        s0->err = err0;
+        s0->graphs_failed = true;
+        return nullptr;
+    }
+    s0->gexec[idx] = exec;
+    return exec;
+}
+
 template <typename T>
 zj_status parts_step_t(const std::vector<zj_solver*>& P, double dt, int nsteps) {
     const size_t n = P.size();
-    std::vector<const double*> U(n);
-    std::vector<T*> Tb(n);
-    if (!P[0]->traces_valid) {
+    zj_solver* s0 = P[0];
+    if (!s0->traces_valid) {
+        std::vector<const double*> U(n);
+        std::vector<T*> Tb(n);
         for (size_t i = 0; i < n; ++i) { U[i] = P[i]->dU[P[i]->cur]; Tb[i] = tbuf<T>(P[i], P[i]->tpar); }
         zj_status st = parts_traces<T>(P, U, Tb);
         if (st != ZJ_OK) return st;
         for (zj_solver* s : P) s->traces_valid = true;
     }
-    std::vector<StageArgsT<T>> A(n);
+    const bool first = !s0->stepped;
     for (int step = 0; step < nsteps; ++step) {
-        for (int stage = 1; stage <= 3; ++stage) {
-            for (size_t i = 0; i < n; ++i) {
-                zj_solver* s = P[i];
-                const int c = s->cur, a1 = (c + 1) % 3, b1 = (c + 2) % 3, p = s->tpar;
-                StageArgsT<T> a = stage_args<T>(s);
-                a.partials = s->dPart;
-                a.U0 = s->dU[c];
-                a.stage = stage;
-                if (stage == 1) { a.U = s->dU[c]; a.Uout = s->dU[a1]; a.Tin = tbuf<T>(s, p); a.Tout = tbuf<T>(s, 1 - p); }
-                if (stage == 2) { a.U = s->dU[a1]; a.Uout = s->dU[b1]; a.Tin = tbuf<T>(s, 1 - p); a.Tout = tbuf<T>(s, p); }
-                if (stage == 3) { a.U = s->dU[b1]; a.Uout = s->dU[a1]; a.Tin = tbuf<T>(s, p); a.Tout = tbuf<T>(s, 1 - p); }
-                A[i] = a;
+        cudaGraphExec_t g = parts_step_graph<T>(P);
+        if (g) {
+            // the graph runs on the rank-0 stream after every part's queued
+            // work; the parts' streams continue after it
+            ZJ_CK(s0, cudaSetDevice(s0->device), "set device");
+            for (size_t i = 1; i < n; ++i) {
+                ZJ_CK(P[i], cudaEventRecord(P[i]->ev_join, P[i]->stream), "join event");
+                ZJ_CK(s0, cudaStreamWaitEvent(s0->stream, P[i]->ev_join, 0), "join wait");
             }
-            zj_status st = parts_stage<T>(P, A);
+            ZJ_CK(s0, cudaGraphLaunch(g, s0->stream), "partition step graph launch");
+            ZJ_CK(s0, cudaEventRecord(s0->ev_join, s0->stream), "fork event");
+            for (size_t i = 1; i < n; ++i) ZJ_CK(P[i], cudaStreamWaitEvent(P[i]->stream, s0->ev_join, 0), "fork wait");
+            for (zj_solver* s : P) {
+                s->cur = (s->cur + 1) % 3;
+                s->tpar = 1 - s->tpar;
+            }
+        } else {
+            zj_status st = parts_enqueue_step<T>(P);
             if (st != ZJ_OK) return st;
+            s0->stepped = true;
         }
         for (zj_solver* s : P) {
-            s->cur = (s->cur + 1) % 3;
-            s->tpar = 1 - s->tpar;
             s->time += dt;
             s->iter += 1;
+        }
+    }
+    if (first) {
+        // capture (without running) the graphs of all six phases now, so
+        // later calls only launch them
+        std::vector<std::pair<int, int>> phase0;
+        for (zj_solver* s : P) phase0.push_back({s->cur, s->tpar});
+        for (int c = 0; c < 3 && !s0->graphs_failed; ++c)
+            for (int p = 0; p < 2 && !s0->graphs_failed; ++p) {
+                for (zj_solver* s : P) { s->cur = c; s->tpar = p; }
+                (void)parts_step_graph<T>(P);
+            }
+        for (size_t i = 0; i < n; ++i) {
+            P[i]->cur = phase0[i].first;
+            P[i]->tpar = phase0[i].second;
         }
     }
     for (zj_solver* s : P) s->has_norm = true;
