@@ -73,3 +73,40 @@ def test_a_part_refuses_single_handle_stepping(zjlib):
     with pytest.raises(L.ZJError) as e:
         PT.PartitionedSolver(mesh, make_params(poly_order=2, compat=True, bcs=[(1, "slipwall")], **KW), 2)
     assert e.value.code == L.ERR_UNSUPPORTED
+
+
+def test_parts_step_graphs_match_plain_launches(zjlib):
+    """The step graphs of a one-device partition replay exactly what the plain
+    launches do (graphs off through the rank-0 part)."""
+    mesh = M.tgv_mesh(16, seed=3)
+    prm = make_params(poly_order=3, rho_inf=1.0, p_inf=1.0 / (1.4 * 0.09), Mach=0.3, riemann="HLLC",
+                      compat=False, viscous=True, Re=2000.0, Pr=0.72, bcs=[(1, "slipwall")], precision="mixed")
+    runs = []
+    for graphs in (True, False):
+        parts = PT.PartitionedSolver(mesh, prm, 3)
+        if not graphs:
+            assert zjlib.zj_set_step_graphs(parts.parts[0].h, 0) == L.OK
+        parts.copyToDevice(M.taylor_green(parts.solution_point_coords()))
+        parts.advance(1e-4, 2)
+        parts.advance(1e-4, 9)      # every buffer phase, graphs captured after the first call
+        runs.append((parts.copyToHost(), parts.computeResidual()))
+        parts.close()
+    assert np.array_equal(runs[0][0], runs[1][0])
+    assert runs[0][1] == runs[1][1]
+
+
+def test_device_arrays_must_be_32_byte_aligned(zjlib):
+    import torch
+    mesh = M.tgv_mesh(8, seed=1)
+    s = FRSolver(mesh, make_params(poly_order=2, compat=False, bcs=[(1, "slipwall")], **KW))
+    n = s.n_elem * s.n_sp * 4
+    buf = torch.zeros(2 * n + 8, dtype=torch.float64, device="cuda")
+    base = buf.data_ptr()
+    assert base % 256 == 0
+    U, R = base, base + 8 * (n + 4)          # both 32-byte aligned
+    assert zjlib.zj_rhs(s.h, C.c_void_p(U), C.c_void_p(R)) == L.OK
+    for off in (8, 16):                          # 8- and 16-byte aligned: refused before any launch
+        assert zjlib.zj_rhs(s.h, C.c_void_p(U + off), C.c_void_p(R)) == L.ERR_ARG
+        assert zjlib.zj_rhs(s.h, C.c_void_p(U), C.c_void_p(R + off)) == L.ERR_ARG
+    torch.cuda.synchronize()
+    s.close()
