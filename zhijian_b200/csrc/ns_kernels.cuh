@@ -44,7 +44,7 @@
 #define ZJ_NSG32_MIN_BLOCKS 6     // mixed-precision gradient kernel (40 registers)
 #endif
 #ifndef ZJ_NSL_MIN_BLOCKS
-#define ZJ_NSL_MIN_BLOCKS 4       // FP64 gradient kernel by lines (per 128 threads)
+#define ZJ_NSL_MIN_BLOCKS 4       // FP64 gradient kernel by lines (CTAs of 128 threads)
 #endif
 #ifndef ZJ_NSL32_MIN_BLOCKS
 #define ZJ_NSL32_MIN_BLOCKS 6     // mixed-precision gradient kernel by lines
@@ -287,7 +287,9 @@ struct LineShape {
     static_assert(OFF_J % 16 == 0 && OFF_D % 16 == 0 && OFF_OPS % 16 == 0, "16-byte aligned regions");
     // A line thread holds a line's states and derivatives: twice the values
     // of a point thread, at half the threads per element.
-    static constexpr int MIN_BLOCKS = sizeof(T) == 8 ? ZJ_NSL_MIN_BLOCKS : ZJ_NSL32_MIN_BLOCKS;
+    // (the counts are per 128 threads; other CTA sizes scale them)
+    static constexpr int MIN_BLOCKS_128 = sizeof(T) == 8 ? ZJ_NSL_MIN_BLOCKS : ZJ_NSL32_MIN_BLOCKS;
+    static constexpr int MIN_BLOCKS = MIN_BLOCKS_128 * 128 / kCtaThreads > 0 ? MIN_BLOCKS_128 * 128 / kCtaThreads : 1;
 };
 
 // 16-byte asynchronous global -> shared copy (cp.async, cached in L2 only),
