@@ -234,7 +234,7 @@ void* zj_get_stream(const zj_solver* s);
 #define ZJ_NOALLOC_SCRATCH_BYTES (32u * 1024u * 1024u)
 zj_status zj_rhs_noalloc(zj_solver* s, const double* U_dev, double* R_dev);
 
-/* ---- mesh partitions (several GPUs) -----------------------------
+/* ---- mesh partitions (several GPUs) ----------------------------------------
  * Replace MeshPartitioner::partition (src/mesh/partitioner.cpp:10-93, METIS
  * k-way on the element dual graph) and MPICommunicator::exchangeHalo
  * (src/parallel/mpi_comm.cpp:68-171).  A partitioned mesh runs as one handle

@@ -4,7 +4,8 @@
 // state, the RK accumulation and the norm partials stay FP64).  Two launches
 // per residual:
 //
-//  k_ns_grad   corrected gradient Q = grad U at the solution points and its
+//  k_ns_grad_lines (float, double; k_ns_grad for dual numbers)
+//              corrected gradient Q = grad U at the solution points and its
 //              traces at the flux points (written for the neighbours);
 //  k_ns_stage  recomputes Q at the solution points, total flux F - F_v, the
 //              common flux = Riemann(U_L, U_R) - F_v(avg U, avg Q).n, FR
