@@ -32,17 +32,25 @@
 #include "zj_physics.cuh"
 #include "phys_kernels.cuh"
 
+// Resident CTAs per SM the launch bounds ask for, counted in CTAs of 128
+// threads (other CTA sizes scale them).
 #ifndef ZJ_NS_MIN_BLOCKS
-#define ZJ_NS_MIN_BLOCKS 2        // FP64 stage kernel (per 256 threads)
+#define ZJ_NS_MIN_BLOCKS 5        // FP64 stage kernel (96 registers)
 #endif
 #ifndef ZJ_NSG_MIN_BLOCKS
-#define ZJ_NSG_MIN_BLOCKS 4       // FP64 gradient kernel
+#define ZJ_NSG_MIN_BLOCKS 8       // FP64 point-per-thread gradient kernel
 #endif
 #ifndef ZJ_NS32_MIN_BLOCKS
-#define ZJ_NS32_MIN_BLOCKS 4      // mixed-precision stage kernel (64 registers)
+#define ZJ_NS32_MIN_BLOCKS 10     // mixed-precision stage kernel (48 registers)
 #endif
 #ifndef ZJ_NSG32_MIN_BLOCKS
-#define ZJ_NSG32_MIN_BLOCKS 6     // mixed-precision gradient kernel (40 registers)
+#define ZJ_NSG32_MIN_BLOCKS 12    // mixed-precision point-per-thread gradient kernel
+#endif
+#ifndef ZJ_NS_MIN_BLOCKS_HI
+#define ZJ_NS_MIN_BLOCKS_HI 4     // FP64 stage kernel from P4 up (fewer spills)
+#endif
+#ifndef ZJ_NS32_MIN_BLOCKS_HI
+#define ZJ_NS32_MIN_BLOCKS_HI 8   // mixed-precision stage kernel from P4 up
 #endif
 #ifndef ZJ_NSL_MIN_BLOCKS
 #define ZJ_NSL_MIN_BLOCKS 4       // FP64 gradient kernel by lines (CTAs of 128 threads)
@@ -57,15 +65,17 @@ namespace {
 using namespace dev;
 using namespace phys;
 
-template <typename T> struct NSMinBlocks;
-// Minimum resident blocks of 256 threads, scaled to the CTA size.
-template <> struct NSMinBlocks<double> {
-    static constexpr int stage = ZJ_NS_MIN_BLOCKS * kCtaScale, grad = ZJ_NSG_MIN_BLOCKS * kCtaScale;
+template <typename T, int P> struct NSMinBlocks;
+constexpr int per_cta(int blocks128) { return blocks128 * 128 / kCtaThreads > 0 ? blocks128 * 128 / kCtaThreads : 1; }
+template <int P> struct NSMinBlocks<double, P> {
+    static constexpr int stage = per_cta(P <= 3 ? ZJ_NS_MIN_BLOCKS : ZJ_NS_MIN_BLOCKS_HI);
+    static constexpr int grad = per_cta(ZJ_NSG_MIN_BLOCKS);
 };
-template <> struct NSMinBlocks<float> {
-    static constexpr int stage = ZJ_NS32_MIN_BLOCKS * kCtaScale, grad = ZJ_NSG32_MIN_BLOCKS * kCtaScale;
+template <int P> struct NSMinBlocks<float, P> {
+    static constexpr int stage = per_cta(P <= 3 ? ZJ_NS32_MIN_BLOCKS : ZJ_NS32_MIN_BLOCKS_HI);
+    static constexpr int grad = per_cta(ZJ_NSG32_MIN_BLOCKS);
 };
-template <> struct NSMinBlocks<Dual> { static constexpr int stage = 1, grad = 1; };
+template <int P> struct NSMinBlocks<Dual, P> { static constexpr int stage = 1, grad = 1; };
 
 // Corrected gradient at solution point (i, j) of one element: su is the
 // element's state in the [var][row][col] shared layout, du its face jumps
@@ -163,7 +173,7 @@ __device__ __forceinline__ void load_face_point(const StageArgsT<T>& a, long lon
 }
 
 template <int P, typename T>
-__global__ void __launch_bounds__(Shape<P, EbDiv<T>::value>::THREADS, NSMinBlocks<T>::grad)
+__global__ void __launch_bounds__(Shape<P, EbDiv<T>::value>::THREADS, NSMinBlocks<T, P>::grad)
 k_ns_grad(const StageArgsT<T> a) {
     using S = Shape<P, EbDiv<T>::value>;
     constexpr int N1 = S::N1, NSP = S::NSP, NFT = S::NFT, TPE = S::TPE, EB = S::EB;
@@ -452,7 +462,7 @@ k_ns_grad_lines(const StageArgsT<T> a) {
 }
 
 template <int P, int RIEM, typename T>
-__global__ void __launch_bounds__(Shape<P, EbDiv<T>::value>::THREADS, NSMinBlocks<T>::stage)
+__global__ void __launch_bounds__(Shape<P, EbDiv<T>::value>::THREADS, NSMinBlocks<T, P>::stage)
 k_ns_stage(const StageArgsT<T> a) {
     using S = Shape<P, EbDiv<T>::value>;
     constexpr int N1 = S::N1, NSP = S::NSP, NFT = S::NFT, TPE = S::TPE, EB = S::EB;
@@ -466,6 +476,11 @@ k_ns_stage(const StageArgsT<T> a) {
     __shared__ __align__(16) T sD[EB * DS];   // face jumps of U, then flux differences
     __shared__ __align__(16) T sU[EB * FS];   // stage state, then the new state
     __shared__ double sRed[32];
+    // A flux-point thread's face data from the loads to the face phase, parked
+    // here (component-major: a warp's accesses fill consecutive banks) so
+    // that it holds no registers through the volume phase: own and neighbour
+    // traces (4 + 4) and the average gradient trace (8).
+    __shared__ T sFP[16 * S::THREADS];
 
     const int tid = threadIdx.x;
     for (int t = tid; t < S::NOPS; t += blockDim.x) sOps[t] = a.ops[t];
@@ -481,8 +496,9 @@ k_ns_stage(const StageArgsT<T> a) {
 
     // ---- A1: loads, face jumps, stage state into shared memory
     FacePoint<T> f;
-    T Qo[8], Qn[8];
+    T* pk = sFP + tid;   // this thread's parked face data, stride S::THREADS
     if (is_fp) {
+        T Qo[8], Qn[8];
         load_face_point<N1>(a, e, edge, fp, f);
         const T* qt = a.TQ + (e * NFT + k) * 8;
         gload8_nc(qt, Qo);
@@ -496,6 +512,13 @@ k_ns_stage(const StageArgsT<T> a) {
 #pragma unroll
         for (int v = 0; v < 4; ++v) d[v] = (f.r.flags & kEdgeOrphan) ? T(0) : T(0.5) * (f.qn[v] - f.qo[v]);
         store4(sD + el * DS + k * 4, d);
+#pragma unroll
+        for (int v = 0; v < 4; ++v) {
+            pk[v * S::THREADS] = f.qo[v];
+            pk[(4 + v) * S::THREADS] = f.qn[v];
+        }
+#pragma unroll
+        for (int v = 0; v < 8; ++v) pk[(8 + v) * S::THREADS] = T(0.5) * (Qo[v] + Qn[v]);
     }
     constexpr bool kRef = UsesRef<T>::value;
     T ue[4] = {T(0), T(0), T(0), T(0)};   // reference state (mixed form)
@@ -551,6 +574,11 @@ k_ns_stage(const StageArgsT<T> a) {
     if (is_fp) {
         T Fd[4] = {T(0), T(0), T(0), T(0)};
         if (!(f.r.flags & kEdgeOrphan)) {
+#pragma unroll
+            for (int v = 0; v < 4; ++v) {
+                f.qo[v] = pk[v * S::THREADS];
+                f.qn[v] = pk[(4 + v) * S::THREADS];
+            }
             const bool right = (f.r.flags & kEdgeRight) != 0;
             T UL[4], UR[4], Fc[4];
 #pragma unroll
@@ -566,8 +594,8 @@ k_ns_stage(const StageArgsT<T> a) {
 #pragma unroll
             for (int v = 0; v < 4; ++v) {
                 Ua[v] = T(0.5) * (UL[v] + UR[v]);
-                dxa[v] = T(0.5) * (Qo[v] + Qn[v]);
-                dya[v] = T(0.5) * (Qo[4 + v] + Qn[4 + v]);
+                dxa[v] = pk[(8 + v) * S::THREADS];
+                dya[v] = pk[(12 + v) * S::THREADS];
             }
             viscous_flux_f(Ua, rcp_any(Ua[0]), dxa, dya, g, inv_reynolds(a), T(a.kfac), Fv, Gv);
             T Fvn[4];
