@@ -53,7 +53,10 @@
 #define ZJ_NS32_MIN_BLOCKS_HI 8   // mixed-precision stage kernel from P4 up
 #endif
 #ifndef ZJ_NSL_MIN_BLOCKS
-#define ZJ_NSL_MIN_BLOCKS 4       // FP64 gradient kernel by lines (CTAs of 128 threads)
+#define ZJ_NSL_MIN_BLOCKS 5       // FP64 gradient kernel by lines (96 registers)
+#endif
+#ifndef ZJ_NSL_MIN_BLOCKS_HI
+#define ZJ_NSL_MIN_BLOCKS_HI 4    // the same from P4 up (no spills)
 #endif
 #ifndef ZJ_NSL32_MIN_BLOCKS
 #define ZJ_NSL32_MIN_BLOCKS 6     // mixed-precision gradient kernel by lines
@@ -299,7 +302,8 @@ struct LineShape {
     // A line thread holds a line's states and derivatives: twice the values
     // of a point thread, at half the threads per element.
     // (the counts are per 128 threads; other CTA sizes scale them)
-    static constexpr int MIN_BLOCKS_128 = sizeof(T) == 8 ? ZJ_NSL_MIN_BLOCKS : ZJ_NSL32_MIN_BLOCKS;
+    static constexpr int MIN_BLOCKS_128 =
+        sizeof(T) == 8 ? (P <= 3 ? ZJ_NSL_MIN_BLOCKS : ZJ_NSL_MIN_BLOCKS_HI) : ZJ_NSL32_MIN_BLOCKS;
     static constexpr int MIN_BLOCKS = MIN_BLOCKS_128 * 128 / kCtaThreads > 0 ? MIN_BLOCKS_128 * 128 / kCtaThreads : 1;
 };
 
