@@ -270,8 +270,12 @@ zj_status zj_solver_create_part(const zj_mesh_desc* mesh, const zj_params* param
 zj_status zj_part_elements(const zj_solver* s, int64_t* global_ids);
 /* All n parts of one partition from one process (any order; each on its own
  * device and stream, ordered by events): nsteps SSP-RK3 steps, one residual
- * of the device states U_dev[rank] into R_dev[rank], synchronisation, and the
- * L2 norm of the last stage's residual over all parts. */
+ * of the device states U_dev[rank] into R_dev[rank] (32-byte aligned),
+ * synchronisation, and the L2 norm of the last stage's residual over all
+ * parts.  When every part is on one device, zj_parts_step replays one CUDA
+ * graph per step after its first call (captured on the rank-0 part's stream
+ * with the others forked from it); zj_set_step_graphs(rank-0 part, 0) turns
+ * that off. */
 zj_status zj_parts_step(zj_solver* const* parts, int n, double dt, int nsteps);
 zj_status zj_parts_rhs(zj_solver* const* parts, int n, const double* const* U_dev, double* const* R_dev);
 zj_status zj_parts_synchronize(zj_solver* const* parts, int n);
