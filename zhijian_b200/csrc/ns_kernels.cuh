@@ -47,10 +47,10 @@
 #define ZJ_NSG32_MIN_BLOCKS 12    // mixed-precision point-per-thread gradient kernel
 #endif
 #ifndef ZJ_NS_MIN_BLOCKS_HI
-#define ZJ_NS_MIN_BLOCKS_HI 4     // FP64 stage kernel from P4 up (fewer spills)
+#define ZJ_NS_MIN_BLOCKS_HI 4     // FP64 stage kernel at P5 (fewer spills)
 #endif
 #ifndef ZJ_NS32_MIN_BLOCKS_HI
-#define ZJ_NS32_MIN_BLOCKS_HI 8   // mixed-precision stage kernel from P4 up
+#define ZJ_NS32_MIN_BLOCKS_HI 8   // mixed-precision stage kernel at P5
 #endif
 #ifndef ZJ_NSL_MIN_BLOCKS
 #define ZJ_NSL_MIN_BLOCKS 5       // FP64 gradient kernel by lines (96 registers)
@@ -71,11 +71,11 @@ using namespace phys;
 template <typename T, int P> struct NSMinBlocks;
 constexpr int per_cta(int blocks128) { return blocks128 * 128 / kCtaThreads > 0 ? blocks128 * 128 / kCtaThreads : 1; }
 template <int P> struct NSMinBlocks<double, P> {
-    static constexpr int stage = per_cta(P <= 3 ? ZJ_NS_MIN_BLOCKS : ZJ_NS_MIN_BLOCKS_HI);
+    static constexpr int stage = per_cta(P <= 4 ? ZJ_NS_MIN_BLOCKS : ZJ_NS_MIN_BLOCKS_HI);
     static constexpr int grad = per_cta(ZJ_NSG_MIN_BLOCKS);
 };
 template <int P> struct NSMinBlocks<float, P> {
-    static constexpr int stage = per_cta(P <= 3 ? ZJ_NS32_MIN_BLOCKS : ZJ_NS32_MIN_BLOCKS_HI);
+    static constexpr int stage = per_cta(P <= 4 ? ZJ_NS32_MIN_BLOCKS : ZJ_NS32_MIN_BLOCKS_HI);
     static constexpr int grad = per_cta(ZJ_NSG32_MIN_BLOCKS);
 };
 template <int P> struct NSMinBlocks<Dual, P> { static constexpr int stage = 1, grad = 1; };
