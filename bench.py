@@ -710,9 +710,10 @@ def partition_case(mesh, args, nparts=4, mode="ns32"):
     """The headline workload split into `nparts` RCB parts on this one GPU and
     stepped by the multi-part driver (each part on its own stream; after each
     launch that writes traces the cut-face rows are gathered, copied into the
-    neighbours' buffers and scattered into their ghost rows): DOF-RHS/s and
-    its ratio to the whole-mesh handle on the same GPU.  It measures the cost
-    of the exchange machinery, not a link: every copy stays on one device."""
+    neighbours' buffers and scattered into their ghost rows; one captured
+    graph per step once the first call has run): DOF-RHS/s and its ratio to
+    the whole-mesh handle on the same GPU.  It measures the cost of the
+    exchange machinery, not a link: every copy stays on one device."""
     import torch
     from zhijian_b200 import meshgen as M
     from zhijian_b200.partition import PartitionedSolver
