@@ -280,6 +280,27 @@ zj_status zj_parts_step(zj_solver* const* parts, int n, double dt, int nsteps);
 zj_status zj_parts_rhs(zj_solver* const* parts, int n, const double* const* U_dev, double* const* R_dev);
 zj_status zj_parts_synchronize(zj_solver* const* parts, int n);
 zj_status zj_parts_residual_norm(zj_solver* const* parts, int n, double* out);
+/* One process per GPU (the caller's MPI or NCCL moves the rows; the
+ * reference's MPICommunicator::exchangeHalo, mpi_comm.cpp:68-171): nsteps
+ * SSP-RK3 steps of the part s alone, on its stream.  At each exchange (the
+ * state traces before the first step, then per stage the gradient traces
+ * after the gradient launch (Navier-Stokes) and the new traces after the
+ * stage launch) the part's cut-face rows are gathered into send_dev, in the
+ * halo plan's order (zj_halo_plan: rows [nbr_off[i], nbr_off[i+1]) for
+ * neighbour nbr[i]; row_bytes bytes each), and exchange(user, kind,
+ * row_bytes, send_dev, recv_dev, stream) is called on this host thread.  It
+ * must fill recv_dev, in the same layout, with the rows every neighbour sent
+ * for this part: complete when it returns, or ordered before work enqueued on
+ * `stream` after it (NCCL sends and receives on that stream).  send_dev is
+ * written by work queued on `stream` before the call.  Nonzero from exchange
+ * stops the step with ZJ_ERR_IO.  The parts' residual norms combine as
+ * sqrt(sum of zj_residual_norm(part)^2), their time steps as the minimum of
+ * zj_compute_dt over the parts; every part must call zj_part_step with the same
+ * dt and nsteps. */
+enum { ZJ_XCHG_TRACES = 1, ZJ_XCHG_GRADIENTS = 2 };
+typedef int (*zj_exchange_fn)(void* user, int kind, int row_bytes, const void* send_dev, void* recv_dev,
+                              void* stream);
+zj_status zj_part_step(zj_solver* s, double dt, int nsteps, zj_exchange_fn exchange, void* user);
 
 /* ---- differentiation (physics mode, FP64) ----------------------------------
  * No reference counterpart: the reference has no adjoint.  All pointers are

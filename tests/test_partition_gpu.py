@@ -110,3 +110,60 @@ def test_device_arrays_must_be_32_byte_aligned(zjlib):
         assert zjlib.zj_rhs(s.h, C.c_void_p(U), C.c_void_p(R + off)) == L.ERR_ARG
     torch.cuda.synchronize()
     s.close()
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_one_part_per_thread_with_a_caller_transport(zjlib, precision):
+    """zj_part_step: each part stepped alone by its own host thread, its cut-face
+    rows moved by the caller's transport (LocalExchange: one process, one
+    device; nccl_exchange is the same contract over torch.distributed), equals
+    the whole mesh bit for bit."""
+    import threading
+    mesh = M.tgv_mesh(16, seed=5)
+    prm = make_params(poly_order=3, rho_inf=1.0, p_inf=1.0 / (1.4 * 0.09), Mach=0.3, riemann="Roe",
+                      compat=False, viscous=True, Re=3000.0, Pr=0.72, bcs=[(1, "slipwall")], precision=precision)
+    whole = FRSolver(mesh, prm)
+    U0 = M.taylor_green(whole.solution_point_coords())
+    whole.copyToDevice(U0)
+    dt = whole.computeTimeStep()
+    whole.advance(dt, 5)
+    part = PT.partition(mesh, 3)
+    procs = [PT.PartProcess(mesh, prm, part, r) for r in range(3)]
+    xchg = PT.LocalExchange([p.plan for p in procs])
+    for p in procs:
+        p.copyToDevice(U0)
+    errors = []
+
+    def run(r):
+        try:
+            procs[r].advance(dt, 2, xchg.for_rank(r))
+            procs[r].advance(dt, 3, xchg.for_rank(r))
+        except Exception as e:
+            errors.append(e)
+    threads = [threading.Thread(target=run, args=(r,)) for r in range(3)]
+    for t in threads:
+        t.start()
+    for t in threads:
+        t.join(timeout=300)
+    assert not errors, errors
+    out = np.empty_like(U0)
+    for p in procs:
+        out[p.elems] = p.copyToHost()
+    assert np.array_equal(out, whole.copyToHost())
+    norms = [p.solver.computeResidual() for p in procs]
+    assert abs(np.sqrt(sum(n * n for n in norms)) - whole.computeResidual()) <= 1e-13 * whole.computeResidual()
+    for p in procs:
+        p.close()
+
+
+def test_part_step_reports_a_failed_transport(zjlib):
+    mesh = M.tgv_mesh(8, seed=1)
+    prm = make_params(poly_order=2, compat=False, bcs=[(1, "slipwall")], **KW)
+    part = PT.partition(mesh, 2)
+    p = PT.PartProcess(mesh, prm, part, 0)
+    p.copyToDevice(M.random_state(mesh.n_elem, 9, 3, 1.4, 1.2, 1.0e5, 0.05))
+    with pytest.raises(RuntimeError):
+        p.advance(1e-6, 1, lambda *args: (_ for _ in ()).throw(RuntimeError("link down")))
+    failing = L.EXCHANGE_FN(lambda *args: 3)
+    assert zjlib.zj_part_step(p.solver.h, 1e-6, 1, failing, None) == L.ERR_IO
+    p.close()

@@ -41,6 +41,12 @@ class Params(C.Structure):
                 ("n_bc", C.c_int), ("bc", BCSpec * MAX_BC)]
 
 
+# int exchange(void* user, int kind, int row_bytes, const void* send_dev,
+#              void* recv_dev, void* stream): the transport of zj_part_step
+EXCHANGE_FN = C.CFUNCTYPE(C.c_int, C.c_void_p, C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p)
+XCHG_TRACES, XCHG_GRADIENTS = 1, 2
+
+
 class MeshDesc(C.Structure):
     _fields_ = [("n_nodes", C.c_int64), ("xy", C.POINTER(C.c_double)),
                 ("n_elem", C.c_int64), ("elem_type", C.POINTER(C.c_int32)),
@@ -121,6 +127,7 @@ def lib():
         "zj_parts_rhs": (ip, [C.POINTER(vp), ip, C.POINTER(vp), C.POINTER(vp)]),
         "zj_parts_synchronize": (ip, [C.POINTER(vp), ip]),
         "zj_parts_residual_norm": (ip, [C.POINTER(vp), ip, dp]),
+        "zj_part_step": (ip, [vp, C.c_double, ip, EXCHANGE_FN, vp]),
     }
     for name, (res, args) in sig.items():
         f = getattr(h, name)

@@ -1651,6 +1651,22 @@ T* grad_buf(const zj_solver* s);
 template <> double* grad_buf<double>(const zj_solver* s) { return s->dTQ; }
 template <> float* grad_buf<float>(const zj_solver* s) { return s->fTQ; }
 
+// The stage launch of a part (physics mode, quadrilaterals): the
+// Navier-Stokes stage after its gradient traces crossed, else the inviscid
+// stage.
+template <typename T>
+cudaError_t launch_part_stage(zj_solver* s, const StageArgsT<T>& a) {
+    if (!is_ns(s)) return launch_phys_stage(s->P, s->prm.riemann, a, s->stream);
+    if constexpr (sizeof(T) == 4) {
+        if (s->tc) {
+            StageArgsT<T> t = a;
+            t.tc_err = s->dTcErr;
+            return launch_ns_stage_tc(s->P, s->prm.riemann, t, &s->tc_map, s->stream);
+        }
+    }
+    return launch_ns_stage(s->P, s->prm.riemann, a, s->stream);
+}
+
 // One residual (stage 0) or SSP-RK3 stage of every part: for Navier-Stokes
 // the gradient launches, their gradient traces across the cuts, then the
 // stage launches; a stage's new traces cross after it.
@@ -1671,21 +1687,7 @@ zj_status parts_stage(const std::vector<zj_solver*>& P, const std::vector<StageA
     for (size_t i = 0; i < P.size(); ++i) {
         zj_solver* s = P[i];
         ZJ_CK(s, cudaSetDevice(s->device), "set device");
-        cudaError_t e;
-        if (!ns) {
-            e = launch_phys_stage(s->P, s->prm.riemann, A[i], s->stream);
-        } else if constexpr (sizeof(T) == 4) {
-            if (s->tc) {
-                StageArgsT<T> t = A[i];
-                t.tc_err = s->dTcErr;
-                e = launch_ns_stage_tc(s->P, s->prm.riemann, t, &s->tc_map, s->stream);
-            } else {
-                e = launch_ns_stage(s->P, s->prm.riemann, A[i], s->stream);
-            }
-        } else {
-            e = launch_ns_stage(s->P, s->prm.riemann, A[i], s->stream);
-        }
-        ZJ_CK(s, e, "stage launch");
+        ZJ_CK(s, launch_part_stage<T>(s, A[i]), "stage launch");
         out.push_back(const_cast<T*>(A[i].Tout));
     }
     if (A[0].stage == 0) return ZJ_OK;
@@ -1703,23 +1705,26 @@ zj_status parts_traces(const std::vector<zj_solver*>& P, const std::vector<const
 
 // One SSP-RK3 step of every part at their common buffer phase (cur, tpar):
 // three stages with the exchanges between them; the phase advances.
+// Launch arguments of SSP-RK3 stage `stage` of a part at its buffer phase.
+template <typename T>
+StageArgsT<T> part_stage_args(zj_solver* s, int stage) {
+    const int c = s->cur, a1 = (c + 1) % 3, b1 = (c + 2) % 3, p = s->tpar;
+    StageArgsT<T> a = stage_args<T>(s);
+    a.partials = s->dPart;
+    a.U0 = s->dU[c];
+    a.stage = stage;
+    if (stage == 1) { a.U = s->dU[c]; a.Uout = s->dU[a1]; a.Tin = tbuf<T>(s, p); a.Tout = tbuf<T>(s, 1 - p); }
+    if (stage == 2) { a.U = s->dU[a1]; a.Uout = s->dU[b1]; a.Tin = tbuf<T>(s, 1 - p); a.Tout = tbuf<T>(s, p); }
+    if (stage == 3) { a.U = s->dU[b1]; a.Uout = s->dU[a1]; a.Tin = tbuf<T>(s, p); a.Tout = tbuf<T>(s, 1 - p); }
+    return a;
+}
+
 template <typename T>
 zj_status parts_enqueue_step(const std::vector<zj_solver*>& P) {
     const size_t n = P.size();
     std::vector<StageArgsT<T>> A(n);
     for (int stage = 1; stage <= 3; ++stage) {
-        for (size_t i = 0; i < n; ++i) {
-            zj_solver* s = P[i];
-            const int c = s->cur, a1 = (c + 1) % 3, b1 = (c + 2) % 3, p = s->tpar;
-            StageArgsT<T> a = stage_args<T>(s);
-            a.partials = s->dPart;
-            a.U0 = s->dU[c];
-            a.stage = stage;
-            if (stage == 1) { a.U = s->dU[c]; a.Uout = s->dU[a1]; a.Tin = tbuf<T>(s, p); a.Tout = tbuf<T>(s, 1 - p); }
-            if (stage == 2) { a.U = s->dU[a1]; a.Uout = s->dU[b1]; a.Tin = tbuf<T>(s, 1 - p); a.Tout = tbuf<T>(s, p); }
-            if (stage == 3) { a.U = s->dU[b1]; a.Uout = s->dU[a1]; a.Tin = tbuf<T>(s, p); a.Tout = tbuf<T>(s, 1 - p); }
-            A[i] = a;
-        }
+        for (size_t i = 0; i < n; ++i) A[i] = part_stage_args<T>(P[i], stage);
         zj_status st = parts_stage<T>(P, A);
         if (st != ZJ_OK) return st;
     }
@@ -1843,6 +1848,58 @@ zj_status parts_step_t(const std::vector<zj_solver*>& P, double dt, int nsteps) 
     return ZJ_OK;
 }
 
+// ---- one process per GPU: a part stepped alone; at each exchange its
+// cut-face rows go to the caller's transport and come back as ghost rows
+
+template <typename T>
+zj_status part_exchange_cb(zj_solver* s, T* buf, int w, int kind, zj_exchange_fn fn, void* user) {
+    const int threads = 256;
+    const long long ni = (long long)s->part.mine.size();
+    if (ni > 0) {
+        k_rows_gather<T><<<(unsigned)((ni * w + threads - 1) / threads), threads, 0, s->stream>>>(
+            buf, s->dSendRows, ni, w, static_cast<T*>(s->dSendBuf));
+        ZJ_CK(s, cudaGetLastError(), "halo gather");
+    }
+    const int rc = fn(user, kind, (int)(w * sizeof(T)), s->dSendBuf, s->dRecvBuf, static_cast<void*>(s->stream));
+    if (rc != 0) return fail(s, ZJ_ERR_IO, "the exchange callback returned " + std::to_string(rc));
+    if (ni > 0) {
+        k_rows_scatter<T><<<(unsigned)((ni * w + threads - 1) / threads), threads, 0, s->stream>>>(
+            static_cast<const T*>(s->dRecvBuf), s->dRecvRows, ni, w, buf);
+        ZJ_CK(s, cudaGetLastError(), "halo scatter");
+    }
+    return ZJ_OK;
+}
+
+template <typename T>
+zj_status part_step_t(zj_solver* s, int nsteps, zj_exchange_fn fn, void* user, double dt) {
+    zj_status st = ZJ_OK;
+    if (!s->traces_valid) {
+        T* tb = tbuf<T>(s, s->tpar);
+        ZJ_CK(s, launch_trace_any(s, s->dU[s->cur], tb), "trace launch");
+        if ((st = part_exchange_cb<T>(s, tb, s->n1 * 4, ZJ_XCHG_TRACES, fn, user)) != ZJ_OK) return st;
+        s->traces_valid = true;
+    }
+    for (int step = 0; step < nsteps; ++step) {
+        for (int stage = 1; stage <= 3; ++stage) {
+            const StageArgsT<T> a = part_stage_args<T>(s, stage);
+            if (is_ns(s)) {
+                ZJ_CK(s, launch_ns_grad(s->P, a, s->stream), "gradient launch");
+                if ((st = part_exchange_cb<T>(s, grad_buf<T>(s), s->n1 * 8, ZJ_XCHG_GRADIENTS, fn, user)) != ZJ_OK)
+                    return st;
+            }
+            ZJ_CK(s, launch_part_stage<T>(s, a), "stage launch");
+            if ((st = part_exchange_cb<T>(s, const_cast<T*>(a.Tout), s->n1 * 4, ZJ_XCHG_TRACES, fn, user)) != ZJ_OK)
+                return st;
+        }
+        s->cur = (s->cur + 1) % 3;
+        s->tpar = 1 - s->tpar;
+        s->time += dt;
+        s->iter += 1;
+    }
+    s->has_norm = true;
+    return ZJ_OK;
+}
+
 template <typename T>
 zj_status parts_rhs_t(const std::vector<zj_solver*>& P, const double* const* Ud, double* const* Rd) {
     const size_t n = P.size();
@@ -1944,6 +2001,22 @@ zj_status zj_parts_step(zj_solver* const* parts, int n, double dt, int nsteps) {
         }
     }
     return P[0]->mixed ? parts_step_t<float>(P, dt, nsteps) : parts_step_t<double>(P, dt, nsteps);
+}
+
+zj_status zj_part_step(zj_solver* s, double dt, int nsteps, zj_exchange_fn exchange, void* user) {
+    if (!s) return ZJ_ERR_ARG;
+    if (!s->is_part) return fail(s, ZJ_ERR_ARG, "zj_part_step steps a part of a partitioned mesh");
+    if (!exchange) return fail(s, ZJ_ERR_ARG, "exchange is NULL");
+    if (nsteps < 0 || !std::isfinite(dt)) return fail(s, ZJ_ERR_ARG, "bad dt or nsteps");
+    if (nsteps == 0) return ZJ_OK;
+    DeviceGuard guard;
+    ZJ_CK(s, cudaSetDevice(s->device), "set device");
+    if (dt != s->last_dt) {
+        k_set_dt<<<1, 1, 0, s->stream>>>(s->dScal, dt);
+        ZJ_CK(s, cudaGetLastError(), "dt launch");
+        s->last_dt = dt;
+    }
+    return s->mixed ? part_step_t<float>(s, nsteps, exchange, user, dt) : part_step_t<double>(s, nsteps, exchange, user, dt);
 }
 
 zj_status zj_parts_rhs(zj_solver* const* parts, int n, const double* const* U_dev, double* const* R_dev) {

@@ -134,3 +134,132 @@ class PartitionedSolver:
         for s in self.parts:
             s.close()
         self.parts = []
+
+
+# ---------------------------------------------------------------------------
+# One process per GPU: a part stepped alone (zj_part_step); the caller's
+# transport moves its cut-face rows at each exchange.
+
+class _DeviceBytes:
+    """A device byte range as an object torch can view without copying
+    (the CUDA array interface)."""
+
+    def __init__(self, ptr: int, nbytes: int):
+        self.__cuda_array_interface__ = {"shape": (int(nbytes),), "typestr": "|u1",
+                                         "data": (int(ptr), False), "version": 2}
+
+
+def device_bytes(ptr: int, nbytes: int):
+    """torch uint8 view of nbytes of device memory at ptr."""
+    import torch
+    return torch.as_tensor(_DeviceBytes(ptr, nbytes), device="cuda")
+
+
+class PartProcess:
+    """Part `rank` of a partition as this process's handle (the reference's
+    rank with its MeshPartitioner slice and MPICommunicator halo).
+    `advance(dt, nsteps, exchange)` steps it; at each exchange the library
+    calls exchange(kind, row_bytes, send_ptr, recv_ptr, stream_ptr) with the
+    part's rows for every neighbour in send (rows [off[i], off[i+1]) of
+    `plan` for neighbour plan["nbr"][i]); it must fill recv with the
+    neighbours' rows for this part in the same layout (see nccl_exchange and
+    LocalExchange)."""
+
+    def __init__(self, mesh, params: L.Params, part: np.ndarray, rank: int):
+        lib = L.lib()
+        self.part = np.ascontiguousarray(part, dtype=np.int32)
+        self.nparts = int(self.part.max()) + 1
+        self.rank = rank
+        d, keep = mesh_desc(mesh)
+        h = C.c_void_p()
+        L.check(lib.zj_solver_create_part(C.byref(d), C.byref(params),
+                                          self.part.ctypes.data_as(C.POINTER(C.c_int32)), self.nparts, rank,
+                                          C.byref(h)))
+        self.solver = FRSolver.from_handle(h, params)
+        self.plan = halo_plan(mesh, self.part, rank)
+        self.elems = self.plan["elems"]
+        self._err = None
+
+    def advance(self, dt: float, nsteps: int, exchange):
+        def cb(user, kind, row_bytes, send, recv, stream):
+            try:
+                return int(exchange(kind, row_bytes, send or 0, recv or 0, stream or 0) or 0)
+            except Exception as e:   # reported after the step returns
+                self._err = e
+                return 1
+        fn = L.EXCHANGE_FN(cb)
+        code = L.lib().zj_part_step(self.solver.h, dt, nsteps, fn, None)
+        if self._err is not None:
+            err, self._err = self._err, None
+            raise err
+        L.check(code, self.solver.h)
+
+    def copyToDevice(self, U_global: np.ndarray):
+        self.solver.copyToDevice(np.ascontiguousarray(U_global[self.elems]))
+
+    def copyToHost(self) -> np.ndarray:
+        return self.solver.copyToHost()
+
+    def close(self):
+        self.solver.close()
+
+
+def nccl_exchange(plan: dict, group=None):
+    """exchange for PartProcess.advance over torch.distributed (NCCL, one
+    process per GPU): per neighbour a send of this part's block and a receive
+    of the neighbour's, batched, ordered on the part's stream."""
+    import torch
+    import torch.distributed as dist
+    nbr, off = [int(q) for q in plan["nbr"]], [int(o) for o in plan["off"]]
+
+    def fn(kind, row_bytes, send_ptr, recv_ptr, stream_ptr):
+        n = off[-1] * row_bytes if off else 0
+        if n == 0:
+            return 0
+        send, recv = device_bytes(send_ptr, n), device_bytes(recv_ptr, n)
+        with torch.cuda.stream(torch.cuda.ExternalStream(stream_ptr)):
+            ops = []
+            for i, q in enumerate(nbr):
+                a, b = off[i] * row_bytes, off[i + 1] * row_bytes
+                ops.append(dist.P2POp(dist.isend, send[a:b], q, group))
+                ops.append(dist.P2POp(dist.irecv, recv[a:b], q, group))
+            for w in dist.batch_isend_irecv(ops):
+                w.wait()   # the part's stream waits for the transfers
+        return 0
+    return fn
+
+
+class LocalExchange:
+    """The transport for parts stepped by threads of one process (all on
+    one device): each thread's exchange publishes its send block, waits for
+    the others, copies its neighbours' blocks for it into its receive buffer
+    and waits again before returning (the senders' buffers are reused by
+    their next exchange).  A failed or missing part breaks the barrier after
+    `timeout` seconds and the steps end with ZJ_ERR_IO."""
+
+    def __init__(self, plans: list, timeout: float = 60.0):
+        import threading
+        self.plans = plans
+        self.sent = {}
+        self.barrier = threading.Barrier(len(plans), timeout=timeout)
+
+    def for_rank(self, rank: int):
+        import torch
+        plan = self.plans[rank]
+
+        def fn(kind, row_bytes, send_ptr, recv_ptr, stream_ptr):
+            torch.cuda.ExternalStream(stream_ptr).synchronize()   # the send block is written
+            self.sent[rank] = send_ptr
+            self.barrier.wait()
+            for i, q in enumerate(plan["nbr"]):
+                pq = self.plans[int(q)]
+                j = int(np.nonzero(pq["nbr"] == rank)[0][0])
+                cnt = int(plan["off"][i + 1] - plan["off"][i])
+                assert cnt == int(pq["off"][j + 1] - pq["off"][j])
+                src = device_bytes(self.sent[int(q)] + int(pq["off"][j]) * row_bytes, cnt * row_bytes)
+                dst = device_bytes(recv_ptr + int(plan["off"][i]) * row_bytes, cnt * row_bytes)
+                dst.copy_(src)
+            torch.cuda.synchronize()
+            self.barrier.wait()
+            return 0
+        return fn
