@@ -47,7 +47,7 @@ __device__ __forceinline__ long long nbr_row(const EdgeRec& r, long long n_elem)
 template <int RS, int VS>
 __device__ __forceinline__ void store_a(const AdjArgs& a, long long idx, int i, int j, double* sA) {
     double l[4];
-    load4(a.L + idx * 4, l);
+    gload4(a.L + idx * 4, l);
     const double iJ = rcp_any(__ldg(a.J + idx));
 #pragma unroll
     for (int v = 0; v < 4; ++v) sA[v * VS + j * RS + i] = -l[v] * iJ;
@@ -99,16 +99,16 @@ __device__ __forceinline__ void transposed_traces(const double* sT, int stride, 
 // Final value of one solution point: W itself, or the fused stage update.
 __device__ __forceinline__ void store_result(const AdjArgs& a, long long idx, const double* w) {
     if (!a.out) {
-        store4(a.W + idx * 4, w);
+        gstore4(a.W + idx * 4, w);
         return;
     }
     double r[4], x[4];
 #pragma unroll
     for (int v = 0; v < 4; ++v) r[v] = a.cw * w[v];
-    if (a.X0) { load4(a.X0 + idx * 4, x); for (int v = 0; v < 4; ++v) r[v] = fma(a.c0, x[v], r[v]); }
-    if (a.X1) { load4(a.X1 + idx * 4, x); for (int v = 0; v < 4; ++v) r[v] = fma(a.c1, x[v], r[v]); }
-    if (a.X2) { load4(a.X2 + idx * 4, x); for (int v = 0; v < 4; ++v) r[v] = fma(a.c2, x[v], r[v]); }
-    store4(a.out + idx * 4, r);
+    if (a.X0) { gload4(a.X0 + idx * 4, x); for (int v = 0; v < 4; ++v) r[v] = fma(a.c0, x[v], r[v]); }
+    if (a.X1) { gload4(a.X1 + idx * 4, x); for (int v = 0; v < 4; ++v) r[v] = fma(a.c1, x[v], r[v]); }
+    if (a.X2) { gload4(a.X2 + idx * 4, x); for (int v = 0; v < 4; ++v) r[v] = fma(a.c2, x[v], r[v]); }
+    gstore4(a.out + idx * 4, r);
 }
 
 // ---------------------------------------------------------------- pass A --
@@ -134,7 +134,7 @@ k_adj_dfbar(const AdjArgs a) {
         const int edge = k / N1, fp = k - edge * N1;
         double t[4];
         trace_point<N1, RS, VS>(sA + el * FS, sW, sW + N1, edge, fp, t);
-        store4(a.Db + (e * NFT + k) * 4, t);
+        gstore4(a.Db + (e * NFT + k) * 4, t);
     }
 }
 
@@ -168,19 +168,19 @@ k_adj_euler(const AdjArgs a) {
         double n[3];
         load_normal(a.enrm + e * 4 + edge, n);
         nx = n[0]; ny = n[1]; len = n[2];
-        load4(a.T + (e * NFT + k) * 4, qo);
+        gload4(a.T + (e * NFT + k) * 4, qo);
         double df[4];
-        load4(a.Db + (e * NFT + k) * 4, df);
+        gload4(a.Db + (e * NFT + k) * 4, df);
         store4(sDF + el * DS + k * 4, df);
-        if (!(r.flags & kEdgeOrphan)) load4(a.T + (nbr_row(r, a.n_elem) * N1 + (N1 - 1 - fp)) * 4, qn);
+        if (!(r.flags & kEdgeOrphan)) gload4(a.T + (nbr_row(r, a.n_elem) * N1 + (N1 - 1 - fp)) * 4, qn);
         if (!(r.flags & (kEdgeOrphan | kEdgeBoundary)))
-            load4(a.Db + (((long long)r.nbr * 4 + r.nbr_edge) * N1 + (N1 - 1 - fp)) * 4, dfn);
+            gload4(a.Db + (((long long)r.nbr * 4 + r.nbr_edge) * N1 + (N1 - 1 - fp)) * 4, dfn);
     }
     double u[4], ji[4], Jd = 1.0;
     if (is_sp) {
         const long long idx = e * NSP + k;
-        load4(a.U + idx * 4, u);
-        load4(a.Jinv + idx * 4, ji);
+        gload4(a.U + idx * 4, u);
+        gload4(a.Jinv + idx * 4, ji);
         Jd = __ldg(a.J + idx);
         store_a<RS, VS>(a, idx, i, j, sA + el * FS);
     }
@@ -257,23 +257,23 @@ k_adj_ns(const AdjArgs a) {
         double n[3];
         load_normal(a.enrm + e * 4 + edge, n);
         nx = n[0]; ny = n[1]; len = n[2];
-        load4(a.T + (e * NFT + k) * 4, qo);
+        gload4(a.T + (e * NFT + k) * 4, qo);
 #pragma unroll
         for (int v = 0; v < 4; ++v) qn[v] = qo[v];
         double df[4];
-        load4(a.Db + (e * NFT + k) * 4, df);
+        gload4(a.Db + (e * NFT + k) * 4, df);
         store4(sDF + el * DS + k * 4, df);
         const double* qt = a.TQ + (e * NFT + k) * 8;
-        load4(qt, Qo);
-        load4(qt + 4, Qo + 4);
+        gload4(qt, Qo);
+        gload4(qt + 4, Qo + 4);
 #pragma unroll
         for (int v = 0; v < 8; ++v) Qn[v] = Qo[v];
-        if (!(r.flags & kEdgeOrphan)) load4(a.T + (nbr_row(r, a.n_elem) * N1 + (N1 - 1 - fp)) * 4, qn);
+        if (!(r.flags & kEdgeOrphan)) gload4(a.T + (nbr_row(r, a.n_elem) * N1 + (N1 - 1 - fp)) * 4, qn);
         if (!(r.flags & (kEdgeOrphan | kEdgeBoundary))) {
             const long long nrow = ((long long)r.nbr * 4 + r.nbr_edge) * N1 + (N1 - 1 - fp);
-            load4(a.Db + nrow * 4, dfn);
-            load4(a.TQ + nrow * 8, Qn);
-            load4(a.TQ + nrow * 8 + 4, Qn + 4);
+            gload4(a.Db + nrow * 4, dfn);
+            gload4(a.TQ + nrow * 8, Qn);
+            gload4(a.TQ + nrow * 8 + 4, Qn + 4);
         }
         double d[4];
 #pragma unroll
@@ -283,8 +283,8 @@ k_adj_ns(const AdjArgs a) {
     double u[4], ji[4], Jd = 1.0;
     if (is_sp) {
         const long long idx = e * NSP + k;
-        load4(a.U + idx * 4, u);
-        load4(a.Jinv + idx * 4, ji);
+        gload4(a.U + idx * 4, u);
+        gload4(a.Jinv + idx * 4, ji);
         Jd = __ldg(a.J + idx);
         store_a<RS, VS>(a, idx, i, j, sA + el * FS);
 #pragma unroll
@@ -392,7 +392,7 @@ k_adj_ns(const AdjArgs a) {
             }
             ub[v] += acc;
         }
-        store4(a.W + (e * NSP + k) * 4, ub);
+        gstore4(a.W + (e * NSP + k) * 4, ub);
     }
     if (is_fp) {
         const double* gL = sOps + N1 * N1 + 2 * N1;
@@ -415,8 +415,8 @@ k_adj_ns(const AdjArgs a) {
             adj::ghost_vjp(qo, nx, ny, edge_bc_type(r.flags), a.bc + (long long)r.nbr_edge * 8, g,
                            hb, tb);
         }
-        store4(a.Tb + (e * NFT + k) * 4, tb);
-        store4(a.DUb + (e * NFT + k) * 4, dub);
+        gstore4(a.Tb + (e * NFT + k) * 4, tb);
+        gstore4(a.DUb + (e * NFT + k) * 4, dub);
     }
 }
 
@@ -439,11 +439,11 @@ k_adj_ns_gather(const AdjArgs a) {
     if (valid && k < NFT) {
         const int edge = k / N1, fp = k - edge * N1;
         double tb[4];
-        load4(a.Tb + (e * NFT + k) * 4, tb);
+        gload4(a.Tb + (e * NFT + k) * 4, tb);
         const EdgeRec r = a.edges[e * 4 + edge];
         if (!(r.flags & (kEdgeOrphan | kEdgeBoundary))) {
             double dn[4];
-            load4(a.DUb + (((long long)r.nbr * 4 + r.nbr_edge) * N1 + (N1 - 1 - fp)) * 4, dn);
+            gload4(a.DUb + (((long long)r.nbr * 4 + r.nbr_edge) * N1 + (N1 - 1 - fp)) * 4, dn);
 #pragma unroll
             for (int v = 0; v < 4; ++v) tb[v] += 0.5 * dn[v];
         }
@@ -452,7 +452,7 @@ k_adj_ns_gather(const AdjArgs a) {
     __syncthreads();
     if (valid && k < NSP) {
         double w[4];
-        load4(a.W + (e * NSP + k) * 4, w);
+        gload4(a.W + (e * NSP + k) * 4, w);
         transposed_traces<N1, 4>(sTb + el * DS, 4, sOps, k % N1, k / N1, w);
         store_result(a, e * NSP + k, w);
     }
