@@ -167,3 +167,27 @@ def test_part_step_reports_a_failed_transport(zjlib):
     failing = L.EXCHANGE_FN(lambda *args: 3)
     assert zjlib.zj_part_step(p.solver.h, 1e-6, 1, failing, None) == L.ERR_IO
     p.close()
+
+
+def test_a_one_part_partition_is_the_whole_mesh(zjlib):
+    """No cut faces: every exchange moves zero rows, through both drivers."""
+    mesh = M.tgv_mesh(12, seed=2)
+    prm = make_params(poly_order=2, rho_inf=1.0, p_inf=1.0 / (1.4 * 0.09), Mach=0.3, riemann="Rusanov",
+                      compat=False, viscous=True, Re=1000.0, Pr=0.72, bcs=[(1, "slipwall")])
+    whole = FRSolver(mesh, prm)
+    U0 = M.taylor_green(whole.solution_point_coords())
+    whole.copyToDevice(U0)
+    whole.advance(1e-4, 4)
+    parts = PT.PartitionedSolver(mesh, prm, 1)
+    parts.copyToDevice(U0)
+    parts.advance(1e-4, 4)
+    assert np.array_equal(parts.copyToHost(), whole.copyToHost())
+    parts.close()
+    one = PT.PartProcess(mesh, prm, np.zeros(mesh.n_elem, dtype=np.int32), 0)
+    one.copyToDevice(U0)
+    calls = []
+    one.advance(1e-4, 4, lambda kind, row_bytes, send, recv, stream: calls.append((kind, row_bytes)) or 0)
+    assert np.array_equal(one.copyToHost(), whole.copyToHost())
+    # the state traces once, then per stage the gradient traces and the new traces
+    assert calls[0] == (L.XCHG_TRACES, 3 * 4 * 8) and len(calls) == 1 + 4 * 3 * 2
+    one.close()
