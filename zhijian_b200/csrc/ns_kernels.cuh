@@ -59,7 +59,10 @@
 #define ZJ_NSL_MIN_BLOCKS_HI 4    // the same from P4 up (no spills)
 #endif
 #ifndef ZJ_NSL32_MIN_BLOCKS
-#define ZJ_NSL32_MIN_BLOCKS 6     // mixed-precision gradient kernel by lines
+#define ZJ_NSL32_MIN_BLOCKS 8     // mixed-precision gradient kernel by lines (64 registers)
+#endif
+#ifndef ZJ_NSL32_MIN_BLOCKS_HI
+#define ZJ_NSL32_MIN_BLOCKS_HI 6  // the same from P4 up (no spills)
 #endif
 
 namespace zj {
@@ -295,7 +298,10 @@ struct LineShape {
     // dynamic shared memory layout (byte offsets, 16-byte aligned)
     static constexpr size_t OFF_U = 0;
     static constexpr size_t OFF_J = OFF_U + sizeof(double) * EB * EU;
-    static constexpr size_t OFF_D = OFF_J + sizeof(T) * EB * EJ;
+    // FP64 metrics are staged with the states; FP32 ones (16 bytes a point)
+    // are read directly, which measured faster than staging them
+    static constexpr bool kStageJ = sizeof(T) == 8;
+    static constexpr size_t OFF_D = OFF_J + (kStageJ ? sizeof(T) * EB * EJ : 0);
     static constexpr size_t OFF_OPS = OFF_D + ((sizeof(T) * EB * ES + 15) & ~size_t(15));
     static constexpr size_t SMEM = OFF_OPS + ((sizeof(T) * NOPS + 15) & ~size_t(15));
     static_assert(OFF_J % 16 == 0 && OFF_D % 16 == 0 && OFF_OPS % 16 == 0, "16-byte aligned regions");
@@ -303,7 +309,8 @@ struct LineShape {
     // of a point thread, at half the threads per element.
     // (the counts are per 128 threads; other CTA sizes scale them)
     static constexpr int MIN_BLOCKS_128 =
-        sizeof(T) == 8 ? (P <= 3 ? ZJ_NSL_MIN_BLOCKS : ZJ_NSL_MIN_BLOCKS_HI) : ZJ_NSL32_MIN_BLOCKS;
+        sizeof(T) == 8 ? (P <= 3 ? ZJ_NSL_MIN_BLOCKS : ZJ_NSL_MIN_BLOCKS_HI)
+                       : (P <= 3 ? ZJ_NSL32_MIN_BLOCKS : ZJ_NSL32_MIN_BLOCKS_HI);
     static constexpr int MIN_BLOCKS = MIN_BLOCKS_128 * 128 / kCtaThreads > 0 ? MIN_BLOCKS_128 * 128 / kCtaThreads : 1;
 };
 
@@ -331,7 +338,7 @@ k_ns_grad_lines(const StageArgsT<T> a) {
     const int tid = threadIdx.x;
     // metrics: 16-byte pieces of the CTA's elements (geometry: before pdl_wait)
     constexpr int KJ = 4 / TW;                 // pieces per point
-    for (int c = tid; c < EB * NSP * KJ; c += L::THREADS) {
+    for (int c = tid; L::kStageJ && c < EB * NSP * KJ; c += L::THREADS) {
         const int el2 = c / (NSP * KJ), r = c - el2 * NSP * KJ, p = r / KJ, h = r - p * KJ;
         bool v2;
         const long long e2 = block_element(a, EB, el2, v2);
@@ -446,7 +453,8 @@ k_ns_grad_lines(const StageArgsT<T> a) {
 #pragma unroll
     for (int m = 0; m < N1; ++m) {
         T ji[4];
-        load4(sj + m * jstride, ji);
+        if constexpr (L::kStageJ) load4(sj + m * jstride, ji);
+        else load4_nc(a.Jinv + (e * NSP + (role ? line + m * N1 : line * N1 + m)) * 4, ji);
         const T wa = WA[m], wb = WB[m];
 #pragma unroll
         for (int v = 0; v < 4; ++v) {
