@@ -255,11 +255,9 @@ k_ns_grad(const StageArgsT<T> a) {
 //
 // 2 N1 threads per element: one per row j (an xi-line of solution points
 // (0..N1-1, j)) and one per column i (an eta-line (i, 0..N1-1)).  The CTA
-// first stages its elements' states and metrics into shared memory with
-// 16-byte cp.async copies (each 16-byte piece fetched once, the metrics before
-// pdl_wait since they never come from a kernel), while every line thread
-// loads the traces at its line's two end points (its own and the
-// neighbour's).  A line thread then takes the corrected derivative along its
+// first stages its elements' states into shared memory with 16-byte cp.async
+// copies (each 16-byte piece fetched once), while every line thread loads the
+// traces at its line's two end points (its own and the neighbour's).  A line thread then takes the corrected derivative along its
 // line in registers (row: dU/dxi with the jumps of edges 1 and 3; column:
 // dU/deta with those of edges 0 and 2) and swaps derivatives with the
 // crossing lines through one shared tile.  It forms Q = (xi_x dU/dxi + eta_x
@@ -290,21 +288,14 @@ struct LineShape {
     // element stride 64 bytes past a multiple of 128
     static constexpr int RU = N1 * 4 + 2;
     static constexpr int EU = N1 * RU + ((8 - (N1 * RU) % 16) + 16) % 16;
-    // staged metrics (T): [el][b][a*4 + c], same padding rules
-    static constexpr int TW = 16 / sizeof(T);            // values per 16 bytes
-    static constexpr int RJ = N1 * 4 + TW;
-    static constexpr int JM = 128 / sizeof(T), JO = 64 / sizeof(T);
-    static constexpr int EJ = N1 * RJ + ((JO - (N1 * RJ) % JM) + JM) % JM;
-    // dynamic shared memory layout (byte offsets, 16-byte aligned)
+    // dynamic shared memory layout (byte offsets, 16-byte aligned); the
+    // metrics are read directly (one 16- or 32-byte load a point), which
+    // measured faster than staging them with the states
     static constexpr size_t OFF_U = 0;
-    static constexpr size_t OFF_J = OFF_U + sizeof(double) * EB * EU;
-    // FP64 metrics are staged with the states; FP32 ones (16 bytes a point)
-    // are read directly, which measured faster than staging them
-    static constexpr bool kStageJ = sizeof(T) == 8;
-    static constexpr size_t OFF_D = OFF_J + (kStageJ ? sizeof(T) * EB * EJ : 0);
+    static constexpr size_t OFF_D = OFF_U + sizeof(double) * EB * EU;
     static constexpr size_t OFF_OPS = OFF_D + ((sizeof(T) * EB * ES + 15) & ~size_t(15));
     static constexpr size_t SMEM = OFF_OPS + ((sizeof(T) * NOPS + 15) & ~size_t(15));
-    static_assert(OFF_J % 16 == 0 && OFF_D % 16 == 0 && OFF_OPS % 16 == 0, "16-byte aligned regions");
+    static_assert(OFF_D % 16 == 0 && OFF_OPS % 16 == 0, "16-byte aligned regions");
     // A line thread holds a line's states and derivatives: twice the values
     // of a point thread, at half the threads per element.
     // (the counts are per 128 threads; other CTA sizes scale them)
@@ -328,23 +319,13 @@ __global__ void __launch_bounds__(LineShape<P, T>::THREADS, LineShape<P, T>::MIN
 k_ns_grad_lines(const StageArgsT<T> a) {
     using L = LineShape<P, T>;
     constexpr int N1 = L::N1, NSP = L::NSP, NFT = L::NFT, EB = L::EB, R = L::R, VB = L::VB, ES = L::ES;
-    constexpr int RU = L::RU, EU = L::EU, RJ = L::RJ, EJ = L::EJ, TW = L::TW;
+    constexpr int RU = L::RU, EU = L::EU;
     extern __shared__ __align__(16) unsigned char smem[];
     double* sU = reinterpret_cast<double*>(smem + L::OFF_U);
-    T* sJ = reinterpret_cast<T*>(smem + L::OFF_J);
     T* sD = reinterpret_cast<T*>(smem + L::OFF_D);
     T* sOps = reinterpret_cast<T*>(smem + L::OFF_OPS);
 
     const int tid = threadIdx.x;
-    // metrics: 16-byte pieces of the CTA's elements (geometry: before pdl_wait)
-    constexpr int KJ = 4 / TW;                 // pieces per point
-    for (int c = tid; L::kStageJ && c < EB * NSP * KJ; c += L::THREADS) {
-        const int el2 = c / (NSP * KJ), r = c - el2 * NSP * KJ, p = r / KJ, h = r - p * KJ;
-        bool v2;
-        const long long e2 = block_element(a, EB, el2, v2);
-        if (v2) cp_async16(sJ + el2 * EJ + (p / N1) * RJ + (p % N1) * 4 + h * TW, a.Jinv + (e2 * NSP + p) * 4 + h * TW);
-    }
-    cp_async_commit();
     for (int t = tid; t < L::NOPS; t += L::THREADS) sOps[t] = a.ops[t];
     pdl_launch_dependents();
     pdl_wait();   // the state and traces come from the previous stage
@@ -363,7 +344,6 @@ k_ns_grad_lines(const StageArgsT<T> a) {
     const long long e = block_element(a, EB, el, valid);
     // staged offset of the line's point m: row j -> (m, j), column i -> (i, m)
     const int ubase = role ? line * 4 : line * RU, ustride = role ? RU : 4;
-    const int jbase = role ? line * 4 : line * RJ, jstride = role ? RJ : 4;
     // derivative-tile offset of point m: (a, b) -> a*R + b
     const int tbase = role ? line * R : line, tstride = role ? 1 : R;
     const int eA = role ? 0 : 1, eB = role ? 2 : 3;
@@ -388,7 +368,7 @@ k_ns_grad_lines(const StageArgsT<T> a) {
         }
     }
     cp_async_wait_all();
-    __syncthreads();   // staged states and metrics, operators
+    __syncthreads();   // staged states, operators
 
     T mine[N1][4];
     if (valid) {
@@ -446,15 +426,13 @@ k_ns_grad_lines(const StageArgsT<T> a) {
     const T* WA = sOps + N1 * N1 + (role ? 0 : N1);   // row: l(+1) at edge 1; column: l(-1) at edge 0
     const T* WB = sOps + N1 * N1 + (role ? N1 : 0);   // row: l(-1) at edge 3; column: l(+1) at edge 2
     const T* so = sD + el * ES + (1 - role) * 4 * VB + tbase;
-    const T* sj = sJ + el * EJ + jbase;
     T tA[8], tB[8];
 #pragma unroll
     for (int c = 0; c < 8; ++c) { tA[c] = T(0); tB[c] = T(0); }
 #pragma unroll
     for (int m = 0; m < N1; ++m) {
         T ji[4];
-        if constexpr (L::kStageJ) load4(sj + m * jstride, ji);
-        else load4_nc(a.Jinv + (e * NSP + (role ? line + m * N1 : line * N1 + m)) * 4, ji);
+        load4_nc(a.Jinv + (e * NSP + (role ? line + m * N1 : line * N1 + m)) * 4, ji);
         const T wa = WA[m], wb = WB[m];
 #pragma unroll
         for (int v = 0; v < 4; ++v) {
